@@ -1,0 +1,468 @@
+/*
+ * ORACLE (test infrastructure only): prove_multi for the Goldilocks/Poseidon2
+ * configuration, restated step by step from
+ *   p3-miden-lifted-stark/src/prover/mod.rs:223-461        (protocol order)
+ *   p3-miden-lifted-stark/src/prover/commit.rs:175-228     (trace commitment)
+ *   p3-miden-lifted-stark/src/prover/quotient.rs:40-238    (quotient)
+ *   p3-miden-lifted-stark/src/prover/constraints/mod.rs:63-179 (constraint fold)
+ *   p3-miden-lifted-stark/src/coset.rs:210-342             (selectors, OOD point)
+ *   p3-miden-lifted-fri/src/prover.rs:35-116               (PCS opening)
+ *   p3-miden-lifted-fri/src/deep/{interpolate,prover}.rs   (DEEP)
+ *   p3-miden-lifted-fri/src/fri/{mod,prover}.rs, fri/fold/arity{2,4,8}.rs (FRI)
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include "oracle.h"
+
+static double g_stage[16];
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+double or_last_stage_seconds(int stage) { return (stage >= 0 && stage < 16) ? g_stage[stage] : 0.0; }
+
+typedef struct {
+    or_tree tree;
+    uint64_t *ldes[8];
+    size_t n;
+} committed;
+
+/* commit_traces: per trace, coset LDE on the nested coset g^(2^lift) and
+ * bit-reversed rows; then an aligned LMCS tree (commit.rs:198-227). */
+static void commit_traces(const or_p2_params *pp, committed *c, const uint64_t *const *traces, const size_t *h,
+                          const size_t *w, size_t n, unsigned log_blowup) {
+    unsigned log_max = or_log2(h[n - 1]);
+    or_matrix mats[8];
+    c->n = n;
+    for (size_t i = 0; i < n; i++) {
+        unsigned lift = log_max - or_log2(h[i]);
+        uint64_t shift = or_exp2(OR_GEN, lift);
+        size_t lh = h[i] << log_blowup;
+        c->ldes[i] = (uint64_t *)malloc(lh * w[i] * 8 + 8);
+        or_coset_lde_bitrev(traces[i], h[i], w[i], log_blowup, shift, c->ldes[i]);
+        mats[i].data = c->ldes[i];
+        mats[i].height = lh;
+        mats[i].width = w[i];
+    }
+    or_tree_build(pp, &c->tree, mats, n, 8);
+}
+static void committed_free(committed *c) {
+    for (size_t i = 0; i < c->n; i++) free(c->ldes[i]);
+    or_tree_free(&c->tree);
+}
+
+/* arity-a fold of one coset row (fri/fold/arity{2,4,8}.rs): evals are
+ * bit-reversed samples y_k = f(s w_a^k); result (1/a) sum_j (beta/s)^j
+ * sum_k y_k w_a^{-jk}. */
+static or_ef fold_row(const or_ef *ev, unsigned log_a, uint64_t s_inv, or_ef beta) {
+    size_t a = (size_t)1 << log_a;
+    uint64_t winv = or_inv(or_root(log_a));
+    or_ef x = or_ef_mulf(beta, s_inv), xp = or_ef_from(1), res = or_ef_from(0);
+    for (size_t j = 0; j < a; j++) {
+        or_ef u = or_ef_from(0);
+        for (size_t k = 0; k < a; k++) {
+            uint64_t wk = or_pow(winv, (j * k) % a);
+            u = or_ef_add(u, or_ef_mulf(ev[or_bitrev(k, log_a)], wk));
+        }
+        res = or_ef_add(res, or_ef_mul(u, xp));
+        xp = or_ef_mul(xp, x);
+    }
+    return or_ef_mulf(res, or_inv((uint64_t)a));
+}
+
+static int cmp_size(const void *a, const void *b) {
+    size_t x = *(const size_t *)a, y = *(const size_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
+             or_proof *out) {
+    memset(out, 0, sizeof(*out));
+    memset(g_stage, 0, sizeof(g_stage));
+    if (n_inst == 0 || n_inst > 8) return 1;
+    for (size_t i = 0; i < n_inst; i++) {
+        if (inst[i].height < 2 || (inst[i].height & (inst[i].height - 1))) return 2;
+        if (i && inst[i].height < inst[i - 1].height) return 3;
+    }
+    const unsigned log_blowup = pcs->log_blowup;
+    const unsigned log_max_h = or_log2(inst[n_inst - 1].height);
+    unsigned log_qd = 0;
+    for (size_t i = 0; i < n_inst; i++) {
+        unsigned l = or_air_log_quotient_degree(inst[i].air);
+        if (l > log_qd) log_qd = l;
+    }
+    if (log_qd > log_blowup) return 4;
+    const unsigned log_lde = log_max_h + log_blowup;
+    const size_t n_lde = (size_t)1 << log_lde;
+    const size_t D = (size_t)1 << log_qd;
+    double t0 = now_s(), t1;
+
+    or_transcript tr;
+    or_tr_init(&tr, pp);
+
+    /* 1. main traces */
+    const uint64_t *traces[8];
+    size_t hs[8], ws[8];
+    for (size_t i = 0; i < n_inst; i++) {
+        traces[i] = inst[i].trace;
+        hs[i] = inst[i].height;
+        ws[i] = inst[i].width;
+    }
+    committed mainc, auxc, quotc;
+    commit_traces(pp, &mainc, traces, hs, ws, n_inst, log_blowup);
+    or_tree_root(&mainc.tree, out->main_root);
+    or_tr_send_commit(&tr, out->main_root);
+    t1 = now_s();
+    g_stage[0] = t1 - t0;
+    t0 = t1;
+
+    /* 2. randomness (max over AIRs of num_randomness = 1) and the dummy aux
+     * traces: one EF column of zeros, flattened to 2 base columns
+     * (p3-miden-lifted-examples/src/lib.rs:93-103, prover/mod.rs:290-345). */
+    or_ef rnd = or_ch_sample_ef(&tr.ch);
+    (void)rnd;
+    uint64_t *auxt[8];
+    size_t aw[8];
+    for (size_t i = 0; i < n_inst; i++) {
+        auxt[i] = (uint64_t *)calloc(hs[i] * 2, 8);
+        aw[i] = 2;
+    }
+    commit_traces(pp, &auxc, (const uint64_t *const *)auxt, hs, aw, n_inst, log_blowup);
+    for (size_t i = 0; i < n_inst; i++) free(auxt[i]);
+    or_tree_root(&auxc.tree, out->aux_root);
+    or_tr_send_commit(&tr, out->aux_root);
+    t1 = now_s();
+    g_stage[1] = t1 - t0;
+    t0 = t1;
+
+    /* 4. constraint folding alpha, accumulation beta */
+    or_ef alpha = or_ch_sample_ef(&tr.ch);
+    or_ef beta = or_ch_sample_ef(&tr.ch);
+    out->alpha[0] = alpha.c0, out->alpha[1] = alpha.c1;
+    out->beta[0] = beta.c0, out->beta[1] = beta.c1;
+
+    /* 5. constraints, ascending heights, cyclic extension + beta Horner */
+    const size_t max_qh = inst[n_inst - 1].height * D;
+    or_ef *acc = (or_ef *)calloc(max_qh, sizeof(or_ef));
+    size_t acc_len = 0;
+    for (size_t ii = 0; ii < n_inst; ii++) {
+        const or_instance *I = &inst[ii];
+        unsigned log_h = or_log2(I->height);
+        unsigned lift = log_max_h - log_h;
+        uint64_t shift = or_exp2(OR_GEN, lift);
+        size_t qh = I->height * D;
+        unsigned log_qh = log_h + log_qd;
+        /* cyclic_extend_and_scale (quotient.rs:348-363) */
+        if (acc_len == 0) {
+            memset(acc, 0, qh * sizeof(or_ef));
+        } else {
+            for (size_t i = 0; i < acc_len; i++) acc[i] = or_ef_mul(acc[i], beta);
+            while (acc_len < qh) {
+                memcpy(acc + acc_len, acc, acc_len * sizeof(or_ef));
+                acc_len *= 2;
+            }
+        }
+        acc_len = qh;
+        /* selectors on the quotient coset (coset.rs:210-247) */
+        uint64_t omega_h_inv = or_inv(or_root(log_h));
+        uint64_t omega_q = or_root(log_qh);
+        size_t K = or_air_num_constraints(I->air, I->width);
+        const uint64_t *lde = mainc.ldes[ii];
+        size_t w = I->width;
+#pragma omp parallel
+        {
+            uint64_t *cons = (uint64_t *)malloc(K * 8);
+#pragma omp for schedule(static)
+            for (size_t m = 0; m < qh; m++) {
+                uint64_t x = or_mul(shift, or_pow(omega_q, m));
+                uint64_t zh = or_sub(or_exp2(x, log_h), 1);
+                uint64_t sel[3];
+                sel[0] = or_mul(zh, or_inv(or_sub(x, 1)));
+                sel[1] = or_mul(zh, or_inv(or_sub(x, omega_h_inv)));
+                sel[2] = or_sub(x, omega_h_inv);
+                const uint64_t *L = lde + or_bitrev(m, log_qh) * w;
+                const uint64_t *N = lde + or_bitrev((m + D) % qh, log_qh) * w;
+                or_air_eval(I->air, w, I->consts, L, N, sel, cons);
+                or_ef f = or_ef_from(0);
+                for (size_t k = 0; k < K; k++) f = or_ef_add(or_ef_mul(f, alpha), or_ef_from(cons[k]));
+                acc[m] = or_ef_add(acc[m], f);
+            }
+            free(cons);
+        }
+    }
+    /* 6. divide by Z_H on the max quotient coset (quotient.rs:380-409) */
+    {
+        uint64_t s_pow_n = or_exp2(OR_GEN, log_max_h);
+        uint64_t wd = or_root(log_qd), p = 1;
+        uint64_t inv_van[64];
+        for (size_t t = 0; t < D; t++) {
+            inv_van[t] = or_inv(or_sub(or_mul(s_pow_n, p), 1));
+            p = or_mul(p, wd);
+        }
+        for (size_t i = 0; i < max_qh; i++) acc[i] = or_ef_mulf(acc[i], inv_van[i & (D - 1)]);
+    }
+    t1 = now_s();
+    g_stage[2] = t1 - t0;
+    t0 = t1;
+
+    /* 7. commit_quotient (quotient.rs:441-546) */
+    {
+        size_t N = inst[n_inst - 1].height, NB = N << log_blowup, qw = 2 * D;
+        uint64_t *qm = (uint64_t *)malloc(NB * qw * 8);
+        uint64_t omega_j_inv = or_inv(or_root(log_max_h + log_qd));
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t col = 0; col < qw; col++) {
+            size_t t = col / 2, comp = col & 1;
+            uint64_t *v = (uint64_t *)calloc(NB, 8);
+            for (size_t r = 0; r < N; r++) v[r] = comp ? acc[r * D + t].c1 : acc[r * D + t].c0;
+            or_intt(v, N);
+            uint64_t rb = 1; /* (omega_j^-k)^t */
+            uint64_t step = or_pow(omega_j_inv, t);
+            for (size_t k = 0; k < N; k++) {
+                v[k] = or_mul(v[k], rb);
+                rb = or_mul(rb, step);
+            }
+            or_ntt(v, NB);
+            for (size_t i = 0; i < NB; i++) qm[or_bitrev(i, log_lde) * qw + col] = v[i];
+            free(v);
+        }
+        or_matrix m = {qm, NB, qw};
+        or_tree_build(pp, &quotc.tree, &m, 1, 8);
+        quotc.ldes[0] = qm;
+        quotc.n = 1;
+        or_tree_root(&quotc.tree, out->quot_root);
+        or_tr_send_commit(&tr, out->quot_root);
+    }
+    free(acc);
+    t1 = now_s();
+    g_stage[3] = t1 - t0;
+    t0 = t1;
+
+    /* 8. OOD point outside H and gK (coset.rs:329-342), z_next = z * w_N */
+    or_ef z;
+    for (;;) {
+        z = or_ch_sample_ef(&tr.ch);
+        int in_h = or_ef_eq(or_ef_exp2(z, log_max_h), or_ef_from(1));
+        int in_gk = or_ef_eq(or_ef_exp2(or_ef_mulf(z, or_inv(OR_GEN)), log_lde), or_ef_from(1));
+        if (!in_h && !in_gk) break;
+    }
+    or_ef zs[2] = {z, or_ef_mulf(z, or_root(log_max_h))};
+    out->z[0] = z.c0, out->z[1] = z.c1;
+
+    /* 9. PCS opening: DEEP (deep/prover.rs:171-409, interpolate.rs:81-201) */
+    committed *trees[3] = {&mainc, &auxc, &quotc};
+    size_t n_mats_total = 0;
+    const or_matrix *allm[24];
+    for (int g = 0; g < 3; g++)
+        for (size_t m = 0; m < trees[g]->tree.n_mats; m++) allm[n_mats_total++] = &trees[g]->tree.mats[m];
+    /* coset points gK, bit-reversed */
+    uint64_t *xs = (uint64_t *)malloc(n_lde * 8);
+    {
+        uint64_t wn = or_root(log_lde);
+#pragma omp parallel for schedule(static)
+        for (size_t i = 0; i < n_lde; i++) xs[i] = or_mul(OR_GEN, or_pow(wn, or_bitrev(i, log_lde)));
+    }
+    or_ef *q = (or_ef *)malloc(n_lde * 2 * sizeof(or_ef));
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n_lde; i++)
+        for (int j = 0; j < 2; j++) q[2 * i + j] = or_ef_inv(or_ef_sub(zs[j], or_ef_from(xs[i])));
+    /* barycentric evaluation of the first d_m rows of each LDE */
+    size_t d = n_lde >> log_blowup;
+    unsigned log_d = or_log2(d);
+    or_ef sj[2];
+    for (int j = 0; j < 2; j++) {
+        or_ef t = or_ef_sub(or_ef_exp2(or_ef_mulf(zs[j], or_inv(OR_GEN)), log_d), or_ef_from(1));
+        sj[j] = or_ef_mulf(t, or_inv((uint64_t)d));
+    }
+    size_t total_aligned = 0, aligned_w[24];
+    for (size_t m = 0; m < n_mats_total; m++) {
+        aligned_w[m] = (allm[m]->width + 7) / 8 * 8;
+        total_aligned += aligned_w[m];
+    }
+    or_ef *evals = (or_ef *)calloc(total_aligned * 2, sizeof(or_ef)); /* [col][j] */
+    {
+        or_ef *wts = (or_ef *)malloc(d * 2 * sizeof(or_ef));
+        size_t off = 0;
+        for (size_t m = 0; m < n_mats_total; m++) {
+            const or_matrix *M = allm[m];
+            size_t dm = M->height >> log_blowup, ratio = d / dm;
+            for (size_t i = 0; i < dm; i++)
+                for (int j = 0; j < 2; j++) {
+                    or_ef s = or_ef_from(0);
+                    for (size_t c = 0; c < ratio; c++) {
+                        size_t ii = i * ratio + c;
+                        s = or_ef_add(s, or_ef_mulf(q[2 * ii + j], xs[ii]));
+                    }
+                    wts[2 * i + j] = s;
+                }
+#pragma omp parallel for schedule(static)
+            for (size_t col = 0; col < M->width; col++)
+                for (int j = 0; j < 2; j++) {
+                    or_ef s = or_ef_from(0);
+                    for (size_t i = 0; i < dm; i++) s = or_ef_add(s, or_ef_mulf(wts[2 * i + j], M->data[i * M->width + col]));
+                    evals[2 * (off + col) + j] = or_ef_mul(s, sj[j]);
+                }
+            off += aligned_w[m];
+        }
+        free(wts);
+    }
+    for (int j = 0; j < 2; j++)
+        for (size_t c = 0; c < total_aligned; c++) or_tr_send_ef(&tr, evals[2 * c + j]);
+    or_tr_grind(&tr, pcs->deep_pow_bits);
+    or_ef ac = or_ch_sample_ef(&tr.ch);
+    or_ef bp = or_ch_sample_ef(&tr.ch);
+    out->deep_alpha[0] = ac.c0, out->deep_alpha[1] = ac.c1;
+    out->deep_beta[0] = bp.c0, out->deep_beta[1] = bp.c1;
+    or_ef fred[2] = {or_ef_from(0), or_ef_from(0)};
+    for (size_t c = 0; c < total_aligned; c++)
+        for (int j = 0; j < 2; j++) fred[j] = or_ef_add(or_ef_mul(fred[j], ac), evals[2 * c + j]);
+    /* coefficients -alpha^{W-1-c} */
+    or_ef *coef = (or_ef *)malloc(total_aligned * sizeof(or_ef));
+    {
+        or_ef p = or_ef_from(OR_P - 1);
+        for (size_t c = total_aligned; c-- > 0;) {
+            coef[c] = p;
+            p = or_ef_mul(p, ac);
+        }
+    }
+    or_ef *deep = (or_ef *)malloc(n_lde * sizeof(or_ef));
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n_lde; i++) {
+        or_ef negf = or_ef_from(0);
+        size_t off = 0;
+        for (size_t m = 0; m < n_mats_total; m++) {
+            const or_matrix *M = allm[m];
+            unsigned liftm = log_lde - or_log2(M->height);
+            const uint64_t *row = M->data + (i >> liftm) * M->width;
+            for (size_t col = 0; col < M->width; col++) negf = or_ef_add(negf, or_ef_mulf(coef[off + col], row[col]));
+            off += aligned_w[m];
+        }
+        or_ef r = or_ef_mul(q[2 * i], or_ef_add(fred[0], negf));
+        r = or_ef_add(r, or_ef_mul(bp, or_ef_mul(q[2 * i + 1], or_ef_add(fred[1], negf))));
+        deep[i] = r;
+    }
+    free(coef);
+    free(evals);
+    free(q);
+    free(xs);
+    t1 = now_s();
+    g_stage[4] = t1 - t0;
+    t0 = t1;
+
+    /* FRI commit phase (fri/prover.rs:190-323) */
+    const unsigned log_a = pcs->log_folding_arity;
+    const size_t arity = (size_t)1 << log_a;
+    size_t dom = n_lde;
+    unsigned log_max_final = pcs->log_final_degree + log_blowup;
+    size_t rounds = log_lde > log_max_final ? (log_lde - log_max_final + log_a - 1) / log_a : 0;
+    unsigned log_final_size = log_lde - (unsigned)rounds * log_a;
+    size_t final_deg = (size_t)1 << (log_final_size > log_blowup ? log_final_size - log_blowup : 0);
+    size_t final_dom = final_deg << log_blowup;
+    or_tree *fri_trees = (or_tree *)calloc(rounds + 1, sizeof(or_tree));
+    uint64_t **fri_data = (uint64_t **)calloc(rounds + 1, sizeof(uint64_t *));
+    size_t nfri = 0;
+    uint64_t *s_inv = (uint64_t *)malloc((n_lde / arity) * 8);
+    {
+        uint64_t ginv = or_inv(or_root(log_lde)), p = 1;
+        size_t ns = n_lde / arity;
+        uint64_t *tmp = (uint64_t *)malloc(ns * 8);
+        for (size_t k = 0; k < ns; k++) {
+            tmp[k] = p;
+            p = or_mul(p, ginv);
+        }
+        unsigned ls = or_log2(ns);
+        for (size_t k = 0; k < ns; k++) s_inv[k] = tmp[or_bitrev(k, ls)];
+        free(tmp);
+    }
+    or_ef *cur = deep;
+    while (dom > final_dom) {
+        size_t fd = dom / arity;
+        /* flattened (dom/arity) x (2*arity) base matrix, unaligned tree */
+        uint64_t *flat = (uint64_t *)malloc(dom * 2 * 8);
+        for (size_t i = 0; i < dom; i++) {
+            flat[2 * i] = cur[i].c0;
+            flat[2 * i + 1] = cur[i].c1;
+        }
+        or_matrix m = {flat, fd, 2 * arity};
+        or_tree_build(pp, &fri_trees[nfri], &m, 1, 1);
+        fri_data[nfri] = flat;
+        uint64_t root[4];
+        or_tree_root(&fri_trees[nfri], root);
+        or_tr_send_commit(&tr, root);
+        nfri++;
+        or_tr_grind(&tr, pcs->folding_pow_bits);
+        or_ef b = or_ch_sample_ef(&tr.ch);
+        or_ef *nxt = (or_ef *)malloc(fd * sizeof(or_ef));
+#pragma omp parallel for schedule(static)
+        for (size_t k = 0; k < fd; k++) nxt[k] = fold_row(cur + k * arity, log_a, s_inv[k], b);
+        free(cur);
+        cur = nxt;
+        dom = fd;
+        size_t nn = dom / arity;
+        for (size_t k = 0; k < nn; k++) s_inv[k] = or_exp2(s_inv[k * arity], log_a);
+    }
+    free(s_inv);
+    /* final polynomial: truncate, bit-reverse, iDFT, descending order */
+    {
+        unsigned lf = or_log2(final_deg);
+        or_ef *v = (or_ef *)malloc(final_deg * sizeof(or_ef));
+        for (size_t i = 0; i < final_deg; i++) v[i] = cur[or_bitrev(i, lf)];
+        uint64_t *c0 = (uint64_t *)malloc(final_deg * 8), *c1 = (uint64_t *)malloc(final_deg * 8);
+        for (size_t i = 0; i < final_deg; i++) c0[i] = v[i].c0, c1[i] = v[i].c1;
+        or_intt(c0, final_deg);
+        or_intt(c1, final_deg);
+        for (size_t i = final_deg; i-- > 0;) or_tr_send_ef(&tr, or_ef_make(c0[i], c1[i]));
+        free(c0);
+        free(c1);
+        free(v);
+    }
+    free(cur);
+    t1 = now_s();
+    g_stage[5] = t1 - t0;
+    t0 = t1;
+
+    /* query phase (prover.rs:85-115) */
+    or_tr_grind(&tr, pcs->query_pow_bits);
+    size_t *idx = (size_t *)malloc(pcs->num_queries * sizeof(size_t));
+    for (unsigned qi = 0; qi < pcs->num_queries; qi++) idx[qi] = or_bitrev(or_ch_sample_bits(&tr.ch, log_lde), log_lde);
+    qsort(idx, pcs->num_queries, sizeof(size_t), cmp_size);
+    size_t nu = 0;
+    for (size_t i = 0; i < pcs->num_queries; i++)
+        if (nu == 0 || idx[nu - 1] != idx[i]) idx[nu++] = idx[i];
+    for (int g = 0; g < 3; g++) or_tree_prove_batch(&trees[g]->tree, idx, nu, &tr);
+    size_t *ridx = (size_t *)malloc(nu * sizeof(size_t));
+    for (size_t r = 0; r < nfri; r++) {
+        size_t nr = 0;
+        for (size_t i = 0; i < nu; i++) {
+            size_t v = idx[i] >> (log_a * (r + 1));
+            if (nr == 0 || ridx[nr - 1] != v) ridx[nr++] = v;
+        }
+        or_tree_prove_batch(&fri_trees[r], ridx, nr, &tr);
+    }
+    free(ridx);
+    free(idx);
+    for (size_t r = 0; r < nfri; r++) {
+        or_tree_free(&fri_trees[r]);
+        free(fri_data[r]);
+    }
+    free(fri_trees);
+    free(fri_data);
+    committed_free(&mainc);
+    committed_free(&auxc);
+    committed_free(&quotc);
+    or_ch_finalize(&tr.ch, out->digest);
+    out->fields = tr.fields;
+    out->n_fields = tr.n_fields;
+    out->commits = tr.commits;
+    out->n_commits = tr.n_commits;
+    t1 = now_s();
+    g_stage[6] = t1 - t0;
+    return 0;
+}
+void or_proof_free(or_proof *p) {
+    free(p->fields);
+    free(p->commits);
+    p->fields = p->commits = NULL;
+}

@@ -1,0 +1,149 @@
+/*
+ * ORACLE (test infrastructure only) — a CPU restatement, in plain C, of the
+ * lifted-STARK prover path of adr1anh/p3-miden v0.5.0 for the Goldilocks +
+ * Poseidon2 configuration. It is the checker for the CUDA product: only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference leg
+ * may load it. The product library never links or calls it.
+ *
+ * Each function cites the reference file:line it restates. Third-party
+ * pieces (Plonky3 0.5.0 crates, rand 0.10) are restated from their published
+ * algorithms; where a constant could not be obtained (the Poseidon2 internal
+ * diagonal, the exact Keccak AIR constraint order) the oracle is
+ * "parity unpinned" for that piece.
+ */
+#ifndef ORACLE_H
+#define ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+#include "or_field.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ hashing */
+typedef struct { uint64_t s[4]; } or_rng;
+void or_rng_seed(or_rng *r, uint64_t seed);
+uint64_t or_rng_next(or_rng *r);
+uint64_t or_rng_field(or_rng *r);
+
+typedef struct {
+    uint64_t rc_init[4][12];
+    uint64_t rc_term[4][12];
+    uint64_t rc_int[22];
+    uint64_t diag[12];
+} or_p2_params;
+
+void or_p2_params_from_seed(or_p2_params *pp, uint64_t seed, const uint64_t diag[12]);
+void or_p2_permute(const or_p2_params *pp, uint64_t *state12);
+void or_sponge_absorb(const or_p2_params *pp, uint64_t *st, const uint64_t *in, size_t n);
+void or_compress(const or_p2_params *pp, const uint64_t *l, const uint64_t *r, uint64_t *out);
+
+typedef struct {
+    const or_p2_params *pp;
+    uint64_t state[12];
+    uint64_t in[8];
+    uint64_t out[8];
+    int n_in, n_out;
+} or_challenger;
+void or_ch_init(or_challenger *c, const or_p2_params *pp);
+void or_ch_observe(or_challenger *c, uint64_t x);
+uint64_t or_ch_sample(or_challenger *c);
+uint64_t or_ch_sample_bits(or_challenger *c, unsigned bits);
+or_ef or_ch_sample_ef(or_challenger *c);
+uint64_t or_ch_grind(or_challenger *c, unsigned bits);
+void or_ch_finalize(or_challenger *c, uint64_t digest[12]);
+
+typedef struct {
+    or_challenger ch;
+    uint64_t *fields;
+    size_t n_fields, cap_fields;
+    uint64_t *commits; /* 4 words each */
+    size_t n_commits, cap_commits;
+} or_transcript;
+void or_tr_init(or_transcript *t, const or_p2_params *pp);
+void or_tr_send_field(or_transcript *t, uint64_t v);
+void or_tr_send_ef(or_transcript *t, or_ef v);
+void or_tr_send_commit(or_transcript *t, const uint64_t *d);
+void or_tr_hint_field(or_transcript *t, uint64_t v);
+void or_tr_hint_commit(or_transcript *t, const uint64_t *d);
+uint64_t or_tr_grind(or_transcript *t, unsigned bits);
+void or_tr_free(or_transcript *t);
+
+/* ------------------------------------------------------------------ DFT */
+void or_ntt(uint64_t *a, size_t n);  /* natural in, natural out: a_i -> sum_k a_k w_n^{ik} */
+void or_intt(uint64_t *a, size_t n); /* inverse, includes 1/n */
+/* Coset LDE of a row-major h x w matrix to (h<<log_blowup) x w on shift*K,
+ * rows stored bit-reversed (p3-miden-lifted-stark/src/prover/commit.rs:217-222). */
+void or_coset_lde_bitrev(const uint64_t *in, size_t h, size_t w, unsigned log_blowup,
+                         uint64_t shift, uint64_t *out);
+
+/* ----------------------------------------------------------------- LMCS */
+typedef struct {
+    const uint64_t *data; /* row-major */
+    size_t height, width;
+} or_matrix;
+typedef struct {
+    size_t n_mats;
+    or_matrix mats[8];
+    size_t alignment;
+    unsigned depth;       /* log2 of the tree height */
+    uint64_t *layers;     /* all digest layers, leaves first, 4 words each */
+    size_t layer_off[40]; /* offset (in digests) of layer l */
+} or_tree;
+void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment);
+void or_tree_root(const or_tree *t, uint64_t out[4]);
+void or_tree_free(or_tree *t);
+void or_tree_prove_batch(const or_tree *t, const size_t *sorted_unique_idx, size_t n_idx, or_transcript *tr);
+
+/* --------------------------------------------------------------- AIRs */
+enum { OR_AIR_CUBIC = 1, OR_AIR_KECCAK = 2 };
+size_t or_air_num_constraints(int air, size_t width);
+unsigned or_air_log_quotient_degree(int air);
+/* Evaluate all constraints of one row pair, in the AIR's emission order.
+ * sel = {is_first_row, is_last_row, is_transition}. */
+void or_air_eval(int air, size_t width, const uint64_t *consts, const uint64_t *local,
+                 const uint64_t *next, const uint64_t sel[3], uint64_t *out);
+/* Trace generators (the caller side of the reference path). */
+void or_cubic_trace(size_t log_h, size_t width, uint64_t seed, uint64_t *consts_out, uint64_t *trace_out);
+size_t or_keccak_num_cols(void);
+void or_keccak_trace(const uint64_t *inputs25, size_t n_perms, size_t log_h, uint64_t *trace_out);
+void or_keccak_inputs(uint64_t seed, size_t n_perms, uint64_t *out25);
+/* debug check: returns index of first failing (row*K + constraint) + 1, or 0 */
+size_t or_check_constraints(int air, size_t height, size_t width, const uint64_t *consts, const uint64_t *trace);
+
+/* --------------------------------------------------------------- prover */
+typedef struct {
+    unsigned log_blowup, log_folding_arity, log_final_degree;
+    unsigned folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
+} or_pcs_params;
+
+typedef struct {
+    int air;
+    size_t height, width;
+    const uint64_t *trace;  /* row-major height x width */
+    const uint64_t *consts; /* AIR constants (cubic: k[width]) */
+} or_instance;
+
+typedef struct {
+    uint64_t *fields;
+    size_t n_fields;
+    uint64_t *commits;
+    size_t n_commits;
+    uint64_t digest[12];
+    /* intermediate values exposed for stage-by-stage parity tests */
+    uint64_t main_root[4], aux_root[4], quot_root[4];
+    uint64_t alpha[2], beta[2], z[2];
+    uint64_t deep_alpha[2], deep_beta[2];
+} or_proof;
+
+int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
+             or_proof *out);
+void or_proof_free(or_proof *p);
+/* Stage timers of the last or_prove call (seconds), by stage index. */
+double or_last_stage_seconds(int stage);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,152 @@
+// C-ABI entry points for the per-stage seams (device pointers in, device or
+// host results out). Declarations and reference citations: include/p3g.h.
+#pragma once
+#include "context.cuh"
+
+struct p3g_ctx {
+    p3g::Ctx c;
+};
+struct p3g_tree {
+    p3g::Tree t;
+};
+
+#define P3G_API extern "C" __attribute__((visibility("default")))
+
+#define P3G_TRY(ctxp, ...)                                    \
+    try {                                                     \
+        __VA_ARGS__;                                          \
+        return p3g::OK;                                       \
+    } catch (const p3g::CudaError &e) {                       \
+        if (ctxp) (ctxp)->c.last_error = e.what;              \
+        return e.status;                                      \
+    } catch (const std::bad_alloc &) {                        \
+        if (ctxp) (ctxp)->c.last_error = "host allocation failed"; \
+        return p3g::ERR_OOM;                                  \
+    }
+
+P3G_API int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_ctx **out) {
+    if (!out || !poseidon2_params130) return p3g::ERR_INVALID;
+    *out = nullptr;
+    p3g_ctx *x = nullptr;
+    try {
+        x = new p3g_ctx();
+        x->c.device = device;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&x->c.stream, cudaStreamNonBlocking));
+        memcpy(x->c.p2, poseidon2_params130, sizeof(x->c.p2));
+        CK(cudaMemcpyToSymbol(c_p2, x->c.p2, sizeof(x->c.p2)));
+        // keep freed blocks in the pool across proofs
+        cudaMemPool_t pool;
+        CK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = UINT64_MAX;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    } catch (const p3g::CudaError &e) {
+        delete x;
+        return e.status;
+    }
+    *out = x;
+    return p3g::OK;
+}
+
+P3G_API void p3g_ctx_destroy(p3g_ctx *x) {
+    if (!x) return;
+    cudaSetDevice(x->c.device);
+    cudaStreamSynchronize(x->c.stream);
+    x->c.tw.clear();
+    cudaStreamSynchronize(x->c.stream);
+    if (x->c.pinned) cudaFreeHost(x->c.pinned);
+    cudaStreamDestroy(x->c.stream);
+    delete x;
+}
+
+P3G_API const char *p3g_last_error(const p3g_ctx *x) { return x ? x->c.last_error.c_str() : "null context"; }
+
+P3G_API int p3g_coset_lde(p3g_ctx *x, const uint64_t *d_in, uint64_t height, uint64_t width, uint32_t log_blowup,
+                          uint64_t shift, uint64_t *d_out) {
+    if (!x || !d_in || !d_out || height == 0 || (height & (height - 1)) || log_blowup > 8) return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        p3g::DBuf tmp = x->c.alloc(height * width);
+        p3g::coset_lde(x->c, d_in, width, height, width, log_blowup, shift % gl::P, d_out, tmp.p);
+        x->c.sync();
+    })
+}
+
+P3G_API int p3g_lmcs_build(p3g_ctx *x, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
+                           uint64_t n, uint32_t alignment, p3g_tree **out) {
+    if (!x || !d_mats || !heights || !widths || !out || n == 0 || n > 64) return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++) {
+        if (heights[i] == 0 || (heights[i] & (heights[i] - 1))) return p3g::ERR_INVALID;
+        if (i && heights[i] < heights[i - 1]) return p3g::ERR_VALIDATION;
+    }
+    *out = nullptr;
+    p3g_tree *t = new p3g_tree();
+    try {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<p3g::Mat> mats;
+        for (uint64_t i = 0; i < n; i++) mats.push_back({d_mats[i], heights[i], widths[i]});
+        p3g::build_tree(x->c, t->t, mats, alignment);
+        x->c.sync();
+    } catch (const p3g::CudaError &e) {
+        x->c.last_error = e.what;
+        delete t;
+        return e.status;
+    }
+    *out = t;
+    return p3g::OK;
+}
+
+P3G_API int p3g_lmcs_root(const p3g_tree *t, uint64_t *out4) {
+    if (!t || !out4) return p3g::ERR_INVALID;
+    memcpy(out4, t->t.root, 32);
+    return p3g::OK;
+}
+
+P3G_API int p3g_lmcs_layer(p3g_ctx *x, const p3g_tree *t, uint32_t level, uint64_t *host_out) {
+    if (!x || !t || !host_out || level > t->t.depth) return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        uint64_t n = t->t.H >> level;
+        CK(cudaMemcpyAsync(host_out, t->t.layers.p + 4 * t->t.layer_off(level), n * 32, cudaMemcpyDeviceToHost,
+                           x->c.stream));
+        x->c.sync();
+    })
+}
+
+P3G_API void p3g_lmcs_free(p3g_tree *t) { delete t; }
+
+namespace p3g {
+__global__ void permute_batch_kernel(uint64_t *st, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t s[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) s[k] = st[i * 12 + k];
+    p2_permute_dev(s);
+#pragma unroll
+    for (int k = 0; k < 12; k++) st[i * 12 + k] = s[k];
+}
+}  // namespace p3g
+
+P3G_API int p3g_poseidon2_permute_batch(p3g_ctx *x, uint64_t *d_states, uint64_t n) {
+    if (!x || (!d_states && n)) return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        if (n) {
+            p3g::permute_batch_kernel<<<(unsigned)((n + 127) / 128), 128, 0, x->c.stream>>>(d_states, n);
+            CK(cudaGetLastError());
+        }
+        x->c.sync();
+    })
+}
+
+#include "host_rng.cuh"
+
+// Poseidon2Goldilocks<12> constants as the goldilocks_poseidon2 dev config
+// builds them (SmallRng::seed_from_u64(2025)), with the placeholder diagonal.
+P3G_API void p3g_default_poseidon2_params(uint64_t *out130) {
+    uint64_t diag[12];
+    p3g::placeholder_diag(diag);
+    p3g::poseidon2_params_from_seed(2025, diag, out130);
+}
+P3G_API void p3g_poseidon2_params_from_seed(uint64_t seed, const uint64_t *diag12, uint64_t *out130) {
+    p3g::poseidon2_params_from_seed(seed, diag12, out130);
+}

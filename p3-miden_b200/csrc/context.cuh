@@ -1,0 +1,345 @@
+// Device context: stream, stream-ordered allocations, twiddle tables, and
+// the host drivers for the LDE and LMCS tree kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gl.cuh"
+#include "merkle.cuh"
+#include "ntt.cuh"
+#include "poseidon2.cuh"
+
+namespace p3g {
+
+enum Status : int {
+    OK = 0,
+    ERR_INVALID = 1,     // bad argument (null pointer, size, unsupported parameter)
+    ERR_VALIDATION = 2,  // instance validation failed (AIR, height order, width)
+    ERR_OOM = 3,         // device allocation refused
+    ERR_TIMEOUT = 4,     // a bounded device-side search gave up
+    ERR_CUDA = 5,        // other CUDA runtime error
+};
+
+struct CudaError {
+    int status;
+    std::string what;
+};
+
+inline void check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        int st = (e == cudaErrorMemoryAllocation) ? ERR_OOM : ERR_CUDA;
+        throw CudaError{st, std::string(what) + ": " + cudaGetErrorString(e)};
+    }
+}
+#define CK(x) ::p3g::check((x), #x)
+
+inline unsigned log2u(uint64_t n) {
+    unsigned l = 0;
+    while ((1ull << l) < n) l++;
+    return l;
+}
+
+// A device buffer owned by a context, freed stream-ordered.
+struct DBuf {
+    uint64_t *p = nullptr;
+    size_t words = 0;
+    cudaStream_t s = nullptr;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept : p(o.p), words(o.words), s(o.s) { o.p = nullptr; }
+    DBuf &operator=(DBuf &&o) noexcept {
+        release();
+        p = o.p, words = o.words, s = o.s;
+        o.p = nullptr;
+        return *this;
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+    }
+    ~DBuf() { release(); }
+};
+
+struct TwTables {
+    DBuf fwd_lo, fwd_hi, inv_lo, inv_hi;
+    uint32_t lo_bits;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t p2[p2::N_PARAMS];
+    std::map<uint32_t, std::unique_ptr<TwTables>> tw;
+    std::string last_error;
+    uint64_t *pinned = nullptr;  // small pinned staging area
+    size_t pinned_words = 0;
+
+    DBuf alloc(size_t words) {
+        DBuf b;
+        b.s = stream;
+        b.words = words;
+        if (words) CK(cudaMallocAsync((void **)&b.p, words * 8, stream));
+        return b;
+    }
+    uint64_t *stage(size_t words) {
+        if (words > pinned_words) {
+            if (pinned) {
+                CK(cudaStreamSynchronize(stream));
+                cudaFreeHost(pinned);
+            }
+            pinned_words = words < 4096 ? 4096 : words;
+            CK(cudaMallocHost((void **)&pinned, pinned_words * 8));
+        }
+        return pinned;
+    }
+    void h2d(uint64_t *dst, const uint64_t *src, size_t words) {
+        if (words) CK(cudaMemcpyAsync(dst, src, words * 8, cudaMemcpyHostToDevice, stream));
+    }
+    void d2h(uint64_t *dst, const uint64_t *src, size_t words) {
+        if (words) CK(cudaMemcpyAsync(dst, src, words * 8, cudaMemcpyDeviceToHost, stream));
+    }
+    void sync() { CK(cudaStreamSynchronize(stream)); }
+    // upload a small host vector to a fresh device buffer
+    DBuf upload(const std::vector<uint64_t> &v) {
+        DBuf b = alloc(v.size());
+        uint64_t *st = stage(v.size());
+        CK(cudaStreamSynchronize(stream));
+        memcpy(st, v.data(), v.size() * 8);
+        h2d(b.p, st, v.size());
+        CK(cudaStreamSynchronize(stream));
+        return b;
+    }
+
+    // Two-level tables of powers of w_{2^L} and its inverse.
+    const TwTables &twiddles(uint32_t L) {
+        auto it = tw.find(L);
+        if (it != tw.end()) return *it->second;
+        auto t = std::make_unique<TwTables>();
+        uint32_t lo_bits = L < 12 ? L : 12;
+        t->lo_bits = lo_bits;
+        uint64_t w = gl::root(L), wi = gl::inv(w);
+        size_t nlo = 1ull << lo_bits, nhi = 1ull << (L - lo_bits);
+        std::vector<uint64_t> a(nlo), b(nhi), c(nlo), d(nhi);
+        uint64_t x = 1, y = 1;
+        for (size_t i = 0; i < nlo; i++) a[i] = x, c[i] = y, x = gl::mul(x, w), y = gl::mul(y, wi);
+        uint64_t W = x, WI = y;  // w^(2^lo_bits)
+        x = 1, y = 1;
+        for (size_t i = 0; i < nhi; i++) b[i] = x, d[i] = y, x = gl::mul(x, W), y = gl::mul(y, WI);
+        t->fwd_lo = upload(a);
+        t->fwd_hi = upload(b);
+        t->inv_lo = upload(c);
+        t->inv_hi = upload(d);
+        auto &ref = *t;
+        tw[L] = std::move(t);
+        return ref;
+    }
+};
+
+// Host-built two-level power table of v for exponents < 2^L.
+inline void pow_table(uint64_t v, uint32_t L, uint32_t lo_bits, std::vector<uint64_t> &out_lo,
+                      std::vector<uint64_t> &out_hi) {
+    size_t nlo = 1ull << lo_bits, nhi = 1ull << (L > lo_bits ? L - lo_bits : 0);
+    out_lo.resize(nlo);
+    out_hi.resize(nhi);
+    uint64_t x = 1;
+    for (size_t i = 0; i < nlo; i++) out_lo[i] = x, x = gl::mul(x, v);
+    uint64_t y = 1;
+    for (size_t i = 0; i < nhi; i++) out_hi[i] = y, y = gl::mul(y, x);
+}
+
+// split L bits into passes of at most 10 bits, sizes as even as possible
+inline std::vector<uint32_t> pass_sizes(uint32_t L) {
+    uint32_t n = L == 0 ? 1 : (L + 9) / 10;
+    std::vector<uint32_t> v(n, L / n);
+    for (uint32_t i = 0; i < L % n; i++) v[i]++;
+    return v;
+}
+
+template <int C, bool DIF>
+inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
+    uint32_t k = a.bhi - a.blo;
+    dim3 grid((unsigned)(h >> k), (unsigned)((a.w + C - 1) / C));
+    size_t smem = (size_t(1) << k) * C * 8;
+    static bool attr_set = false;
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(ntt::ntt_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1024 * C * 8));
+        attr_set = true;
+    }
+    ntt::ntt_pass_kernel<C, DIF><<<grid, 256, smem, ctx.stream>>>(a);
+    CK(cudaGetLastError());
+}
+template <bool DIF>
+inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
+    if (a.w <= 2) launch_pass<2, DIF>(ctx, a, h);
+    else if (a.w <= 4) launch_pass<4, DIF>(ctx, a, h);
+    else launch_pass<8, DIF>(ctx, a, h);
+}
+
+// Bit-reversed coset LDE: in (h x w, row stride ld_in) -> out ((h<<lb) x w,
+// stride w). tmp must hold h*w words. If col_bases is non-empty, coefficient
+// k of base column col is additionally multiplied by col_bases[col/2]^k.
+inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h, uint64_t w, uint32_t log_blowup,
+                      uint64_t shift, uint64_t *d_out, uint64_t *d_tmp, const std::vector<uint64_t> &col_bases = {}) {
+    if (w == 0) return;
+    const uint32_t L = log2u(h);
+    const uint64_t B = 1ull << log_blowup;
+    const TwTables &tw = ctx.twiddles(L);
+    auto sizes = pass_sizes(L);
+    // inverse transform (DIT, ascending bit ranges)
+    {
+        uint32_t blo = 0;
+        for (size_t pi = 0; pi < sizes.size(); pi++) {
+            ntt::PassArgs a{};
+            a.src = pi == 0 ? d_in : d_tmp;
+            a.ld_src = pi == 0 ? ld_in : w;
+            a.dst = d_tmp;
+            a.ld_dst = w;
+            a.w = w;
+            a.L = L;
+            a.blo = blo;
+            a.bhi = blo + sizes[pi];
+            a.src_bitrev = pi == 0;
+            a.tw = ntt::PowTab{tw.inv_lo.p, tw.inv_hi.p, tw.lo_bits};
+            a.has_scale = 0;
+            launch_pass_any<false>(ctx, a, h);
+            blo = a.bhi;
+        }
+    }
+    DBuf colpow_lo, colpow_hi;
+    if (!col_bases.empty()) {
+        uint32_t lo_bits = L < 10 ? L : 10;
+        size_t nlo = 1ull << lo_bits, nhi = 1ull << (L - lo_bits);
+        std::vector<uint64_t> all_lo, all_hi, lo, hi;
+        for (uint64_t cb : col_bases) {
+            pow_table(cb, L, lo_bits, lo, hi);
+            all_lo.insert(all_lo.end(), lo.begin(), lo.end());
+            all_hi.insert(all_hi.end(), hi.begin(), hi.end());
+        }
+        colpow_lo = ctx.upload(all_lo);
+        colpow_hi = ctx.upload(all_hi);
+        uint64_t n = h * w;
+        ntt::scale_rows_by_colpow_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(
+            d_tmp, h, w, colpow_lo.p, colpow_hi.p, lo_bits, nhi);
+        CK(cudaGetLastError());
+        (void)nlo;
+    }
+    // forward transform per coset (DIF, descending bit ranges)
+    const uint64_t wb = gl::root(L + log_blowup);
+    const uint64_t hinv = gl::inv(h % gl::P);
+    uint32_t lo_bits = L < 12 ? L : 12;
+    std::vector<uint64_t> lo, hi;
+    std::vector<DBuf> keep;
+    uint64_t sk = shift;
+    for (uint64_t k = 0; k < B; k++) {
+        pow_table(sk, L, lo_bits, lo, hi);
+        DBuf dlo = ctx.upload(lo), dhi = ctx.upload(hi);
+        uint64_t *blk = d_out + gl::bitrev(k, log_blowup) * h * w;
+        uint32_t bhi = L;
+        for (size_t pi = 0; pi < sizes.size(); pi++) {
+            ntt::PassArgs a{};
+            a.src = pi == 0 ? d_tmp : blk;
+            a.ld_src = w;
+            a.dst = blk;
+            a.ld_dst = w;
+            a.w = w;
+            a.L = L;
+            a.bhi = bhi;
+            a.blo = bhi - sizes[pi];
+            a.src_bitrev = 0;
+            a.tw = ntt::PowTab{tw.fwd_lo.p, tw.fwd_hi.p, tw.lo_bits};
+            a.has_scale = pi == 0;
+            a.scale = ntt::PowTab{dlo.p, dhi.p, lo_bits};
+            a.scale_const = hinv;
+            launch_pass_any<true>(ctx, a, h);
+            bhi = a.blo;
+        }
+        keep.push_back(std::move(dlo));
+        keep.push_back(std::move(dhi));
+        sk = gl::mul(sk, wb);
+    }
+}
+
+// ------------------------------------------------------------------ trees
+struct Mat {
+    const uint64_t *d;  // device, row-major, stride = width
+    uint64_t h, w;
+};
+struct Tree {
+    DBuf layers;
+    uint32_t depth = 0;
+    uint64_t H = 0;
+    uint32_t alignment = 1;
+    std::vector<Mat> mats;
+    uint64_t root[4] = {0, 0, 0, 0};
+    uint64_t layer_off(uint32_t l) const { return 2 * H - 2 * (H >> l); }
+};
+
+inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t alignment) {
+    t.mats = mats;
+    t.alignment = alignment ? alignment : 1;
+    t.H = mats.back().h;
+    t.depth = log2u(t.H);
+    t.layers = ctx.alloc((2 * t.H - 1) * 4);
+    // height classes in order; at most MAX_MATS matrices per launch
+    struct Launch {
+        std::vector<size_t> idx;
+        uint64_t h;
+    };
+    std::vector<Launch> launches;
+    for (size_t i = 0; i < mats.size(); i++) {
+        if (launches.empty() || launches.back().h != mats[i].h || launches.back().idx.size() == merkle::MAX_MATS)
+            launches.push_back({{}, mats[i].h});
+        launches.back().idx.push_back(i);
+    }
+    uint64_t max_state_h = 0;
+    for (size_t li = 0; li + 1 < launches.size(); li++) max_state_h = std::max(max_state_h, launches[li].h);
+    DBuf st_a, st_b;
+    if (max_state_h) {
+        st_a = ctx.alloc(max_state_h * 12);
+        st_b = ctx.alloc(max_state_h * 12);
+    }
+    const uint64_t *prev = nullptr;
+    uint32_t prev_log = 0;
+    for (size_t li = 0; li < launches.size(); li++) {
+        merkle::ClassArgs a{};
+        a.n_mats = (int)launches[li].idx.size();
+        for (int m = 0; m < a.n_mats; m++) {
+            a.data[m] = mats[launches[li].idx[m]].d;
+            a.width[m] = mats[launches[li].idx[m]].w;
+        }
+        a.log_h = log2u(launches[li].h);
+        a.prev = prev;
+        a.prev_log_h = prev_log;
+        bool last = li + 1 == launches.size();
+        uint64_t *out_states = (li % 2 == 0) ? st_a.p : st_b.p;
+        a.states_out = last ? nullptr : out_states;
+        a.digests_out = last ? t.layers.p : nullptr;
+        uint64_t n = launches[li].h;
+        merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
+        CK(cudaGetLastError());
+        prev = out_states;
+        prev_log = a.log_h;
+    }
+    uint32_t l = 0;
+    while (l < t.depth) {
+        uint64_t n_parents = t.H >> (l + 1);
+        uint32_t blk = (uint32_t)std::min<uint64_t>(256, n_parents);
+        uint32_t levels = std::min<uint32_t>(log2u(blk) + 1, t.depth - l);
+        unsigned grid = (unsigned)(n_parents / blk);
+        merkle::compress_kernel<<<grid, blk, 0, ctx.stream>>>(t.layers.p, t.H, l, levels);
+        CK(cudaGetLastError());
+        l += levels;
+    }
+    ctx.d2h(ctx.stage(4), t.layers.p + 4 * t.layer_off(t.depth), 4);
+    ctx.sync();
+    memcpy(t.root, ctx.pinned, 32);
+}
+
+}  // namespace p3g

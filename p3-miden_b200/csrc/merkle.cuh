@@ -1,0 +1,130 @@
+// Lifted Merkle tree (LMCS) kernels: leaf sponge absorption with virtual
+// lifting, and layer compression.
+//
+// Leaf semantics (p3-miden-lmcs/src/lifted_tree.rs:385-483): leaf j of a tree
+// of height H absorbs, for every matrix m in ascending-height order, row
+// j >> log2(H/h_m) of m, each row in its own absorb call (overwrite mode,
+// rate 8, zero-padded partial chunk; field_sponge.rs:164-182), then squeezes
+// state[0..4]. Matrices are processed one height class at a time: the
+// states of a class of height h are computed from the states of the
+// previous class at index j >> log2(h/h_prev); nothing is upsampled in
+// memory.
+//
+// Digest layers of a tree of height H live in one buffer of 2H-1 digests
+// (4 words each), layer l (H >> l digests) at digest offset 2H - 2(H >> l).
+#pragma once
+#include "gl.cuh"
+#include "poseidon2.cuh"
+
+__constant__ uint64_t c_p2[p2::N_PARAMS];
+
+struct P2Const {
+    __device__ __forceinline__ uint64_t operator[](int i) const { return c_p2[i]; }
+};
+__device__ __forceinline__ void p2_permute_dev(uint64_t *s) { p2::permute(s, P2Const()); }
+
+namespace merkle {
+
+constexpr int MAX_MATS = 8;
+
+struct ClassArgs {
+    const uint64_t *data[MAX_MATS];
+    uint64_t width[MAX_MATS];
+    int n_mats;
+    uint32_t log_h;         // height of this class
+    const uint64_t *prev;   // states of the previous class (12 words each), or null
+    uint32_t prev_log_h;
+    uint64_t *states_out;   // 12 words per leaf, or null when squeezing
+    uint64_t *digests_out;  // 4 words per leaf, or null
+};
+
+__device__ __forceinline__ void absorb_row(uint64_t *s, const uint64_t *row, uint64_t w) {
+    uint64_t i = 0;
+    for (; i + 8 <= w; i += 8) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) s[j] = __ldg(row + i + j);
+        p2_permute_dev(s);
+    }
+    if (i < w) {
+        uint64_t rem = w - i;
+#pragma unroll
+        for (int j = 0; j < 8; j++) s[j] = (uint64_t)j < rem ? __ldg(row + i + j) : 0;
+        p2_permute_dev(s);
+    }
+}
+
+__global__ void __launch_bounds__(128) leaf_class_kernel(const __grid_constant__ ClassArgs a) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >> a.log_h) return;
+    uint64_t s[12];
+    if (a.prev) {
+        const uint64_t *p = a.prev + (j >> (a.log_h - a.prev_log_h)) * 12;
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = p[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = 0;
+    }
+    for (int m = 0; m < a.n_mats; m++) absorb_row(s, a.data[m] + j * a.width[m], a.width[m]);
+    if (a.digests_out) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) a.digests_out[j * 4 + i] = s[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 12; i++) a.states_out[j * 12 + i] = s[i];
+    }
+}
+
+__device__ __forceinline__ void compress2(const uint64_t *l, const uint64_t *r, uint64_t *out) {
+    uint64_t s[12];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        s[i] = l[i];
+        s[4 + i] = r[i];
+        s[8 + i] = 0;
+    }
+    p2_permute_dev(s);
+#pragma unroll
+    for (int i = 0; i < 4; i++) out[i] = s[i];
+}
+
+// One block compresses 2*blockDim.x digests of layer `l_in` through `levels`
+// layers (2^levels <= 2*blockDim.x), writing every produced layer.
+__global__ void __launch_bounds__(256) compress_kernel(uint64_t *layers, uint64_t H, uint32_t l_in, uint32_t levels) {
+    __shared__ uint64_t sm[256 * 4];
+    const uint64_t n_in = H >> l_in;
+    const uint64_t off_in = 2 * H - 2 * (H >> l_in);
+    const uint32_t t = threadIdx.x;
+    const uint64_t parent = (uint64_t)blockIdx.x * blockDim.x + t;  // index in layer l_in+1
+    uint64_t d[4];
+    if (2 * parent + 1 < n_in) {
+        compress2(layers + 4 * (off_in + 2 * parent), layers + 4 * (off_in + 2 * parent + 1), d);
+        uint64_t off1 = 2 * H - 2 * (H >> (l_in + 1));
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            layers[4 * (off1 + parent) + i] = d[i];
+            sm[4 * t + i] = d[i];
+        }
+    }
+    __syncthreads();
+    uint32_t active = blockDim.x;
+    for (uint32_t lv = 1; lv < levels; lv++) {
+        active >>= 1;
+        uint64_t n_l = H >> (l_in + lv + 1);
+        uint64_t pidx = (uint64_t)blockIdx.x * active + t;
+        if (t < active && pidx < n_l) {
+            compress2(sm + 4 * (2 * t), sm + 4 * (2 * t + 1), d);
+            uint64_t off = 2 * H - 2 * (H >> (l_in + lv + 1));
+#pragma unroll
+            for (int i = 0; i < 4; i++) layers[4 * (off + pidx) + i] = d[i];
+        }
+        __syncthreads();
+        if (t < active && pidx < n_l) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) sm[4 * t + i] = d[i];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace merkle

@@ -1,0 +1,120 @@
+// Batched two-adic NTTs over row-major Goldilocks matrices and the
+// bit-reversed coset LDE built from them.
+//
+// A matrix is h x w, row-major, one polynomial per column. A pass loads a
+// group of G = 2^k rows (stride 2^blo) for a tile of C columns into shared
+// memory, runs k radix-2 stages on it and stores it back; a transform of
+// size 2^L is ceil(L/10) passes. Rows are C*8 contiguous bytes per tile, so
+// any row permutation (bit reversal on load) is free at that granularity.
+//
+// Coset LDE of a trace on s*K, |K| = h*B (used for traces, aux traces and
+// quotient chunks):
+//   1. inverse transform, DIT: rows read at bit-reversed positions, output
+//      natural-order coefficients (times h);
+//   2. for each of the B cosets (s*w_{hB}^k)*H of K: scale coefficient i by
+//      (s*w_{hB}^k)^i / h and run a forward DIF transform of size h; DIF
+//      leaves its output in bit-reversed order, which is exactly the
+//      committed layout: coset k occupies rows [bitrev_B(k)*h, +h) of the
+//      bit-reversed LDE.
+#pragma once
+#include "gl.cuh"
+
+namespace ntt {
+
+// Two-level power table: v^e = hi[e >> lo_bits] * lo[e & (2^lo_bits - 1)].
+struct PowTab {
+    const uint64_t *lo;
+    const uint64_t *hi;
+    uint32_t lo_bits;
+    __device__ __forceinline__ uint64_t at(uint64_t e) const {
+        uint64_t a = __ldg(lo + (e & ((1ull << lo_bits) - 1)));
+        uint64_t eh = e >> lo_bits;
+        return eh ? gl::mul(a, __ldg(hi + eh)) : a;
+    }
+};
+
+struct PassArgs {
+    const uint64_t *src;
+    uint64_t *dst;
+    uint64_t ld_src, ld_dst;  // row strides in elements
+    uint64_t w;               // columns
+    uint32_t L;               // log2 of transform size
+    uint32_t blo, bhi;        // bit range handled by this pass
+    uint32_t src_bitrev;      // 1: element p is read from source row bitrev_L(p)
+    PowTab tw;                // powers of the transform root (forward or inverse)
+    uint32_t has_scale;       // multiply loaded element at natural index i by scale_const * scale.at(i)
+    PowTab scale;
+    uint64_t scale_const;
+};
+
+// DIF stages act on bits L-1-t (t ascending => bits descending).
+// DIT stages act on bits t (ascending).
+template <int C, bool DIF>
+__global__ void __launch_bounds__(256) ntt_pass_kernel(const __grid_constant__ PassArgs a) {
+    extern __shared__ uint64_t sm[];
+    const uint32_t k = a.bhi - a.blo;
+    const uint32_t G = 1u << k;
+    const uint64_t S = 1ull << a.blo;
+    const uint64_t g = blockIdx.x;
+    const uint64_t base = (g & (S - 1)) | ((g >> a.blo) << a.bhi);
+    const uint64_t col0 = (uint64_t)blockIdx.y * C;
+    const int tid = threadIdx.x;
+    const int c = tid % C;
+    const int rstep = blockDim.x / C;
+    const bool col_ok = col0 + c < a.w;
+    // load
+    for (uint32_t m = tid / C; m < G; m += rstep) {
+        uint64_t i = base + (uint64_t)m * S;
+        uint64_t row = a.src_bitrev ? gl::bitrev(i, a.L) : i;
+        uint64_t v = col_ok ? __ldg(a.src + row * a.ld_src + col0 + c) : 0;
+        if (a.has_scale) v = gl::mul(v, gl::mul(a.scale_const, a.scale.at(i)));
+        sm[m * C + c] = v;
+    }
+    __syncthreads();
+    const uint64_t base_lo = base & (S - 1);
+    const uint32_t nbf = G / 2;
+    for (uint32_t st = 0; st < k; st++) {
+        // bit position inside the group handled at this step
+        const uint32_t q = DIF ? (k - 1 - st) : st;
+        const uint32_t b = a.blo + q;  // global bit
+        const uint32_t half = 1u << q;
+        for (uint32_t j = tid / C; j < nbf; j += rstep) {
+            uint32_t m = ((j >> q) << (q + 1)) | (j & (half - 1));
+            uint64_t jlow = base_lo + ((uint64_t)(m & (half - 1)) << a.blo);
+            uint64_t u = sm[m * C + c], v = sm[(m + half) * C + c];
+            if (DIF) {
+                // stage t = L-1-b: (u, v) -> (u+v, (u-v) * w^{(i mod 2^b) << t})
+                uint64_t e = jlow << (a.L - 1 - b);
+                sm[m * C + c] = gl::add(u, v);
+                sm[(m + half) * C + c] = gl::mul(gl::sub(u, v), a.tw.at(e));
+            } else {
+                // stage t = b: v *= w^{(i mod 2^b) << (L-1-b)}
+                uint64_t e = jlow << (a.L - 1 - b);
+                uint64_t tv = gl::mul(v, a.tw.at(e));
+                sm[m * C + c] = gl::add(u, tv);
+                sm[(m + half) * C + c] = gl::sub(u, tv);
+            }
+        }
+        __syncthreads();
+    }
+    if (!col_ok) return;
+    for (uint32_t m = tid / C; m < G; m += rstep) {
+        uint64_t i = base + (uint64_t)m * S;
+        a.dst[i * a.ld_dst + col0 + c] = sm[m * C + c];
+    }
+}
+
+// Multiply row k, column col of a row-major matrix by col_base[col/2]^k
+// (quotient chunk de-shifting, quotient.rs:484-497). col_base holds one
+// value per EF column.
+__global__ void scale_rows_by_colpow_kernel(uint64_t *m, uint64_t h, uint64_t w, const uint64_t *col_base_pows_lo,
+                                            const uint64_t *col_base_pows_hi, uint32_t lo_bits, uint64_t hi_len) {
+    uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= h * w) return;
+    uint64_t r = idx / w, col = idx % w, t = col / 2;
+    uint64_t lo = col_base_pows_lo[t * (1ull << lo_bits) + (r & ((1ull << lo_bits) - 1))];
+    uint64_t hi = col_base_pows_hi[t * hi_len + (r >> lo_bits)];
+    m[idx] = gl::mul(m[idx], gl::mul(lo, hi));
+}
+
+}  // namespace ntt

@@ -1,0 +1,264 @@
+"""ctypes binding of the CPU oracle (oracle/build/liboracle.so).
+
+Test infrastructure only: the oracle is the checker for the CUDA product and
+is never part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+LIB_PATH = ORACLE_DIR / "build" / "liboracle.so"
+
+P = 0xFFFFFFFF00000001
+AIR_CUBIC = 1
+AIR_KECCAK = 2
+
+u64p = C.POINTER(C.c_uint64)
+
+
+class PcsParams(C.Structure):
+    _fields_ = [(n, C.c_uint) for n in (
+        "log_blowup", "log_folding_arity", "log_final_degree",
+        "folding_pow_bits", "deep_pow_bits", "num_queries", "query_pow_bits")]
+
+
+class Instance(C.Structure):
+    _fields_ = [("air", C.c_int), ("height", C.c_size_t), ("width", C.c_size_t),
+                ("trace", u64p), ("consts", u64p)]
+
+
+class Proof(C.Structure):
+    _fields_ = [("fields", u64p), ("n_fields", C.c_size_t),
+                ("commits", u64p), ("n_commits", C.c_size_t),
+                ("digest", C.c_uint64 * 12),
+                ("main_root", C.c_uint64 * 4), ("aux_root", C.c_uint64 * 4),
+                ("quot_root", C.c_uint64 * 4),
+                ("alpha", C.c_uint64 * 2), ("beta", C.c_uint64 * 2), ("z", C.c_uint64 * 2),
+                ("deep_alpha", C.c_uint64 * 2), ("deep_beta", C.c_uint64 * 2)]
+
+
+class P2Params(C.Structure):
+    _fields_ = [("rc_init", C.c_uint64 * 48), ("rc_term", C.c_uint64 * 48),
+                ("rc_int", C.c_uint64 * 22), ("diag", C.c_uint64 * 12)]
+
+
+class Matrix(C.Structure):
+    _fields_ = [("data", u64p), ("height", C.c_size_t), ("width", C.c_size_t)]
+
+
+class Tree(C.Structure):
+    _fields_ = [("n_mats", C.c_size_t), ("mats", Matrix * 8), ("alignment", C.c_size_t),
+                ("depth", C.c_uint), ("layers", u64p), ("layer_off", C.c_size_t * 40)]
+
+
+class Challenger(C.Structure):
+    _fields_ = [("pp", C.c_void_p), ("state", C.c_uint64 * 12), ("inp", C.c_uint64 * 8),
+                ("out", C.c_uint64 * 8), ("n_in", C.c_int), ("n_out", C.c_int)]
+
+
+class Transcript(C.Structure):
+    _fields_ = [("ch", Challenger), ("fields", u64p), ("n_fields", C.c_size_t),
+                ("cap_fields", C.c_size_t), ("commits", u64p), ("n_commits", C.c_size_t),
+                ("cap_commits", C.c_size_t)]
+
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        for name, res, args in [
+            ("or_x_mul", C.c_uint64, [C.c_uint64, C.c_uint64]),
+            ("or_x_mul_ref", C.c_uint64, [C.c_uint64, C.c_uint64]),
+            ("or_x_add", C.c_uint64, [C.c_uint64, C.c_uint64]),
+            ("or_x_sub", C.c_uint64, [C.c_uint64, C.c_uint64]),
+            ("or_x_inv", C.c_uint64, [C.c_uint64]),
+            ("or_x_root", C.c_uint64, [C.c_uint]),
+            ("or_x_ef_mul", None, [u64p, u64p, u64p]),
+            ("or_x_ef_inv", None, [u64p, u64p]),
+            ("or_p2_default_params", None, [C.POINTER(P2Params)]),
+            ("or_p2_placeholder_diag", None, [u64p]),
+            ("or_p2_params_from_seed", None, [C.POINTER(P2Params), C.c_uint64, u64p]),
+            ("or_p2_permute", None, [C.POINTER(P2Params), u64p]),
+            ("or_sponge_absorb", None, [C.POINTER(P2Params), u64p, u64p, C.c_size_t]),
+            ("or_compress", None, [C.POINTER(P2Params), u64p, u64p, u64p]),
+            ("or_rng_seed", None, [u64p, C.c_uint64]),
+            ("or_rng_next", C.c_uint64, [u64p]),
+            ("or_rng_field", C.c_uint64, [u64p]),
+            ("or_ntt", None, [u64p, C.c_size_t]),
+            ("or_intt", None, [u64p, C.c_size_t]),
+            ("or_coset_lde_bitrev", None, [u64p, C.c_size_t, C.c_size_t, C.c_uint, C.c_uint64, u64p]),
+            ("or_tree_build", None, [C.POINTER(P2Params), C.POINTER(Tree), C.POINTER(Matrix), C.c_size_t, C.c_size_t]),
+            ("or_tree_root", None, [C.POINTER(Tree), u64p]),
+            ("or_tree_free", None, [C.POINTER(Tree)]),
+            ("or_tree_prove_batch", None, [C.POINTER(Tree), C.POINTER(C.c_size_t), C.c_size_t, C.POINTER(Transcript)]),
+            ("or_tr_init", None, [C.POINTER(Transcript), C.POINTER(P2Params)]),
+            ("or_tr_free", None, [C.POINTER(Transcript)]),
+            ("or_ch_init", None, [C.POINTER(Challenger), C.POINTER(P2Params)]),
+            ("or_ch_observe", None, [C.POINTER(Challenger), C.c_uint64]),
+            ("or_ch_sample", C.c_uint64, [C.POINTER(Challenger)]),
+            ("or_ch_sample_bits", C.c_uint64, [C.POINTER(Challenger), C.c_uint]),
+            ("or_ch_grind", C.c_uint64, [C.POINTER(Challenger), C.c_uint]),
+            ("or_ch_finalize", None, [C.POINTER(Challenger), u64p]),
+            ("or_air_num_constraints", C.c_size_t, [C.c_int, C.c_size_t]),
+            ("or_air_eval", None, [C.c_int, C.c_size_t, u64p, u64p, u64p, u64p, u64p]),
+            ("or_cubic_trace", None, [C.c_size_t, C.c_size_t, C.c_uint64, u64p, u64p]),
+            ("or_keccak_num_cols", C.c_size_t, []),
+            ("or_keccak_trace", None, [u64p, C.c_size_t, C.c_size_t, u64p]),
+            ("or_keccak_inputs", None, [C.c_uint64, C.c_size_t, u64p]),
+            ("or_check_constraints", C.c_size_t, [C.c_int, C.c_size_t, C.c_size_t, u64p, u64p]),
+            ("or_prove", C.c_int, [C.POINTER(P2Params), C.POINTER(PcsParams), C.POINTER(Instance), C.c_size_t, C.POINTER(Proof)]),
+            ("or_proof_free", None, [C.POINTER(Proof)]),
+            ("or_last_stage_seconds", C.c_double, [C.c_int]),
+        ]:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(u64p)
+
+
+def default_p2() -> P2Params:
+    pp = P2Params()
+    lib().or_p2_default_params(C.byref(pp))
+    return pp
+
+
+def p2_to_array(pp: P2Params) -> np.ndarray:
+    """Flatten to the product's layout: rc_init[48], rc_term[48], rc_int[22], diag[12]."""
+    return np.frombuffer(bytes(pp), dtype=np.uint64).copy()
+
+
+def permute(pp: P2Params, st) -> np.ndarray:
+    a = np.array(st, dtype=np.uint64)
+    lib().or_p2_permute(C.byref(pp), ptr(a))
+    return a
+
+
+def coset_lde_bitrev(trace: np.ndarray, log_blowup: int, shift: int) -> np.ndarray:
+    h, w = trace.shape
+    out = np.zeros((h << log_blowup, w), dtype=np.uint64)
+    t = np.ascontiguousarray(trace, dtype=np.uint64)
+    lib().or_coset_lde_bitrev(ptr(t), h, w, log_blowup, shift, ptr(out))
+    return out
+
+
+class OracleTree:
+    """LMCS tree over row-major matrices (ascending heights)."""
+
+    def __init__(self, pp: P2Params, mats, alignment: int):
+        self._keep = [np.ascontiguousarray(m, dtype=np.uint64) for m in mats]
+        arr = (Matrix * len(mats))()
+        for i, m in enumerate(self._keep):
+            arr[i] = Matrix(ptr(m), m.shape[0], m.shape[1])
+        self.t = Tree()
+        self.pp = pp
+        lib().or_tree_build(C.byref(pp), C.byref(self.t), arr, len(mats), alignment)
+
+    def root(self) -> np.ndarray:
+        r = np.zeros(4, dtype=np.uint64)
+        lib().or_tree_root(C.byref(self.t), ptr(r))
+        return r
+
+    def layer(self, l: int) -> np.ndarray:
+        n = 1 << (self.t.depth - l)
+        off = self.t.layer_off[l]
+        buf = np.ctypeslib.as_array(self.t.layers, shape=((2 << self.t.depth) * 4,))
+        return buf[off * 4:(off + n) * 4].reshape(n, 4).copy()
+
+    def prove_batch(self, indices) -> tuple[np.ndarray, np.ndarray]:
+        idx = sorted(set(int(i) for i in indices))
+        arr = (C.c_size_t * max(1, len(idx)))(*idx)
+        tr = Transcript()
+        lib().or_tr_init(C.byref(tr), C.byref(self.pp))
+        lib().or_tree_prove_batch(C.byref(self.t), arr, len(idx), C.byref(tr))
+        f = np.ctypeslib.as_array(tr.fields, shape=(tr.n_fields,)).copy() if tr.n_fields else np.zeros(0, np.uint64)
+        c = (np.ctypeslib.as_array(tr.commits, shape=(tr.n_commits * 4,)).reshape(-1, 4).copy()
+             if tr.n_commits else np.zeros((0, 4), np.uint64))
+        lib().or_tr_free(C.byref(tr))
+        return f, c
+
+    def __del__(self):
+        try:
+            lib().or_tree_free(C.byref(self.t))
+        except Exception:
+            pass
+
+
+def cubic_trace(log_h: int, width: int, seed: int):
+    k = np.zeros(width, dtype=np.uint64)
+    t = np.zeros((1 << log_h, width), dtype=np.uint64)
+    lib().or_cubic_trace(log_h, width, seed, ptr(k), ptr(t))
+    return k, t
+
+
+def keccak_inputs(seed: int, n_perms: int) -> np.ndarray:
+    out = np.zeros((n_perms, 25), dtype=np.uint64)
+    lib().or_keccak_inputs(seed, n_perms, ptr(out))
+    return out
+
+
+def keccak_trace(inputs: np.ndarray, log_h: int) -> np.ndarray:
+    w = lib().or_keccak_num_cols()
+    t = np.zeros((1 << log_h, w), dtype=np.uint64)
+    inp = np.ascontiguousarray(inputs, dtype=np.uint64)
+    lib().or_keccak_trace(ptr(inp), inp.shape[0], log_h, ptr(t))
+    return t
+
+
+def check_constraints(air: int, trace: np.ndarray, consts=None) -> int:
+    h, w = trace.shape
+    c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
+    t = np.ascontiguousarray(trace, dtype=np.uint64)
+    return int(lib().or_check_constraints(air, h, w, ptr(c), ptr(t)))
+
+
+def prove(pp: P2Params, pcs: dict, instances):
+    """instances: list of (air, trace ndarray, consts ndarray|None). Returns a dict."""
+    keep = []
+    arr = (Instance * len(instances))()
+    for i, (air, trace, consts) in enumerate(instances):
+        t = np.ascontiguousarray(trace, dtype=np.uint64)
+        c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
+        keep += [t, c]
+        arr[i] = Instance(air, t.shape[0], t.shape[1], ptr(t), ptr(c))
+    pr = PcsParams(**pcs)
+    proof = Proof()
+    rc = lib().or_prove(C.byref(pp), C.byref(pr), arr, len(instances), C.byref(proof))
+    if rc != 0:
+        raise ValueError(f"oracle prove failed with status {rc}")
+    out = {
+        "fields": np.ctypeslib.as_array(proof.fields, shape=(proof.n_fields,)).copy(),
+        "commits": np.ctypeslib.as_array(proof.commits, shape=(proof.n_commits * 4,)).reshape(-1, 4).copy(),
+        "digest": np.array(proof.digest[:], dtype=np.uint64),
+    }
+    for k in ("main_root", "aux_root", "quot_root", "alpha", "beta", "z", "deep_alpha", "deep_beta"):
+        out[k] = np.array(getattr(proof, k)[:], dtype=np.uint64)
+    out["stage_seconds"] = [lib().or_last_stage_seconds(i) for i in range(7)]
+    lib().or_proof_free(C.byref(proof))
+    return out
+
+
+def set_threads(n: int):
+    os.environ["OMP_NUM_THREADS"] = str(n)

@@ -1,0 +1,64 @@
+"""Stage-by-stage parity of the CUDA kernels against the CPU oracle
+(bit-exact: all arithmetic is exact modular integer arithmetic)."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+P = O.P
+
+
+def rand_mat(rng, h, w):
+    return rng.integers(0, P, size=(h, w), dtype=np.uint64)
+
+
+@pytest.mark.parametrize("log_h,w,log_blowup", [(0, 3, 1), (1, 1, 1), (3, 5, 2), (6, 9, 1), (10, 33, 1),
+                                                (11, 2, 3), (12, 64, 3), (13, 17, 1), (21, 3, 1)])
+def test_coset_lde_matches_oracle(product, gpu_ctx, log_h, w, log_blowup):
+    rng = np.random.default_rng(log_h * 100 + w)
+    t = rand_mat(rng, 1 << log_h, w)
+    shift = int(rng.integers(1, P))
+    want = O.coset_lde_bitrev(t, log_blowup, shift)
+    got = product.to_host(product.coset_lde(gpu_ctx, product.to_device(t), log_blowup, shift))
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
+
+
+def test_poseidon2_params_match_oracle(product):
+    pp = O.default_p2()
+    assert np.array_equal(product.default_poseidon2_params(), O.p2_to_array(pp))
+
+
+def test_poseidon2_permutation_matches_oracle(product, gpu_ctx):
+    pp = O.default_p2()
+    rng = np.random.default_rng(5)
+    st = rng.integers(0, P, size=(300, 12), dtype=np.uint64)
+    st[0] = 0
+    want = np.stack([O.permute(pp, s) for s in st])
+    got = product.to_host(product.poseidon2_permute_batch(gpu_ctx, product.to_device(st)))
+    assert np.array_equal(got, want)
+
+
+SCENARIOS = [
+    [(1, 1)], [(1, 7)], [(2, 3), (4, 5), (8, 8)],
+    [(1, 5), (1, 3), (2, 7), (4, 1), (8, 9)],
+    [(4, 7), (8, 8), (16, 11)], [(8, 13), (16, 25)],
+    [(1, 16), (4, 15), (8, 16), (16, 22)],
+    [(4, 7), (4, 8), (8, 11), (8, 16)], [(16, 7)],
+    [(1024, 3), (4096, 20), (1 << 15, 9)],
+]
+
+
+@pytest.mark.parametrize("scenario", range(len(SCENARIOS)))
+@pytest.mark.parametrize("alignment", [1, 8])
+def test_lmcs_tree_matches_oracle(product, gpu_ctx, scenario, alignment):
+    """Matrix scenarios of p3-miden-dev-utils/src/fixtures.rs:54-81 (rate 8)."""
+    rng = np.random.default_rng(scenario)
+    mats = [rand_mat(rng, h, w) for h, w in SCENARIOS[scenario]]
+    pp = O.default_p2()
+    ot = O.OracleTree(pp, mats, alignment)
+    gt = product.LmcsTree(gpu_ctx, [product.to_device(m) for m in mats], alignment)
+    assert np.array_equal(gt.root(), ot.root())
+    for l in range(gt.depth + 1):
+        assert np.array_equal(gt.layer(l), ot.layer(l))

@@ -1,0 +1,166 @@
+"""CPU checks of the oracle itself: arithmetic, DFT definition, Keccak-f
+against SHA3 (hashlib), constraint vanishing on generated traces, the
+sponge padding rule (field_sponge.rs:196-267) and challenger semantics."""
+import hashlib
+import random
+
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+P = O.P
+L = O.lib()
+
+
+def test_mul_matches_exact_remainder():
+    r = random.Random(1)
+    cases = [(P - 1, P - 1), (0, P - 1), (2**64 - 2**32, 2**32), (1, 1)]
+    cases += [(r.randrange(P), r.randrange(P)) for _ in range(20000)]
+    for a, b in cases:
+        assert L.or_x_mul(a, b) == (a * b) % P
+
+
+def test_extension_field():
+    r = random.Random(2)
+    for _ in range(200):
+        a = [r.randrange(P), r.randrange(P)]
+        b = [r.randrange(P), r.randrange(P)]
+        out = (O.C.c_uint64 * 2)()
+        L.or_x_ef_mul((O.C.c_uint64 * 2)(*a), (O.C.c_uint64 * 2)(*b), out)
+        assert out[0] == (a[0] * b[0] + 7 * a[1] * b[1]) % P
+        assert out[1] == (a[0] * b[1] + a[1] * b[0]) % P
+        inv = (O.C.c_uint64 * 2)()
+        L.or_x_ef_inv((O.C.c_uint64 * 2)(*a), inv)
+        one = (O.C.c_uint64 * 2)()
+        L.or_x_ef_mul((O.C.c_uint64 * 2)(*a), inv, one)
+        assert list(one) == [1, 0]
+
+
+def test_two_adic_roots():
+    assert L.or_x_root(32) == 0x185629DCDA58878C
+    for k in range(1, 33):
+        w = L.or_x_root(k)
+        assert pow(w, 2**k, P) == 1 and pow(w, 2 ** (k - 1), P) == P - 1
+    assert L.or_x_root(2) == 2**48  # w_4 = 2^48
+
+
+def test_ntt_definition_and_inverse():
+    r = random.Random(3)
+    for n in (1, 2, 8, 32):
+        a = np.array([r.randrange(P) for _ in range(n)], dtype=np.uint64)
+        b = a.copy()
+        L.or_ntt(O.ptr(b), n)
+        w = L.or_x_root(n.bit_length() - 1)
+        for i in range(n):
+            assert int(b[i]) == sum(int(a[k]) * pow(w, i * k, P) for k in range(n)) % P
+        L.or_intt(O.ptr(b), n)
+        assert np.array_equal(a, b)
+
+
+def test_coset_lde_is_evaluation_on_coset():
+    r = np.random.default_rng(4)
+    h, w, lb = 8, 3, 2
+    t = r.integers(0, P, size=(h, w), dtype=np.uint64)
+    shift = 7
+    lde = O.coset_lde_bitrev(t, lb, shift)
+    # interpolate column 0 on H, evaluate at shift * w_{hB}^i
+    c = t[:, 0].copy()
+    L.or_intt(O.ptr(c), h)
+    wn = L.or_x_root(5)
+    for i in range(h << lb):
+        x = shift * pow(wn, i, P) % P
+        v = sum(int(c[k]) * pow(x, k, P) for k in range(h)) % P
+        row = int("{:05b}".format(i)[::-1], 2)
+        assert int(lde[row, 0]) == v
+
+
+def test_keccak_rounds_match_sha3():
+    st = np.zeros((1, 25), dtype=np.uint64)
+    st[0, 0] = 0x06
+    st[0, 16] = 0x8000000000000000
+    t = O.keccak_trace(st, 5)
+    row = t[23]
+
+    def lane(x, y):
+        base = 2629 if (x, y) == (0, 0) else 2465 + (y * 5 + x) * 4
+        return sum(int(row[base + l]) << (16 * l) for l in range(4))
+
+    out = b"".join(lane(i % 5, i // 5).to_bytes(8, "little") for i in range(4))
+    assert out == hashlib.sha3_256(b"").digest()
+
+
+def test_keccak_trace_satisfies_constraints():
+    inp = O.keccak_inputs(1, 42)
+    t = O.keccak_trace(inp, 10)
+    assert t.shape == (1024, 2633)
+    assert O.check_constraints(O.AIR_KECCAK, t) == 0
+    assert L.or_air_num_constraints(O.AIR_KECCAK, 2633) == 3182
+    bad = t.copy()
+    bad[5, 300] ^= 1  # flip a c bit
+    assert O.check_constraints(O.AIR_KECCAK, bad) != 0
+
+
+def test_cubic_trace_satisfies_constraints():
+    k, t = O.cubic_trace(7, 16, 11)
+    assert O.check_constraints(O.AIR_CUBIC, t, k) == 0
+    t[3, 2] = (int(t[3, 2]) + 1) % P
+    assert O.check_constraints(O.AIR_CUBIC, t, k) != 0
+
+
+def test_sponge_zero_padding_equivalence():
+    pp = O.default_p2()
+    for n in range(1, 25):
+        x = np.arange(1, n + 1, dtype=np.uint64)
+        pad = np.concatenate([x, np.zeros((-n) % 8, dtype=np.uint64)])
+        s1 = np.zeros(12, dtype=np.uint64)
+        s2 = np.zeros(12, dtype=np.uint64)
+        L.or_sponge_absorb(O.C.byref(pp), O.ptr(s1), O.ptr(x), n)
+        L.or_sponge_absorb(O.C.byref(pp), O.ptr(s2), O.ptr(pad), len(pad))
+        assert np.array_equal(s1, s2)
+    s = np.zeros(12, dtype=np.uint64)
+    L.or_sponge_absorb(O.C.byref(pp), O.ptr(s), O.ptr(np.zeros(1, np.uint64)), 0)
+    assert not s.any()  # empty input is a no-op
+
+
+def test_challenger_sampling_order():
+    pp = O.default_p2()
+    ch = O.Challenger()
+    L.or_ch_init(O.C.byref(ch), O.C.byref(pp))
+    for v in (1, 2, 3):
+        L.or_ch_observe(O.C.byref(ch), v)
+    s = [L.or_ch_sample(O.C.byref(ch)) for _ in range(9)]
+    st = np.zeros(12, dtype=np.uint64)
+    st[:3] = [1, 2, 3]
+    st = O.permute(pp, st)
+    # outputs pop from the end of the rate; a fresh duplex after 8 samples
+    assert s[:8] == [int(st[i]) for i in range(7, -1, -1)]
+    st2 = O.permute(pp, st)
+    assert s[8] == int(st2[7])
+
+
+def test_grind_finds_smallest_witness():
+    pp = O.default_p2()
+    ch = O.Challenger()
+    L.or_ch_init(O.C.byref(ch), O.C.byref(pp))
+    L.or_ch_observe(O.C.byref(ch), 42)
+    bits = 6
+    base = O.Challenger.from_buffer_copy(ch)
+    w = L.or_ch_grind(O.C.byref(ch), bits)
+    for cand in range(w + 1):
+        t = O.Challenger.from_buffer_copy(base)
+        L.or_ch_observe(O.C.byref(t), cand)
+        ok = L.or_ch_sample_bits(O.C.byref(t), bits) == 0
+        assert ok == (cand == w)
+    assert L.or_ch_grind(O.C.byref(O.Challenger.from_buffer_copy(base)), 0) == 0
+
+
+def test_oracle_prove_is_deterministic():
+    pp = O.default_p2()
+    k, t = O.cubic_trace(5, 8, 3)
+    pcs = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bits=2,
+               deep_pow_bits=0, num_queries=4, query_pow_bits=0)
+    a = O.prove(pp, pcs, [(O.AIR_CUBIC, t, k)])
+    b = O.prove(pp, pcs, [(O.AIR_CUBIC, t, k)])
+    assert np.array_equal(a["fields"], b["fields"]) and np.array_equal(a["commits"], b["commits"])
+    assert np.array_equal(a["digest"], b["digest"])
