@@ -249,3 +249,123 @@ def poseidon2_permute_batch(ctx: Context, states_dev):
     torch.cuda.synchronize(ctx.device)
     ctx.check(lib().p3g_poseidon2_permute_batch(ctx.handle, states_dev.data_ptr(), states_dev.shape[0]))
     return states_dev
+
+
+# -------------------------------------------------------------- prover
+@dataclass(frozen=True)
+class PcsParams:
+    """PcsParams::new argument order (p3-miden-lifted-fri/src/params.rs:170-178)."""
+    log_blowup: int
+    log_folding_arity: int
+    log_final_degree: int
+    folding_pow_bits: int
+    deep_pow_bits: int
+    num_queries: int
+    query_pow_bits: int
+
+    def as_c(self) -> PcsParamsC:
+        return PcsParamsC(self.log_blowup, self.log_folding_arity, self.log_final_degree,
+                          self.folding_pow_bits, self.deep_pow_bits, self.num_queries, self.query_pow_bits)
+
+
+@dataclass
+class AirWitness:
+    """One instance: AIR id, row-major trace (numpy host array or torch CUDA
+    tensor of int64 bit patterns) and the AIR's constants (cubic: k[w])."""
+    air: int
+    trace: object
+    consts: np.ndarray | None = None
+
+
+@dataclass
+class TranscriptData:
+    fields: np.ndarray
+    commitments: np.ndarray  # (n, 4)
+
+    def to_bytes(self) -> bytes:
+        """Raw payload: field words then commitment words, little-endian u64."""
+        return self.fields.astype("<u8").tobytes() + self.commitments.astype("<u8").tobytes()
+
+
+@dataclass
+class StarkOutput:
+    digest: np.ndarray
+    proof: TranscriptData
+    stage_ms: list
+    gpu_launches: int
+    h2d_bytes: int
+    d2h_bytes: int
+
+
+STAGES = ("commit main", "commit aux", "constraints", "commit quotient", "DEEP", "FRI commit", "queries")
+
+
+def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> StarkOutput:
+    """prove_multi (p3-miden-lifted-stark/src/prover/mod.rs:223-461) on the GPU.
+
+    Instances must be in ascending height order. The challenger starts from
+    the configuration's fresh DuplexChallenger state."""
+    n = len(instances)
+    arr = (InstanceC * max(1, n))()
+    keep = []
+    for i, w in enumerate(instances):
+        t = w.trace
+        if isinstance(t, np.ndarray):
+            t = np.ascontiguousarray(t, dtype=np.uint64)
+            keep.append(t)
+            ptr, on_dev = t.ctypes.data, 0
+            h, wd = t.shape
+        else:  # torch tensor (host pinned or CUDA)
+            keep.append(t)
+            ptr, on_dev = t.data_ptr(), int(t.is_cuda)
+            h, wd = t.shape
+        c = np.ascontiguousarray(w.consts if w.consts is not None else np.zeros(0), dtype=np.uint64)
+        keep.append(c)
+        arr[i] = InstanceC(w.air, on_dev, h, wd, C.cast(C.c_void_p(ptr), u64p),
+                           c.ctypes.data_as(u64p) if c.size else None, c.size)
+    if any(not isinstance(w.trace, np.ndarray) and w.trace.is_cuda for w in instances):
+        import torch
+        torch.cuda.synchronize(ctx.device)
+    pc = pcs.as_c()
+    out = ProofC()
+    ctx.check(lib().p3g_prove(ctx.handle, C.byref(pc), arr, n, C.byref(out)))
+    try:
+        fields = np.ctypeslib.as_array(out.fields, shape=(out.n_fields,)).copy()
+        commits = np.ctypeslib.as_array(out.commits, shape=(out.n_commits * 4,)).reshape(-1, 4).copy()
+        res = StarkOutput(np.array(out.digest[:], dtype=np.uint64), TranscriptData(fields, commits),
+                          list(out.stage_ms[:len(STAGES)]), int(out.gpu_launches), int(out.h2d_bytes),
+                          int(out.d2h_bytes))
+    finally:
+        lib().p3g_proof_free(C.byref(out))
+    return res
+
+
+def prove_single(ctx: Context, pcs: PcsParams, witness: AirWitness) -> StarkOutput:
+    return prove_multi(ctx, pcs, [witness])
+
+
+# ------------------------------------------------------- trace builders
+def keccak_inputs(seed: int, n_perms: int) -> np.ndarray:
+    out = np.zeros((n_perms, 25), dtype=np.uint64)
+    _check(lib().p3g_keccak_inputs(seed, n_perms, _ptr(out)))
+    return out
+
+
+def generate_keccak_trace(inputs: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """p3-miden-lifted-examples/src/keccak.rs:54-56: next_power_of_two(24 * n) rows."""
+    inputs = np.ascontiguousarray(inputs, dtype=np.uint64).reshape(-1, 25)
+    n = inputs.shape[0]
+    h = max(1, n * KECCAK_ROWS_PER_HASH)
+    log_h = (h - 1).bit_length()
+    if out is None:
+        out = np.empty((1 << log_h, KECCAK_NUM_COLS), dtype=np.uint64)
+    _check(lib().p3g_keccak_trace(_ptr(inputs), n, log_h, out.ctypes.data_as(u64p)))
+    return out
+
+
+def generate_cubic_trace(log_h: int, width: int, seed: int, out: np.ndarray | None = None):
+    k = np.zeros(width, dtype=np.uint64)
+    if out is None:
+        out = np.empty((1 << log_h, width), dtype=np.uint64)
+    _check(lib().p3g_cubic_trace(log_h, width, seed, _ptr(k), out.ctypes.data_as(u64p)))
+    return k, out

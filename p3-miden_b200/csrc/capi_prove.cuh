@@ -1,0 +1,212 @@
+// C-ABI entry points for the whole proof and for the caller-side helpers
+// (trace generation). Declarations and reference citations: include/p3g.h.
+#pragma once
+#include <cstdlib>
+
+#include "capi_stage.cuh"
+#include "prover.cuh"
+#include "traces.cuh"
+
+struct p3g_pcs_params_c {
+    uint32_t log_blowup, log_folding_arity, log_final_degree;
+    uint32_t folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
+};
+struct p3g_instance_c {
+    int32_t air;
+    int32_t trace_on_device;
+    uint64_t height, width;
+    const uint64_t *trace;
+    const uint64_t *consts;
+    uint64_t n_consts;
+};
+struct p3g_proof_c {
+    uint64_t *fields;
+    uint64_t n_fields;
+    uint64_t *commits;
+    uint64_t n_commits;
+    uint64_t digest[12];
+    double stage_ms[12];
+    uint64_t gpu_launches;
+    uint64_t h2d_bytes, d2h_bytes;
+};
+
+namespace p3g {
+// Upload the Keccak round constants and rho offsets used by the constraint kernel.
+inline void upload_keccak_tables() {
+    const keccak::Tables &T = keccak::tables();
+    int rot[25];
+    for (int x = 0; x < 5; x++)
+        for (int y = 0; y < 5; y++) rot[x * 5 + y] = T.rot[x][y];
+    CK(cudaMemcpyToSymbol(quot::c_keccak_rc, T.rc, sizeof(T.rc)));
+    CK(cudaMemcpyToSymbol(quot::c_keccak_rot, rot, sizeof(rot)));
+}
+
+// Validation mirroring prove_multi's checks (prover/mod.rs:238-264,
+// p3-miden-lifted-air/src/instance.rs:93-115) and PcsParams::new
+// (p3-miden-lifted-fri/src/params.rs:170-204).
+inline int validate(const p3g_pcs_params_c *pcs, const p3g_instance_c *inst, uint64_t n) {
+    if (!pcs || !inst || n == 0 || n > 8) return ERR_INVALID;
+    if (pcs->log_folding_arity < 1 || pcs->log_folding_arity > 3) return ERR_INVALID;
+    if (pcs->log_blowup == 0 || pcs->log_blowup > 8) return ERR_INVALID;
+    if (pcs->num_queries == 0) return ERR_INVALID;
+    if (pcs->folding_pow_bits > 30 || pcs->deep_pow_bits > 30 || pcs->query_pow_bits > 30) return ERR_INVALID;
+    uint64_t prev = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const p3g_instance_c &I = inst[i];
+        if (!I.trace) return ERR_INVALID;
+        if (I.height == 0 || (I.height & (I.height - 1))) return ERR_VALIDATION;
+        if (I.height < prev) return ERR_VALIDATION;  // not ascending
+        prev = I.height;
+        if (I.air == AIR_KECCAK) {
+            if (I.width != (uint64_t)keccak::NCOLS) return ERR_VALIDATION;
+        } else if (I.air == AIR_CUBIC) {
+            if (I.width == 0 || !I.consts || I.n_consts != I.width) return ERR_VALIDATION;
+        } else {
+            return ERR_VALIDATION;
+        }
+    }
+    if (prev < 2) return ERR_VALIDATION;  // max trace height must be >= 2
+    uint32_t log_qd = 0;
+    for (uint64_t i = 0; i < n; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
+    if (log_qd > pcs->log_blowup) return ERR_VALIDATION;  // ConstraintDegreeTooHigh
+    if (log2u(prev) + pcs->log_blowup > 32) return ERR_INVALID;  // two-adicity of Goldilocks
+    return OK;
+}
+}  // namespace p3g
+
+P3G_API int p3g_prove(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instance_c *inst, uint64_t n,
+                      p3g_proof_c *out) {
+    if (!x || !out) return p3g::ERR_INVALID;
+    memset(out, 0, sizeof(*out));
+    int v = p3g::validate(pcs, inst, n);
+    if (v != p3g::OK) {
+        x->c.last_error = "instance or parameter validation failed";
+        return v;
+    }
+    try {
+        CK(cudaSetDevice(x->c.device));
+        static bool tables = false;
+        if (!tables) {
+            p3g::upload_keccak_tables();
+            tables = true;
+        }
+        std::vector<p3g::Instance> ins(n);
+        for (uint64_t i = 0; i < n; i++)
+            ins[i] = {inst[i].air, inst[i].trace_on_device, inst[i].height, inst[i].width, inst[i].trace, inst[i].consts,
+                      inst[i].n_consts};
+        p3g::PcsParams pp{pcs->log_blowup,     pcs->log_folding_arity, pcs->log_final_degree, pcs->folding_pow_bits,
+                          pcs->deep_pow_bits,  pcs->num_queries,       pcs->query_pow_bits};
+        p3g::ProofOut po;
+        p3g::prove(x->c, pp, ins.data(), n, po);
+        out->n_fields = po.fields.size();
+        out->n_commits = po.commits.size() / 4;
+        out->fields = (uint64_t *)malloc(std::max<size_t>(1, po.fields.size()) * 8);
+        out->commits = (uint64_t *)malloc(std::max<size_t>(1, po.commits.size()) * 8);
+        if (!out->fields || !out->commits) throw std::bad_alloc();
+        memcpy(out->fields, po.fields.data(), po.fields.size() * 8);
+        memcpy(out->commits, po.commits.data(), po.commits.size() * 8);
+        memcpy(out->digest, po.digest, sizeof(po.digest));
+        for (int s = 0; s < 12; s++) out->stage_ms[s] = po.stage_ms[s];
+        out->gpu_launches = po.launches;
+        out->h2d_bytes = po.h2d;
+        out->d2h_bytes = po.d2h;
+    } catch (const p3g::CudaError &e) {
+        x->c.last_error = e.what;
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        x->c.last_error = "host allocation failed";
+        return p3g::ERR_OOM;
+    }
+    return p3g::OK;
+}
+
+P3G_API void p3g_proof_free(p3g_proof_c *p) {
+    if (!p) return;
+    free(p->fields);
+    free(p->commits);
+    p->fields = p->commits = nullptr;
+    p->n_fields = p->n_commits = 0;
+}
+
+P3G_API int p3g_keccak_inputs(uint64_t seed, uint64_t n_perms, uint64_t *out25) {
+    if (!out25 && n_perms) return p3g::ERR_INVALID;
+    p3g::keccak_inputs(seed, n_perms, out25);
+    return p3g::OK;
+}
+P3G_API int p3g_keccak_trace(const uint64_t *inputs25, uint64_t n_perms, uint32_t log_height, uint64_t *out) {
+    if (!out || (!inputs25 && n_perms) || log_height > 30) return p3g::ERR_INVALID;
+    if (n_perms * 24 > (1ull << log_height)) return p3g::ERR_INVALID;
+    p3g::keccak_trace(inputs25, n_perms, log_height, out);
+    return p3g::OK;
+}
+P3G_API int p3g_cubic_trace(uint32_t log_height, uint64_t width, uint64_t seed, uint64_t *consts_out,
+                            uint64_t *trace_out) {
+    if (!consts_out || !trace_out || width == 0 || log_height > 30) return p3g::ERR_INVALID;
+    p3g::cubic_trace(log_height, width, seed, consts_out, trace_out);
+    return p3g::OK;
+}
+P3G_API uint64_t p3g_air_num_constraints(int32_t air, uint64_t width) { return p3g::air_num_constraints(air, width); }
+
+// Proof-of-work witness search for a challenger state (GrindingChallenger::grind).
+P3G_API int p3g_grind(p3g_ctx *x, const uint64_t *state12, const uint64_t *pending, uint32_t n_pending, uint32_t bits,
+                      uint64_t *witness) {
+    if (!x || !state12 || !witness || n_pending > 7 || (n_pending && !pending) || bits > 30) return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        if (bits == 0) {
+            *witness = 0;
+        } else {
+            ::fri::GrindArgs g{};
+            memcpy(g.state, state12, 96);
+            for (uint32_t i = 0; i < n_pending; i++) g.pending[i] = pending[i];
+            g.n_pending = n_pending;
+            g.bits = bits;
+            p3g::DBuf fb = x->c.alloc(1);
+            uint64_t found = ~0ull;
+            for (uint64_t base = 0; base < (1ull << 36) && found == ~0ull; base += (1ull << 22)) {
+                CK(cudaMemsetAsync(fb.p, 0xff, 8, x->c.stream));
+                g.base = base;
+                g.count = 1ull << 22;
+                g.found = (unsigned long long *)fb.p;
+                ::fri::grind_kernel<<<148 * 8, 128, 0, x->c.stream>>>(g);
+                CK(cudaGetLastError());
+                x->c.d2h(x->c.stage(1), fb.p, 1);
+                x->c.sync();
+                found = x->c.pinned[0];
+            }
+            if (found == ~0ull) throw p3g::CudaError{p3g::ERR_TIMEOUT, "grind: search bound reached"};
+            *witness = found;
+        }
+    })
+}
+
+// LmcsTree::prove_batch hints for sorted unique indices.
+P3G_API int p3g_lmcs_prove_batch(p3g_ctx *x, const p3g_tree *t, const uint64_t *indices, uint64_t n,
+                                 uint64_t *fields_out, uint64_t *n_fields, uint64_t *commits_out, uint64_t *n_commits) {
+    if (!x || !t || !fields_out || !n_fields || !commits_out || !n_commits || (n && !indices)) return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++) {
+        if (indices[i] >= t->t.H) return p3g::ERR_INVALID;
+        if (i && indices[i] <= indices[i - 1]) return p3g::ERR_INVALID;
+    }
+    P3G_TRY(x, {
+        std::vector<uint64_t> idx(indices, indices + n);
+        p3g::OpeningPlan p;
+        p3g::plan_openings(t->t, idx, p);
+        uint64_t nf = 0;
+        for (auto &r : p.rows) nf += r.padded;
+        if (nf > *n_fields || p.sibs.size() > *n_commits) throw p3g::CudaError{p3g::ERR_INVALID, "output buffers too small"};
+        uint64_t of = 0, oc = 0;
+        for (auto &r : p.rows) {
+            CK(cudaMemcpyAsync(fields_out + of, r.src, r.len * 8, cudaMemcpyDeviceToHost, x->c.stream));
+            x->c.sync();
+            for (uint64_t k = r.len; k < r.padded; k++) fields_out[of + k] = 0;
+            of += r.padded;
+        }
+        for (auto *s : p.sibs) {
+            CK(cudaMemcpyAsync(commits_out + 4 * oc, s, 32, cudaMemcpyDeviceToHost, x->c.stream));
+            oc++;
+        }
+        x->c.sync();
+        *n_fields = of;
+        *n_commits = oc;
+    })
+}

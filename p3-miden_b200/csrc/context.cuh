@@ -80,6 +80,7 @@ struct Ctx {
     std::string last_error;
     uint64_t *pinned = nullptr;  // small pinned staging area
     size_t pinned_words = 0;
+    uint64_t launches = 0;       // kernels launched by this context
 
     DBuf alloc(size_t words) {
         DBuf b;
@@ -174,6 +175,7 @@ inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     }
     ntt::ntt_pass_kernel<C, DIF><<<grid, 256, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
+    ctx.launches++;
 }
 template <bool DIF>
 inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
@@ -228,6 +230,7 @@ inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h
         ntt::scale_rows_by_colpow_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(
             d_tmp, h, w, colpow_lo.p, colpow_hi.p, lo_bits, nhi);
         CK(cudaGetLastError());
+        ctx.launches++;
         (void)nlo;
     }
     // forward transform per coset (DIF, descending bit ranges)
@@ -281,6 +284,24 @@ struct Tree {
     uint64_t layer_off(uint32_t l) const { return 2 * H - 2 * (H >> l); }
 };
 
+// Compress layer 0 (already filled) up to the root and fetch the root.
+inline void finish_tree(Ctx &ctx, Tree &t) {
+    uint32_t l = 0;
+    while (l < t.depth) {
+        uint64_t n_parents = t.H >> (l + 1);
+        uint32_t blk = (uint32_t)std::min<uint64_t>(256, n_parents);
+        uint32_t levels = std::min<uint32_t>(log2u(blk) + 1, t.depth - l);
+        unsigned grid = (unsigned)(n_parents / blk);
+        merkle::compress_kernel<<<grid, blk, 0, ctx.stream>>>(t.layers.p, t.H, l, levels);
+        CK(cudaGetLastError());
+        ctx.launches++;
+        l += levels;
+    }
+    ctx.d2h(ctx.stage(4), t.layers.p + 4 * t.layer_off(t.depth), 4);
+    ctx.sync();
+    memcpy(t.root, ctx.pinned, 32);
+}
+
 inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t alignment) {
     t.mats = mats;
     t.alignment = alignment ? alignment : 1;
@@ -324,22 +345,11 @@ inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t
         uint64_t n = launches[li].h;
         merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
         CK(cudaGetLastError());
+        ctx.launches++;
         prev = out_states;
         prev_log = a.log_h;
     }
-    uint32_t l = 0;
-    while (l < t.depth) {
-        uint64_t n_parents = t.H >> (l + 1);
-        uint32_t blk = (uint32_t)std::min<uint64_t>(256, n_parents);
-        uint32_t levels = std::min<uint32_t>(log2u(blk) + 1, t.depth - l);
-        unsigned grid = (unsigned)(n_parents / blk);
-        merkle::compress_kernel<<<grid, blk, 0, ctx.stream>>>(t.layers.p, t.H, l, levels);
-        CK(cudaGetLastError());
-        l += levels;
-    }
-    ctx.d2h(ctx.stage(4), t.layers.p + 4 * t.layer_off(t.depth), 4);
-    ctx.sync();
-    memcpy(t.root, ctx.pinned, 32);
+    finish_tree(ctx, t);
 }
 
 }  // namespace p3g

@@ -1,0 +1,137 @@
+// FRI commit-phase kernels (p3-miden-lifted-fri/src/fri/prover.rs:190-292,
+// fri/fold/arity{2,4,8}.rs) and the proof-of-work grind.
+//
+// Round r commits the evaluations (bit-reversed, n_r EF) as an
+// (n_r/a) x 2a base matrix (EF flattened), one leaf per row, unaligned
+// tree. Folding row k (the coset s*<w_a>, s = w_{n_r}^{bitrev(k)}) with
+// challenge beta gives (1/a) sum_j (beta/s)^j sum_t y_t w_a^{-jt}, where the
+// row holds y_t at position bitrev_{log a}(t).
+//
+// The fold of round r is fused with the leaf hash of round r+1: one thread
+// folds a consecutive rows, stores the a folded values and hashes them as
+// one leaf of the next tree.
+#pragma once
+#include "gl.cuh"
+#include "merkle.cuh"
+#include "ntt.cuh"
+
+namespace fri {
+
+struct FoldArgs {
+    const uint64_t *in;  // n_in EF
+    uint64_t n_out;      // n_in / a
+    uint32_t log_a;
+    uint32_t log_nin;     // log2 n_in
+    uint32_t log_n0;      // log2 of the root of the s_inv table
+    ntt::PowTab w0inv;    // powers of w_{n0}^{-1}
+    gl::ef beta;
+    uint64_t winv_a[8];   // w_a^{-t}, t < a
+    uint64_t inv_a;       // 1/a
+    uint64_t *out;        // n_out EF
+    uint64_t *digests;    // (n_out / a) digests of the next round, or null
+};
+
+__device__ __forceinline__ gl::ef fold_one(const FoldArgs &a, uint64_t k) {
+    const uint32_t A = 1u << a.log_a;
+    // s_inv = w_{n_in}^{-bitrev_{log n_out}(k)} = w_{n0}^{-(bitrev << (log n0 - log n_in))}
+    uint64_t e = gl::bitrev(k, a.log_nin - a.log_a) << (a.log_n0 - a.log_nin);
+    uint64_t s_inv = a.w0inv.at(e);
+    gl::ef x = gl::ef_mulf(a.beta, s_inv);
+    const uint64_t *row = a.in + 2 * k * A;
+    if (A == 2) {
+        gl::ef y0{row[0], row[1]}, y1{row[2], row[3]};
+        gl::ef r = gl::ef_add(gl::ef_add(y0, y1), gl::ef_mul(gl::ef_sub(y0, y1), x));
+        return gl::ef_mulf(r, a.inv_a);
+    }
+    gl::ef y[8];
+    for (uint32_t t = 0; t < A; t++) {
+        uint64_t p = gl::bitrev(t, a.log_a);
+        y[t] = gl::ef{row[2 * p], row[2 * p + 1]};
+    }
+    gl::ef res = gl::ef_zero(), xp = gl::ef_one();
+    for (uint32_t j = 0; j < A; j++) {
+        gl::ef u = gl::ef_zero();
+        for (uint32_t t = 0; t < A; t++) u = gl::ef_add(u, gl::ef_mulf(y[t], a.winv_a[(j * t) & (A - 1)]));
+        res = gl::ef_add(res, gl::ef_mul(u, xp));
+        xp = gl::ef_mul(xp, x);
+    }
+    return gl::ef_mulf(res, a.inv_a);
+}
+
+// thread g folds outputs [g*a, g*a + a)
+__global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ FoldArgs a) {
+    const uint32_t A = 1u << a.log_a;
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g * A >= a.n_out) return;
+    uint64_t buf[16];
+    const uint32_t cnt = (uint32_t)((a.n_out - g * A) < A ? (a.n_out - g * A) : A);
+    for (uint32_t u = 0; u < cnt; u++) {
+        gl::ef v = fold_one(a, g * A + u);
+        a.out[2 * (g * A + u)] = v.c0;
+        a.out[2 * (g * A + u) + 1] = v.c1;
+        buf[2 * u] = v.c0;
+        buf[2 * u + 1] = v.c1;
+    }
+    if (a.digests && cnt == A) {
+        uint64_t s[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = 0;
+        const uint32_t W = 2 * A;
+        for (uint32_t i = 0; i < W; i += 8) {
+#pragma unroll
+            for (uint32_t j = 0; j < 8; j++) s[j] = (i + j < W) ? buf[i + j] : 0;
+            p2_permute_dev(s);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) a.digests[4 * g + i] = s[i];
+    }
+}
+
+// leaves of round 0: leaf k absorbs the 2a words of EF values [k*a, k*a + a)
+__global__ void __launch_bounds__(128) leaf_hash_kernel(const uint64_t *evals, uint64_t n_leaves, uint32_t log_a,
+                                                        uint64_t *digests) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_leaves) return;
+    const uint32_t W = 2u << log_a;
+    const uint64_t *row = evals + k * W;
+    uint64_t s[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = 0;
+    for (uint32_t i = 0; i < W; i += 8) {
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++) s[j] = (i + j < W) ? __ldg(row + i + j) : 0;
+        p2_permute_dev(s);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) digests[4 * k + i] = s[i];
+}
+
+// Proof-of-work search over witnesses [base, base + count): the challenger
+// with `n_pending` buffered inputs observes w and samples; success when the
+// sampled word (state[7] after the duplex) has its low `bits` bits zero.
+struct GrindArgs {
+    uint64_t state[12];
+    uint64_t pending[8];
+    uint32_t n_pending;
+    uint32_t bits;
+    uint64_t base;
+    uint64_t count;
+    unsigned long long *found;  // atomicMin target, initialised to ~0
+};
+__global__ void __launch_bounds__(128) grind_kernel(const __grid_constant__ GrindArgs a) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t mask = (1ull << a.bits) - 1;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.count; t += stride) {
+        uint64_t w = a.base + t;
+        if (w >= *((volatile unsigned long long *)a.found)) return;
+        uint64_t s[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = a.state[i];
+        for (uint32_t i = 0; i < a.n_pending; i++) s[i] = a.pending[i];
+        s[a.n_pending] = w;
+        p2_permute_dev(s);
+        if ((s[7] & mask) == 0) atomicMin(a.found, (unsigned long long)w);
+    }
+}
+
+}  // namespace fri

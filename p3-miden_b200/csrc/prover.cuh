@@ -1,0 +1,590 @@
+// prove_multi on one device: the protocol control flow of
+// p3-miden-lifted-stark/src/prover/mod.rs:223-461 with every O(n) stage on
+// the GPU and the transcript on the host.
+#pragma once
+#include <algorithm>
+#include <chrono>
+#include <set>
+
+#include "context.cuh"
+#include "deep.cuh"
+#include "fri.cuh"
+#include "quotient.cuh"
+#include "transcript.cuh"
+
+namespace p3g {
+
+enum Air : int { AIR_CUBIC = 1, AIR_KECCAK = 2 };
+
+struct PcsParams {
+    uint32_t log_blowup, log_folding_arity, log_final_degree;
+    uint32_t folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
+};
+
+struct Instance {
+    int32_t air;
+    int32_t trace_on_device;
+    uint64_t height, width;
+    const uint64_t *trace;
+    const uint64_t *consts;
+    uint64_t n_consts;
+};
+
+struct ProofOut {
+    std::vector<uint64_t> fields, commits;
+    uint64_t digest[12];
+    double stage_ms[12];
+    uint64_t launches = 0, h2d = 0, d2h = 0;
+};
+
+inline uint64_t air_num_constraints(int air, uint64_t width) {
+    if (air == AIR_CUBIC) return width;
+    if (air == AIR_KECCAK) return 3182;
+    return 0;
+}
+// Both AIRs have maximal constraint degree 3 (is_transition counts 0,
+// is_first_row 1): log2_ceil(3 - 1) = 1 (p3-miden-lifted-air/src/air.rs:267-289).
+inline uint32_t air_log_quotient_degree(int air) {
+    (void)air;
+    return 1;
+}
+
+struct Launcher {
+    Ctx &ctx;
+    uint64_t n = 0;
+    template <typename K, typename... Args>
+    void operator()(K kernel, dim3 grid, dim3 block, size_t smem, Args... args) {
+        kernel<<<grid, block, smem, ctx.stream>>>(args...);
+        CK(cudaGetLastError());
+        n++;
+    }
+};
+
+inline unsigned blocks_for(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Query-phase openings of one tree (p3-miden-lmcs/src/lifted_tree.rs:157-224):
+// rows per unique index per matrix (padded to the alignment), then sibling
+// digests level by level, left to right.
+struct OpeningPlan {
+    struct RowRef {
+        const uint64_t *src;
+        uint64_t len, padded;
+    };
+    std::vector<RowRef> rows;
+    std::vector<const uint64_t *> sibs;
+};
+inline void plan_openings(const Tree &t, const std::vector<uint64_t> &idx, OpeningPlan &p) {
+    for (uint64_t i : idx)
+        for (const Mat &m : t.mats) {
+            uint32_t lift = t.depth - log2u(m.h);
+            uint64_t r = i >> lift;
+            uint64_t pad = (m.w + t.alignment - 1) / t.alignment * t.alignment;
+            p.rows.push_back({m.d + r * m.w, m.w, pad});
+        }
+    std::vector<uint64_t> known = idx;
+    for (uint32_t l = 0; l < t.depth; l++) {
+        std::vector<uint64_t> parents;
+        for (size_t i = 0; i < known.size(); i++) {
+            uint64_t pos = known[i], par = pos >> 1;
+            if (!parents.empty() && parents.back() == par) continue;
+            bool has_l, has_r;
+            if ((pos & 1) == 0) {
+                has_l = true;
+                has_r = i + 1 < known.size() && known[i + 1] == pos + 1;
+            } else {
+                has_l = false;
+                has_r = true;
+            }
+            const uint64_t *layer = t.layers.p + 4 * t.layer_off(l);
+            if (has_l && !has_r) p.sibs.push_back(layer + 4 * (2 * par + 1));
+            if (!has_l && has_r) p.sibs.push_back(layer + 4 * (2 * par));
+            parents.push_back(par);
+        }
+        known.swap(parents);
+    }
+}
+
+struct Seg {
+    const uint64_t *src;
+    uint64_t len;
+    uint64_t dst;
+};
+__global__ void gather_kernel(const Seg *segs, uint64_t n, uint64_t *out) {
+    for (uint64_t s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = segs[s];
+        for (uint64_t i = threadIdx.x; i < g.len; i += blockDim.x) out[g.dst + i] = g.src[i];
+    }
+}
+
+// Upload (or alias) a trace, returning a device pointer.
+inline const uint64_t *trace_on_device(Ctx &ctx, const Instance &in, DBuf &hold, ProofOut &po) {
+    if (in.trace_on_device) return in.trace;
+    size_t words = in.height * in.width;
+    hold = ctx.alloc(words);
+    CK(cudaMemcpyAsync(hold.p, in.trace, words * 8, cudaMemcpyHostToDevice, ctx.stream));
+    po.h2d += words * 8;
+    return hold.p;
+}
+
+inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, ProofOut &po) {
+    using clk = std::chrono::steady_clock;
+    Launcher L{ctx};
+    const uint32_t lb = pcs.log_blowup;
+    const uint64_t B = 1ull << lb;
+    const uint32_t log_max_h = log2u(inst[n_inst - 1].height);
+    uint32_t log_qd = 0;
+    for (size_t i = 0; i < n_inst; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
+    const uint64_t D = 1ull << log_qd;
+    const uint32_t log_lde = log_max_h + lb;
+    const uint64_t n = 1ull << log_lde;
+    Transcript tr(ctx.p2);
+
+    cudaEvent_t ev[9];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ev[0], ctx.stream));
+
+    // ---- 1. main traces: coset LDE on g^(2^lift) K, bit-reversed; aligned tree
+    uint64_t max_hw = 0;
+    for (size_t i = 0; i < n_inst; i++) max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, 2));
+    max_hw = std::max(max_hw, inst[n_inst - 1].height * 2 * D);
+    DBuf tmp = ctx.alloc(max_hw);
+    std::vector<DBuf> main_lde(n_inst), aux_lde(n_inst);
+    std::vector<Mat> main_mats, aux_mats;
+    const uint64_t launches_before = ctx.launches;
+    for (size_t i = 0; i < n_inst; i++) {
+        DBuf hold;
+        const uint64_t *dt = trace_on_device(ctx, inst[i], hold, po);
+        uint64_t h = inst[i].height, w = inst[i].width;
+        main_lde[i] = ctx.alloc((h << lb) * w);
+        uint64_t shift = gl::exp2k(gl::GEN, log_max_h - log2u(h));
+        coset_lde(ctx, dt, w, h, w, lb, shift, main_lde[i].p, tmp.p);
+        main_mats.push_back({main_lde[i].p, h << lb, w});
+    }
+    Tree main_tree;
+    build_tree(ctx, main_tree, main_mats, 8);
+    tr.send_commit(main_tree.root);
+    CK(cudaEventRecord(ev[1], ctx.stream));
+
+    // ---- 2. randomness (max num_randomness over the AIRs = 1) and the
+    // 1-column zero aux traces flattened to 2 base columns
+    (void)tr.ch.sample_ef();
+    for (size_t i = 0; i < n_inst; i++) {
+        uint64_t h = inst[i].height;
+        DBuf z = ctx.alloc(h * 2);
+        CK(cudaMemsetAsync(z.p, 0, h * 16, ctx.stream));
+        aux_lde[i] = ctx.alloc((h << lb) * 2);
+        uint64_t shift = gl::exp2k(gl::GEN, log_max_h - log2u(h));
+        coset_lde(ctx, z.p, 2, h, 2, lb, shift, aux_lde[i].p, tmp.p);
+        aux_mats.push_back({aux_lde[i].p, h << lb, 2});
+    }
+    Tree aux_tree;
+    build_tree(ctx, aux_tree, aux_mats, 8);
+    tr.send_commit(aux_tree.root);
+    CK(cudaEventRecord(ev[2], ctx.stream));
+
+    // ---- 4./5. alpha, beta; constraints with cyclic extension
+    const gl::ef alpha = tr.ch.sample_ef();
+    const gl::ef beta = tr.ch.sample_ef();
+    const uint64_t max_qh = inst[n_inst - 1].height * D;
+    DBuf acc = ctx.alloc(2 * max_qh);
+    uint64_t acc_len = 0;
+    for (size_t ii = 0; ii < n_inst; ii++) {
+        const Instance &I = inst[ii];
+        const uint32_t log_h = log2u(I.height);
+        const uint64_t qh = I.height * D;
+        const uint32_t log_qh = log_h + log_qd;
+        if (acc_len == 0) {
+            CK(cudaMemsetAsync(acc.p, 0, qh * 16, ctx.stream));
+        } else {
+            L(quot::scale_ef_kernel, blocks_for(acc_len, 256), 256, 0, acc.p, acc_len, beta);
+            if (qh > acc_len) L(quot::tile_ef_kernel, blocks_for(qh - acc_len, 256), 256, 0, acc.p, acc_len, qh);
+        }
+        acc_len = qh;
+        const uint64_t K = air_num_constraints(I.air, I.width);
+        std::vector<uint64_t> ap(2 * K);
+        gl::ef p = gl::ef_one();
+        for (uint64_t k = K; k-- > 0;) {
+            ap[2 * k] = p.c0, ap[2 * k + 1] = p.c1;
+            p = gl::ef_mul(p, alpha);
+        }
+        DBuf d_ap = ctx.upload(ap);
+        DBuf d_consts;
+        if (I.air == AIR_CUBIC) d_consts = ctx.upload(std::vector<uint64_t>(I.consts, I.consts + I.width));
+        const TwTables &twq = ctx.twiddles(log_qh);
+        quot::EvalArgs a{};
+        a.lde = main_lde[ii].p;
+        a.w = I.width;
+        a.log_qh = log_qh;
+        a.log_h = log_h;
+        a.D = D;
+        a.shift = gl::exp2k(gl::GEN, log_max_h - log_h);
+        a.wq = ntt::PowTab{twq.fwd_lo.p, twq.fwd_hi.p, twq.lo_bits};
+        a.omega_h_inv = gl::inv(gl::root(log_h));
+        {
+            uint64_t s_pow_n = gl::exp2k(a.shift, log_h), wd = gl::root(log_qd), x = 1;
+            for (uint64_t t = 0; t < D; t++) a.zh[t] = gl::sub(gl::mul(s_pow_n, x), 1), x = gl::mul(x, wd);
+        }
+        a.alpha_pows = d_ap.p;
+        a.consts = d_consts.p;
+        a.acc = acc.p;
+        if (I.air == AIR_CUBIC) L(quot::cubic_eval_kernel, blocks_for(qh * 32, 256), 256, 0, a);
+        else L(quot::keccak_eval_kernel, blocks_for(qh, 128), 128, 0, a);
+        ctx.sync();  // keep d_ap / d_consts alive until the kernel ran
+    }
+    // ---- 6. divide by Z_H on the max quotient coset
+    {
+        quot::VanArgs v{};
+        v.D = D;
+        uint64_t s_pow_n = gl::exp2k(gl::GEN, log_max_h), wd = gl::root(log_qd), x = 1;
+        for (uint64_t t = 0; t < D; t++) v.inv_van[t] = gl::inv(gl::sub(gl::mul(s_pow_n, x), 1)), x = gl::mul(x, wd);
+        L(quot::divide_vanishing_kernel, blocks_for(max_qh, 256), 256, 0, acc.p, max_qh, v);
+    }
+    CK(cudaEventRecord(ev[3], ctx.stream));
+
+    // ---- 7. quotient chunks: N x D EF -> (N*B) x 2D base on gK
+    const uint64_t N = inst[n_inst - 1].height;
+    DBuf quot_lde = ctx.alloc((N << lb) * 2 * D);
+    {
+        std::vector<uint64_t> col_bases(D);
+        uint64_t wji = gl::inv(gl::root(log_max_h + log_qd)), x = 1;
+        for (uint64_t t = 0; t < D; t++) col_bases[t] = x, x = gl::mul(x, wji);
+        coset_lde(ctx, acc.p, 2 * D, N, 2 * D, lb, 1, quot_lde.p, tmp.p, col_bases);
+    }
+    acc.release();
+    Tree quot_tree;
+    build_tree(ctx, quot_tree, {{quot_lde.p, N << lb, 2 * D}}, 8);
+    tr.send_commit(quot_tree.root);
+    CK(cudaEventRecord(ev[4], ctx.stream));
+
+    // ---- 8. OOD point outside H and gK (coset.rs:329-342)
+    gl::ef z;
+    const uint64_t ginv = gl::inv(gl::GEN);
+    for (;;) {
+        z = tr.ch.sample_ef();
+        bool in_h = gl::ef_eq(gl::ef_exp2k(z, log_max_h), gl::ef_one());
+        bool in_gk = gl::ef_eq(gl::ef_exp2k(gl::ef_mulf(z, ginv), log_lde), gl::ef_one());
+        if (!in_h && !in_gk) break;
+    }
+    const gl::ef zs[2] = {z, gl::ef_mulf(z, gl::root(log_max_h))};
+
+    // ---- 9. DEEP
+    std::vector<const Mat *> all;
+    for (auto &m : main_tree.mats) all.push_back(&m);
+    for (auto &m : aux_tree.mats) all.push_back(&m);
+    for (auto &m : quot_tree.mats) all.push_back(&m);
+    const TwTables &twn = ctx.twiddles(log_lde);
+    DBuf q = ctx.alloc(4 * n);
+    {
+        deep::PQArgs a{};
+        a.n = n;
+        a.log_n = log_lde;
+        a.wn = ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits};
+        a.z[0] = zs[0];
+        a.z[1] = zs[1];
+        a.q = q.p;
+        L(deep::point_quotients_kernel, blocks_for((n + deep::CHUNK - 1) / deep::CHUNK, 128), 128, 0, a);
+    }
+    const uint64_t d = n >> lb;
+    const uint32_t log_d = log2u(d);
+    std::map<uint64_t, DBuf> weights;
+    weights[d] = ctx.alloc(4 * d);
+    L(deep::top_weights_kernel, blocks_for(d, 256), 256, 0, q.p, d, log_lde,
+      ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits}, weights[d].p);
+    for (const Mat *m : all) {
+        uint64_t dm = m->h >> lb;
+        if (weights.count(dm)) continue;
+        weights[dm] = ctx.alloc(4 * dm);
+        L(deep::fold_weights_kernel, blocks_for(dm, 256), 256, 0, weights[d].p, dm, d / dm, weights[dm].p);
+    }
+    gl::ef sj[2];
+    for (int j = 0; j < 2; j++) {
+        gl::ef t = gl::ef_sub(gl::ef_exp2k(gl::ef_mulf(zs[j], ginv), log_d), gl::ef_one());
+        sj[j] = gl::ef_mulf(t, gl::inv(d % gl::P));
+    }
+    std::vector<uint64_t> aligned_w;
+    uint64_t total_aligned = 0, total_w = 0;
+    for (const Mat *m : all) {
+        aligned_w.push_back((m->w + 7) / 8 * 8);
+        total_aligned += aligned_w.back();
+        total_w += m->w;
+    }
+    DBuf evals = ctx.alloc(4 * total_w);
+    {
+        uint64_t off = 0;
+        for (const Mat *m : all) {
+            uint64_t dm = m->h >> lb;
+            uint64_t col_tiles = (m->w + 31) / 32;
+            uint64_t target_blocks = 4 * 148;
+            uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, (target_blocks + col_tiles - 1) / col_tiles));
+            uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
+            n_chunks = (dm + rpc - 1) / rpc;
+            DBuf part = ctx.alloc(n_chunks * m->w * 4);
+            L(deep::colsum_kernel, dim3((unsigned)n_chunks, (unsigned)col_tiles), 256, 0, m->d, m->w, dm,
+              weights[dm].p, rpc, part.p);
+            L(deep::colsum_finish_kernel, blocks_for(m->w, 128), 128, 0, part.p, n_chunks, m->w, sj[0], sj[1],
+              evals.p + 4 * off);
+            off += m->w;
+        }
+    }
+    std::vector<uint64_t> h_evals(4 * total_w);
+    ctx.d2h(h_evals.data(), evals.p, 4 * total_w);
+    ctx.sync();
+    po.d2h += 32 * total_w;
+    // send aligned evals per point (deep/prover.rs:271-277)
+    for (int j = 0; j < 2; j++) {
+        uint64_t off = 0;
+        for (size_t mi = 0; mi < all.size(); mi++) {
+            for (uint64_t c = 0; c < aligned_w[mi]; c++) {
+                if (c < all[mi]->w) tr.send_ef(gl::ef{h_evals[4 * (off + c) + 2 * j], h_evals[4 * (off + c) + 2 * j + 1]});
+                else tr.send_ef(gl::ef_zero());
+            }
+            off += all[mi]->w;
+        }
+    }
+    // grind(deep_pow_bits), then alpha (columns) and beta (points)
+    auto grind = [&](uint32_t bits) {
+        if (bits == 0) {
+            tr.fields.push_back(0);
+            return;
+        }
+        fri::GrindArgs g{};
+        memcpy(g.state, tr.ch.state, sizeof(g.state));
+        for (int i = 0; i < tr.ch.n_in; i++) g.pending[i] = tr.ch.in[i];
+        g.n_pending = tr.ch.n_in;
+        g.bits = bits;
+        DBuf fb = ctx.alloc(1);
+        uint64_t found = ~0ull;
+        const uint64_t batch = 1ull << 22;
+        for (uint64_t base = 0; base < (1ull << 36); base += batch) {
+            CK(cudaMemsetAsync(fb.p, 0xff, 8, ctx.stream));
+            g.base = base;
+            g.count = batch;
+            g.found = (unsigned long long *)fb.p;
+            L(fri::grind_kernel, 148 * 8, 128, 0, g);
+            ctx.d2h(ctx.stage(1), fb.p, 1);
+            ctx.sync();
+            found = ctx.pinned[0];
+            if (found != ~0ull) break;
+        }
+        if (found == ~0ull) throw CudaError{ERR_TIMEOUT, "grind: no witness found within the search bound"};
+        if (!tr.ch.check_witness(bits, found)) throw CudaError{ERR_CUDA, "grind: device witness rejected by host"};
+        tr.ch.observe(found);
+        (void)tr.ch.sample_bits(bits);
+        tr.fields.push_back(found);
+    };
+    grind(pcs.deep_pow_bits);
+    const gl::ef ac = tr.ch.sample_ef();
+    const gl::ef bp = tr.ch.sample_ef();
+    gl::ef fred[2] = {gl::ef_zero(), gl::ef_zero()};
+    {
+        uint64_t off = 0;
+        for (size_t mi = 0; mi < all.size(); mi++) {
+            for (uint64_t c = 0; c < aligned_w[mi]; c++)
+                for (int j = 0; j < 2; j++) {
+                    gl::ef v = c < all[mi]->w ? gl::ef{h_evals[4 * (off + c) + 2 * j], h_evals[4 * (off + c) + 2 * j + 1]}
+                                              : gl::ef_zero();
+                    fred[j] = gl::ef_add(gl::ef_mul(fred[j], ac), v);
+                }
+            off += all[mi]->w;
+        }
+    }
+    // coefficients -alpha^{W-1-c} over the aligned flat columns
+    std::vector<uint64_t> coef(2 * total_aligned);
+    {
+        gl::ef p = gl::ef{gl::P - 1, 0};
+        for (uint64_t c = total_aligned; c-- > 0;) {
+            coef[2 * c] = p.c0, coef[2 * c + 1] = p.c1;
+            p = gl::ef_mul(p, ac);
+        }
+    }
+    DBuf d_coef = ctx.upload(coef);
+    std::vector<DBuf> dots(all.size());
+    deep::AssembleArgs aa{};
+    {
+        uint64_t off = 0;
+        for (size_t mi = 0; mi < all.size(); mi++) {
+            const Mat *m = all[mi];
+            dots[mi] = ctx.alloc(2 * m->h);
+            const uint64_t *cf = d_coef.p + 2 * off;
+            if (m->w >= 16) {
+                size_t smem = 16 * m->w;
+                static bool attr = false;
+                if (!attr) {
+                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+                    attr = true;
+                }
+                unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(m->h * 32, 256), 148 * 16);
+                L(deep::rowdot_warp_kernel, grid, 256, smem, m->d, m->h, m->w, cf, dots[mi].p);
+            } else {
+                L(deep::rowdot_thread_kernel, blocks_for(m->h, 256), 256, 0, m->d, m->h, m->w, cf, dots[mi].p);
+            }
+            aa.dots[mi] = dots[mi].p;
+            aa.lift[mi] = log_lde - log2u(m->h);
+            off += aligned_w[mi];
+        }
+    }
+    aa.n_dots = (int)all.size();
+    aa.q = q.p;
+    aa.n = n;
+    aa.fred[0] = fred[0];
+    aa.fred[1] = fred[1];
+    aa.beta = bp;
+    DBuf layer = ctx.alloc(2 * n);
+    aa.out = layer.p;
+    L(deep::assemble_kernel, blocks_for(n, 256), 256, 0, aa);
+    q.release();
+    weights.clear();
+    dots.clear();
+    CK(cudaEventRecord(ev[5], ctx.stream));
+
+    // ---- FRI commit phase
+    const uint32_t log_a = pcs.log_folding_arity;
+    const uint64_t arity = 1ull << log_a;
+    const uint32_t log_max_final = pcs.log_final_degree + lb;
+    const uint64_t rounds = log_lde > log_max_final ? (log_lde - log_max_final + log_a - 1) / log_a : 0;
+    const uint32_t log_final_size = log_lde - (uint32_t)rounds * log_a;
+    const uint64_t final_deg = 1ull << (log_final_size > lb ? log_final_size - lb : 0);
+    const uint64_t final_dom = final_deg << lb;
+    const TwTables &tw0 = ctx.twiddles(log_lde);
+    std::vector<DBuf> fri_layers;
+    std::vector<std::unique_ptr<Tree>> fri_trees;
+    uint64_t dom = n;
+    fri_layers.push_back(std::move(layer));
+    std::unique_ptr<Tree> next_tree;
+    {
+        auto t = std::make_unique<Tree>();
+        if (dom > final_dom) {
+            build_tree(ctx, *t, {{fri_layers[0].p, dom / arity, 2 * arity}}, 1);
+            next_tree = std::move(t);
+        }
+    }
+    uint64_t winv_a[8];
+    {
+        uint64_t wi = gl::inv(gl::root(log_a)), x = 1;
+        for (uint64_t t = 0; t < 8; t++) winv_a[t] = x, x = gl::mul(x, wi);
+    }
+    while (dom > final_dom) {
+        Tree &cur = *next_tree;
+        tr.send_commit(cur.root);
+        fri_trees.push_back(std::move(next_tree));
+        grind(pcs.folding_pow_bits);
+        const gl::ef fb = tr.ch.sample_ef();
+        const uint64_t nout = dom / arity;
+        DBuf out = ctx.alloc(2 * nout);
+        fri::FoldArgs fa{};
+        fa.in = fri_layers.back().p;
+        fa.n_out = nout;
+        fa.log_a = log_a;
+        fa.log_nin = log2u(dom);
+        fa.log_n0 = log_lde;
+        fa.w0inv = ntt::PowTab{tw0.inv_lo.p, tw0.inv_hi.p, tw0.lo_bits};
+        fa.beta = fb;
+        memcpy(fa.winv_a, winv_a, sizeof(winv_a));
+        fa.inv_a = gl::inv(arity);
+        fa.out = out.p;
+        bool more = nout > final_dom;
+        std::unique_ptr<Tree> nt;
+        if (more) {
+            nt = std::make_unique<Tree>();
+            nt->mats = {{out.p, nout / arity, 2 * arity}};
+            nt->alignment = 1;
+            nt->H = nout / arity;
+            nt->depth = log2u(nt->H);
+            nt->layers = ctx.alloc((2 * nt->H - 1) * 4);
+            fa.digests = nt->layers.p;
+        }
+        L(fri::fold_hash_kernel, blocks_for((nout + arity - 1) / arity, 128), 128, 0, fa);
+        if (more) {
+            finish_tree(ctx, *nt);
+            next_tree = std::move(nt);
+        }
+        fri_layers.push_back(std::move(out));
+        dom = nout;
+    }
+    // final polynomial: first final_deg values, bit-reversed, iDFT, descending order
+    {
+        std::vector<uint64_t> last(2 * dom);
+        ctx.d2h(last.data(), fri_layers.back().p, 2 * dom);
+        ctx.sync();
+        po.d2h += 16 * dom;
+        uint32_t lf = log2u(final_deg);
+        std::vector<gl::ef> v(final_deg), c(final_deg);
+        for (uint64_t i = 0; i < final_deg; i++) {
+            uint64_t s = gl::bitrev(i, lf);
+            v[i] = gl::ef{last[2 * s], last[2 * s + 1]};
+        }
+        uint64_t winv = gl::inv(gl::root(lf)), finv = gl::inv(final_deg % gl::P);
+        for (uint64_t k = 0; k < final_deg; k++) {
+            gl::ef s = gl::ef_zero();
+            for (uint64_t i = 0; i < final_deg; i++) s = gl::ef_add(s, gl::ef_mulf(v[i], gl::pow(winv, (i * k) % final_deg)));
+            c[k] = gl::ef_mulf(s, finv);
+        }
+        for (uint64_t k = final_deg; k-- > 0;) tr.send_ef(c[k]);
+    }
+    CK(cudaEventRecord(ev[6], ctx.stream));
+
+    // ---- query phase
+    grind(pcs.query_pow_bits);
+    std::set<uint64_t> idxset;
+    for (uint32_t qi = 0; qi < pcs.num_queries; qi++) idxset.insert(gl::bitrev(tr.ch.sample_bits(log_lde), log_lde));
+    std::vector<uint64_t> idx(idxset.begin(), idxset.end());
+    std::vector<OpeningPlan> plans;
+    std::vector<const Tree *> order = {&main_tree, &aux_tree, &quot_tree};
+    for (auto *t : order) {
+        plans.emplace_back();
+        plan_openings(*t, idx, plans.back());
+    }
+    for (size_t r = 0; r < fri_trees.size(); r++) {
+        std::set<uint64_t> s;
+        for (uint64_t i : idx) s.insert(i >> (log_a * (r + 1)));
+        plans.emplace_back();
+        plan_openings(*fri_trees[r], std::vector<uint64_t>(s.begin(), s.end()), plans.back());
+    }
+    std::vector<Seg> segs;
+    uint64_t total = 0;
+    for (auto &p : plans) {
+        for (auto &r : p.rows) segs.push_back({r.src, r.len, total}), total += r.len;
+        for (auto *s : p.sibs) segs.push_back({s, 4, total}), total += 4;
+    }
+    std::vector<uint64_t> gathered(total);
+    if (!segs.empty()) {
+        DBuf d_segs = ctx.alloc(segs.size() * 3);
+        DBuf d_out = ctx.alloc(total);
+        std::vector<uint64_t> raw(segs.size() * 3);
+        memcpy(raw.data(), segs.data(), segs.size() * sizeof(Seg));
+        DBuf up = ctx.upload(raw);
+        L(gather_kernel, (unsigned)std::min<size_t>(segs.size(), 65535), 128, 0, (const Seg *)up.p, (uint64_t)segs.size(),
+          d_out.p);
+        ctx.d2h(gathered.data(), d_out.p, total);
+        ctx.sync();
+        po.d2h += 8 * total;
+    }
+    {
+        uint64_t off = 0;
+        for (auto &p : plans) {
+            for (auto &r : p.rows) {
+                for (uint64_t k = 0; k < r.len; k++) tr.hint_field(gathered[off + k]);
+                for (uint64_t k = r.len; k < r.padded; k++) tr.hint_field(0);
+                off += r.len;
+            }
+            for (size_t s = 0; s < p.sibs.size(); s++) {
+                tr.hint_commit(&gathered[off]);
+                off += 4;
+            }
+        }
+    }
+    CK(cudaEventRecord(ev[7], ctx.stream));
+    ctx.sync();
+    tr.finalize(po.digest);
+    for (int s = 0; s < 7; s++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
+        po.stage_ms[s] = ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    po.fields = std::move(tr.fields);
+    po.commits = std::move(tr.commits);
+    po.launches = L.n + ctx.launches - launches_before;
+}
+
+}  // namespace p3g

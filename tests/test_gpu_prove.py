@@ -1,0 +1,75 @@
+"""Whole-proof parity: the GPU prover's transcript (fields, commitments,
+digest) is bit-identical to the oracle's on the same traces and parameters."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+
+
+def pcs_dict(p):
+    return dict(log_blowup=p.log_blowup, log_folding_arity=p.log_folding_arity,
+                log_final_degree=p.log_final_degree, folding_pow_bits=p.folding_pow_bits,
+                deep_pow_bits=p.deep_pow_bits, num_queries=p.num_queries, query_pow_bits=p.query_pow_bits)
+
+
+def check_same(gpu, orc):
+    assert np.array_equal(gpu.proof.commitments, orc["commits"]), "commitments differ"
+    assert len(gpu.proof.fields) == len(orc["fields"])
+    diff = np.nonzero(gpu.proof.fields != orc["fields"])[0]
+    assert diff.size == 0, f"first differing field at {diff[:5]}"
+    assert np.array_equal(gpu.digest, orc["digest"])
+
+
+@pytest.mark.parametrize("arity", [1, 2, 3])
+def test_cubic_single_trace(product, gpu_ctx, arity):
+    k, t = O.cubic_trace(8, 12, 21)
+    pcs = product.PcsParams(2, arity, 0, 4, 0, 12, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k)])
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_CUBIC, t, k)])
+    check_same(gpu, orc)
+
+
+def test_cubic_lifted_three_traces(product, gpu_ctx):
+    """Lifted multi-trace: three traces of ascending heights in one tree."""
+    specs = [(4, 32, 1), (7, 8, 2), (9, 4, 3)]
+    inst, oinst = [], []
+    for log_h, w, seed in specs:
+        k, t = O.cubic_trace(log_h, w, seed)
+        inst.append(product.AirWitness(product.AIR_CUBIC, t, k))
+        oinst.append((O.AIR_CUBIC, t, k))
+    pcs = product.PcsParams(3, 2, 0, 5, 2, 20, 3)
+    gpu = product.prove_multi(gpu_ctx, pcs, inst)
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), oinst)
+    check_same(gpu, orc)
+
+
+def test_keccak_small(product, gpu_ctx):
+    inputs = O.keccak_inputs(1, 5)
+    t = O.keccak_trace(inputs, 7)
+    pcs = product.PcsParams(1, 1, 0, 6, 0, 16, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, t)])
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t, None)])
+    check_same(gpu, orc)
+
+
+def test_keccak_42_perms_config(product, gpu_ctx):
+    """The CPU-runnable Keccak workload: 42 permutations, 2^10 rows, the
+    example's parameters (log_blowup 1, arity 2, final degree 0, folding PoW
+    16, 100 queries)."""
+    inputs = O.keccak_inputs(1, 42)
+    t = O.keccak_trace(inputs, 10)
+    pcs = product.PcsParams(1, 1, 0, 16, 0, 100, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, t)])
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t, None)])
+    check_same(gpu, orc)
+
+
+def test_device_resident_trace(product, gpu_ctx):
+    k, t = O.cubic_trace(6, 8, 5)
+    pcs = product.PcsParams(1, 1, 0, 3, 0, 8, 0)
+    host = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k)])
+    dev = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, product.to_device(t), k)])
+    assert np.array_equal(host.proof.fields, dev.proof.fields)
+    assert np.array_equal(host.digest, dev.digest)

@@ -18,7 +18,7 @@ def rand_mat(rng, h, w):
 def test_coset_lde_matches_oracle(product, gpu_ctx, log_h, w, log_blowup):
     rng = np.random.default_rng(log_h * 100 + w)
     t = rand_mat(rng, 1 << log_h, w)
-    shift = int(rng.integers(1, P))
+    shift = int(rng.integers(1, P, dtype=np.uint64))
     want = O.coset_lde_bitrev(t, log_blowup, shift)
     got = product.to_host(product.coset_lde(gpu_ctx, product.to_device(t), log_blowup, shift))
     assert got.shape == want.shape
