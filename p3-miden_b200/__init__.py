@@ -295,9 +295,10 @@ class StarkOutput:
     gpu_launches: int
     h2d_bytes: int
     d2h_bytes: int
+    device_ms: float  # whole proof on the device timeline (CUDA events)
 
 
-STAGES = ("commit main", "commit aux", "constraints", "commit quotient", "DEEP", "FRI commit", "queries")
+STAGES = ("main LDE", "main tree", "commit aux", "constraints", "commit quotient", "DEEP", "FRI commit", "queries")
 
 
 def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> StarkOutput:
@@ -334,7 +335,7 @@ def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> St
         commits = np.ctypeslib.as_array(out.commits, shape=(out.n_commits * 4,)).reshape(-1, 4).copy()
         res = StarkOutput(np.array(out.digest[:], dtype=np.uint64), TranscriptData(fields, commits),
                           list(out.stage_ms[:len(STAGES)]), int(out.gpu_launches), int(out.h2d_bytes),
-                          int(out.d2h_bytes))
+                          int(out.d2h_bytes), float(out.stage_ms[11]))
     finally:
         lib().p3g_proof_free(C.byref(out))
     return res

@@ -139,7 +139,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     const uint64_t n = 1ull << log_lde;
     Transcript tr(ctx.p2);
 
-    cudaEvent_t ev[9];
+    cudaEvent_t ev[10];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventRecord(ev[0], ctx.stream));
 
@@ -160,10 +160,11 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         coset_lde(ctx, dt, w, h, w, lb, shift, main_lde[i].p, tmp.p);
         main_mats.push_back({main_lde[i].p, h << lb, w});
     }
+    CK(cudaEventRecord(ev[1], ctx.stream));
     Tree main_tree;
     build_tree(ctx, main_tree, main_mats, 8);
     tr.send_commit(main_tree.root);
-    CK(cudaEventRecord(ev[1], ctx.stream));
+    CK(cudaEventRecord(ev[2], ctx.stream));
 
     // ---- 2. randomness (max num_randomness over the AIRs = 1) and the
     // 1-column zero aux traces flattened to 2 base columns
@@ -180,7 +181,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     Tree aux_tree;
     build_tree(ctx, aux_tree, aux_mats, 8);
     tr.send_commit(aux_tree.root);
-    CK(cudaEventRecord(ev[2], ctx.stream));
+    CK(cudaEventRecord(ev[3], ctx.stream));
 
     // ---- 4./5. alpha, beta; constraints with cyclic extension
     const gl::ef alpha = tr.ch.sample_ef();
@@ -239,7 +240,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         for (uint64_t t = 0; t < D; t++) v.inv_van[t] = gl::inv(gl::sub(gl::mul(s_pow_n, x), 1)), x = gl::mul(x, wd);
         L(quot::divide_vanishing_kernel, blocks_for(max_qh, 256), 256, 0, acc.p, max_qh, v);
     }
-    CK(cudaEventRecord(ev[3], ctx.stream));
+    CK(cudaEventRecord(ev[4], ctx.stream));
 
     // ---- 7. quotient chunks: N x D EF -> (N*B) x 2D base on gK
     const uint64_t N = inst[n_inst - 1].height;
@@ -254,7 +255,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     Tree quot_tree;
     build_tree(ctx, quot_tree, {{quot_lde.p, N << lb, 2 * D}}, 8);
     tr.send_commit(quot_tree.root);
-    CK(cudaEventRecord(ev[4], ctx.stream));
+    CK(cudaEventRecord(ev[5], ctx.stream));
 
     // ---- 8. OOD point outside H and gK (coset.rs:329-342)
     gl::ef z;
@@ -435,7 +436,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     q.release();
     weights.clear();
     dots.clear();
-    CK(cudaEventRecord(ev[5], ctx.stream));
+    CK(cudaEventRecord(ev[6], ctx.stream));
 
     // ---- FRI commit phase
     const uint32_t log_a = pcs.log_folding_arity;
@@ -521,7 +522,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         }
         for (uint64_t k = final_deg; k-- > 0;) tr.send_ef(c[k]);
     }
-    CK(cudaEventRecord(ev[6], ctx.stream));
+    CK(cudaEventRecord(ev[7], ctx.stream));
 
     // ---- query phase
     grind(pcs.query_pow_bits);
@@ -573,13 +574,18 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             }
         }
     }
-    CK(cudaEventRecord(ev[7], ctx.stream));
+    CK(cudaEventRecord(ev[8], ctx.stream));
     ctx.sync();
     tr.finalize(po.digest);
-    for (int s = 0; s < 7; s++) {
+    for (int s = 0; s < 8; s++) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
         po.stage_ms[s] = ms;
+    }
+    {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[0], ev[8]));
+        po.stage_ms[11] = ms;  // whole proof on the device timeline
     }
     for (auto &e : ev) cudaEventDestroy(e);
     po.fields = std::move(tr.fields);
