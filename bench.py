@@ -32,7 +32,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 N_PERMS = 10922
-LOG_H = 18
+LOG_H = 18  # overridden by --log-h for small profiling cases
 PCS = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bits=16,
            deep_pow_bits=0, num_queries=100, query_pow_bits=0)
 WORKLOAD = "keccak-f1600 AIR, 10922 perms -> 2^18 x 2633 Goldilocks trace, lifted STARK (Poseidon2-12 LMCS)"
@@ -305,7 +305,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--log-h", type=int, default=18,
+                    help="trace height (log2); 18 is the measured workload, smaller values are profiling cases")
     args = ap.parse_args()
+    global LOG_H, N_PERMS
+    if args.log_h != LOG_H:
+        LOG_H = args.log_h
+        N_PERMS = (1 << LOG_H) // 24
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

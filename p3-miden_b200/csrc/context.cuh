@@ -71,6 +71,9 @@ struct TwTables {
     DBuf fwd_lo, fwd_hi, inv_lo, inv_hi;
     uint32_t lo_bits;
 };
+struct Tw1024 {
+    DBuf fwd, inv;  // w_1024^j and w_1024^-j, j < 512
+};
 
 struct Ctx {
     int device = 0;
@@ -81,6 +84,19 @@ struct Ctx {
     uint64_t *pinned = nullptr;  // small pinned staging area
     size_t pinned_words = 0;
     uint64_t launches = 0;       // kernels launched by this context
+    std::unique_ptr<Tw1024> t1024;
+
+    const Tw1024 &tw1024() {
+        if (!t1024) {
+            t1024 = std::make_unique<Tw1024>();
+            uint64_t w = gl::root(10), wi = gl::inv(w), x = 1, y = 1;
+            std::vector<uint64_t> a(512), b(512);
+            for (int j = 0; j < 512; j++) a[j] = x, b[j] = y, x = gl::mul(x, w), y = gl::mul(y, wi);
+            t1024->fwd = upload(a);
+            t1024->inv = upload(b);
+        }
+        return *t1024;
+    }
 
     DBuf alloc(size_t words) {
         DBuf b;
@@ -167,10 +183,11 @@ template <int C, bool DIF>
 inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     uint32_t k = a.bhi - a.blo;
     dim3 grid((unsigned)(h >> k), (unsigned)((a.w + C - 1) / C));
-    size_t smem = (size_t(1) << k) * C * 8;
+    size_t smem = ((size_t(1) << k) * C + 512 + 16) * 8;
     static bool attr_set = false;
     if (!attr_set) {
-        CK(cudaFuncSetAttribute(ntt::ntt_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1024 * C * 8));
+        CK(cudaFuncSetAttribute(ntt::ntt_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (1024 * C + 512 + 16) * 8));
         attr_set = true;
     }
     ntt::ntt_pass_kernel<C, DIF><<<grid, 256, smem, ctx.stream>>>(a);
@@ -209,6 +226,7 @@ inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h
             a.bhi = blo + sizes[pi];
             a.src_bitrev = pi == 0;
             a.tw = ntt::PowTab{tw.inv_lo.p, tw.inv_hi.p, tw.lo_bits};
+            a.tw1024 = ctx.tw1024().inv.p;
             a.has_scale = 0;
             launch_pass_any<false>(ctx, a, h);
             blo = a.bhi;
@@ -242,6 +260,7 @@ inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h
     uint64_t sk = shift;
     for (uint64_t k = 0; k < B; k++) {
         pow_table(sk, L, lo_bits, lo, hi);
+        for (auto &v : lo) v = gl::mul(v, hinv);  // the inverse transform's 1/h
         DBuf dlo = ctx.upload(lo), dhi = ctx.upload(hi);
         uint64_t *blk = d_out + gl::bitrev(k, log_blowup) * h * w;
         uint32_t bhi = L;
@@ -257,9 +276,9 @@ inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h
             a.blo = bhi - sizes[pi];
             a.src_bitrev = 0;
             a.tw = ntt::PowTab{tw.fwd_lo.p, tw.fwd_hi.p, tw.lo_bits};
+            a.tw1024 = ctx.tw1024().fwd.p;
             a.has_scale = pi == 0;
             a.scale = ntt::PowTab{dlo.p, dhi.p, lo_bits};
-            a.scale_const = hinv;
             launch_pass_any<true>(ctx, a, h);
             bhi = a.blo;
         }

@@ -18,10 +18,29 @@
 
 __constant__ uint64_t c_p2[p2::N_PARAMS];
 
-struct P2Const {
-    __device__ __forceinline__ uint64_t operator[](int i) const { return c_p2[i]; }
-};
-__device__ __forceinline__ void p2_permute_dev(uint64_t *s) { p2::permute(s, P2Const()); }
+// Device permutation: one looped copy of the round body per call site, so
+// that kernels stay small enough for the instruction cache (the fully
+// unrolled form stalled on instruction fetch). Rounds 0-3 and 26-29 are
+// external, 4-25 internal; constants come from the __constant__ table.
+__device__ __forceinline__ void p2_permute_dev(uint64_t *s) {
+    p2::ext_linear(s);
+#pragma unroll 1
+    for (int r = 0; r < 30; r++) {
+        if (r < 4 || r >= 26) {
+            const int off = r < 4 ? p2::OFF_INIT + 12 * r : p2::OFF_TERM + 12 * (r - 26);
+#pragma unroll
+            for (int i = 0; i < 12; i++) s[i] = p2::sbox(gl::add(s[i], c_p2[off + i]));
+            p2::ext_linear(s);
+        } else {
+            s[0] = p2::sbox(gl::add(s[0], c_p2[p2::OFF_INT + r - 4]));
+            uint64_t sum = s[0];
+#pragma unroll
+            for (int i = 1; i < 12; i++) sum = gl::add(sum, s[i]);
+#pragma unroll
+            for (int i = 0; i < 12; i++) s[i] = gl::add(gl::mul(s[i], c_p2[p2::OFF_DIAG + i]), sum);
+        }
+    }
+}
 
 namespace merkle {
 
@@ -38,17 +57,18 @@ struct ClassArgs {
     uint64_t *digests_out;  // 4 words per leaf, or null
 };
 
+// absorb one row (rate 8, overwrite mode, zero-padded last chunk); a single
+// permutation call site
 __device__ __forceinline__ void absorb_row(uint64_t *s, const uint64_t *row, uint64_t w) {
-    uint64_t i = 0;
-    for (; i + 8 <= w; i += 8) {
+#pragma unroll 1
+    for (uint64_t i = 0; i < w; i += 8) {
+        if (i + 8 <= w) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) s[j] = __ldg(row + i + j);
-        p2_permute_dev(s);
-    }
-    if (i < w) {
-        uint64_t rem = w - i;
+            for (int j = 0; j < 8; j++) s[j] = __ldg(row + i + j);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; j++) s[j] = (uint64_t)j < rem ? __ldg(row + i + j) : 0;
+            for (int j = 0; j < 8; j++) s[j] = i + j < w ? __ldg(row + i + j) : 0;
+        }
         p2_permute_dev(s);
     }
 }
