@@ -1,0 +1,148 @@
+/*
+ * p3g.h — C ABI of libp3miden_b200.so, the B200 (sm_100a) implementation of
+ * the lifted-STARK prover hot path of adr1anh/p3-miden v0.5.0 for the
+ * Goldilocks + Poseidon2 configuration (goldilocks_poseidon2:
+ * p3-miden-dev-utils/src/configs.rs:393-407).
+ *
+ * Conventions
+ *  - Field elements are canonical Goldilocks values (< 2^64 - 2^32 + 1) in
+ *    uint64_t. Extension elements (F[x]/(x^2 - 7)) are two words (c0, c1).
+ *  - Matrices are row-major, height x width, one polynomial per column.
+ *  - "d_" pointers are device pointers on the context's device; all others
+ *    are host pointers.
+ *  - Every call returns a status (P3G_OK = 0) and never aborts the process
+ *    or traps the GPU; p3g_last_error() describes the last failure of a
+ *    context. Calls on one context must come from one host thread at a time.
+ *  - Results are bit-identical to the reference prover's on the same inputs
+ *    (see the oracle under oracle/ and the parity tests).
+ */
+#ifndef P3G_H
+#define P3G_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum p3g_status {
+    P3G_OK = 0,
+    P3G_ERR_INVALID = 1,    /* bad argument: null pointer, size, unsupported parameter */
+    P3G_ERR_VALIDATION = 2, /* ProverError / AirValidationError equivalents */
+    P3G_ERR_OOM = 3,        /* device allocation refused */
+    P3G_ERR_TIMEOUT = 4,    /* a bounded search gave up (proof-of-work) */
+    P3G_ERR_CUDA = 5        /* other CUDA runtime error */
+};
+
+enum p3g_air {
+    P3G_AIR_CUBIC = 1,  /* c_i[r+1] = c_i[r]^3 + c_{(i+1) mod w}[r] + k_i, degree 3 */
+    P3G_AIR_KECCAK = 2  /* Keccak-f[1600] AIR, 2633 columns, 24 rows per permutation */
+};
+
+typedef struct p3g_ctx p3g_ctx;
+typedef struct p3g_tree p3g_tree;
+
+/* PcsParams::new(log_blowup, log_folding_arity, log_final_degree,
+ * folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits)
+ * (p3-miden-lifted-fri/src/params.rs:170-204). */
+typedef struct {
+    uint32_t log_blowup, log_folding_arity, log_final_degree;
+    uint32_t folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
+} p3g_pcs_params;
+
+/* One (AIR, AirWitness) pair of prove_multi (p3-miden-lifted-stark/src/
+ * prover/mod.rs:223-227; AirWitness: p3-miden-lifted-air/src/instance.rs:17-24).
+ * The trace is borrowed for the duration of the call. */
+typedef struct {
+    int32_t air;             /* enum p3g_air */
+    int32_t trace_on_device; /* 0: host memory (pinned is fastest), 1: device memory */
+    uint64_t height, width;  /* power-of-two height; instances in ascending height order */
+    const uint64_t *trace;   /* row-major height x width */
+    const uint64_t *consts;  /* host; cubic AIR: k[width]; Keccak: NULL */
+    uint64_t n_consts;
+} p3g_instance;
+
+/* StarkOutput { digest, proof: TranscriptData { fields, commitments } }
+ * (p3-miden-lifted-stark/src/proof.rs:39-44, p3-miden-transcript/src/data.rs:11-14).
+ * Buffers are malloc'ed by the library; release with p3g_proof_free. */
+typedef struct {
+    uint64_t *fields;
+    uint64_t n_fields;
+    uint64_t *commits; /* 4 words per commitment */
+    uint64_t n_commits;
+    uint64_t digest[12];
+    double stage_ms[12]; /* device time per protocol stage; [11] = whole proof */
+    uint64_t gpu_launches;
+    uint64_t h2d_bytes, d2h_bytes;
+} p3g_proof;
+
+/* ------------------------------------------------------------ context */
+/* Creates a context on `device` with the Poseidon2 constants
+ * [rc_init 4x12 | rc_term 4x12 | rc_int 22 | diag 12] (130 words): the
+ * StarkConfig's permutation (config.rs:26-42, configs.rs:214-233). */
+int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_ctx **out);
+void p3g_ctx_destroy(p3g_ctx *ctx);
+const char *p3g_last_error(const p3g_ctx *ctx);
+
+/* Poseidon2Goldilocks<12>::new_from_rng_128(SmallRng::seed_from_u64(2025))
+ * round constants (configs.rs:215-218) with this build's placeholder
+ * internal diagonal. */
+void p3g_default_poseidon2_params(uint64_t *out130);
+void p3g_poseidon2_params_from_seed(uint64_t seed, const uint64_t *diag12, uint64_t *out130);
+
+/* ------------------------------------------------------------- prover */
+/* prove_multi (p3-miden-lifted-stark/src/prover/mod.rs:223-461) with a fresh
+ * challenger (configs.rs:231-233). */
+int p3g_prove(p3g_ctx *ctx, const p3g_pcs_params *pcs, const p3g_instance *instances, uint64_t n,
+              p3g_proof *out);
+void p3g_proof_free(p3g_proof *proof);
+
+/* ------------------------------------------------------- stage seams */
+/* TwoAdicSubgroupDft::coset_lde_batch(trace, log_blowup, shift) followed by
+ * bit_reverse_rows (p3-miden-lifted-stark/src/prover/commit.rs:217-222;
+ * trait from p3-dft 0.5.0). d_in: height x width, d_out: (height << log_blowup) x width. */
+int p3g_coset_lde(p3g_ctx *ctx, const uint64_t *d_in, uint64_t height, uint64_t width, uint32_t log_blowup,
+                  uint64_t shift, uint64_t *d_out);
+
+/* Lmcs::build_tree / build_aligned_tree (p3-miden-lmcs/src/lib.rs:191-197,
+ * lmcs.rs:412-440) over device matrices sorted by ascending height;
+ * alignment 1 = build_tree, 8 = build_aligned_tree (the sponge rate). */
+int p3g_lmcs_build(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
+                   uint64_t n, uint32_t alignment, p3g_tree **out);
+/* LmcsTree::root (lib.rs:264) */
+int p3g_lmcs_root(const p3g_tree *tree, uint64_t *out4);
+/* digest layer `level` (0 = leaves) copied to host: (height >> level) x 4 words */
+int p3g_lmcs_layer(p3g_ctx *ctx, const p3g_tree *tree, uint32_t level, uint64_t *host_out);
+/* LmcsTree::prove_batch hints (lifted_tree.rs:157-224) for strictly
+ * ascending indices: rows (padded to the alignment) into fields_out, sibling
+ * digests into commits_out; *n_fields / *n_commits are capacities on entry
+ * and counts on return. */
+int p3g_lmcs_prove_batch(p3g_ctx *ctx, const p3g_tree *tree, const uint64_t *indices, uint64_t n,
+                         uint64_t *fields_out, uint64_t *n_fields, uint64_t *commits_out, uint64_t *n_commits);
+void p3g_lmcs_free(p3g_tree *tree);
+
+/* The configuration's permutation (Poseidon2Goldilocks<12>::permute_mut) on
+ * n device states of 12 words, in place. */
+int p3g_poseidon2_permute_batch(p3g_ctx *ctx, uint64_t *d_states, uint64_t n);
+
+/* GrindingChallenger::grind (p3-miden-transcript/src/prover.rs:140-144;
+ * DuplexChallenger, p3-challenger 0.5.0): the smallest witness w such that a
+ * challenger with sponge state `state12` and `n_pending` buffered inputs,
+ * after observing w, samples a word whose low `bits` bits are zero. */
+int p3g_grind(p3g_ctx *ctx, const uint64_t *state12, const uint64_t *pending, uint32_t n_pending, uint32_t bits,
+              uint64_t *witness);
+
+/* ------------------------------------------------- caller-side helpers */
+/* generate_keccak_trace (p3-miden-lifted-examples/src/keccak.rs:54-56):
+ * 2^log_height x 2633, n_perms * 24 <= 2^log_height. */
+int p3g_keccak_trace(const uint64_t *inputs25, uint64_t n_perms, uint32_t log_height, uint64_t *out);
+/* SmallRng::seed_from_u64(seed).random::<[u64; 25]>() per permutation
+ * (p3-miden-lifted-examples/src/bin/lifted_keccak.rs:167-170) */
+int p3g_keccak_inputs(uint64_t seed, uint64_t n_perms, uint64_t *out25);
+/* Cubic AIR trace: k then row 0 drawn from SmallRng(seed), forward iteration. */
+int p3g_cubic_trace(uint32_t log_height, uint64_t width, uint64_t seed, uint64_t *consts_out, uint64_t *trace_out);
+uint64_t p3g_air_num_constraints(int32_t air, uint64_t width);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* P3G_H */
