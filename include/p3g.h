@@ -131,6 +131,19 @@ int p3g_poseidon2_permute_batch(p3g_ctx *ctx, uint64_t *d_states, uint64_t n);
 int p3g_grind(p3g_ctx *ctx, const uint64_t *state12, const uint64_t *pending, uint32_t n_pending, uint32_t bits,
               uint64_t *witness);
 
+/* No counterpart in the reference. The coset LDE of p3g_coset_lde for
+ * callers that cannot allocate device memory (a fixed, pre-reserved HBM
+ * budget, or a host runtime whose allocator forbids cudaMalloc/cudaFree on
+ * its hot path): it allocates nothing, using a 16.1 MiB static device array
+ * inside the library (held by every GPU that loads it). Limits: height <=
+ * 2^22 and height * width <= 2^21 words (p3g_coset_lde_noalloc_max_words),
+ * else P3G_ERR_INVALID. Asynchronous on `stream`; the first call on a device
+ * does a one-time set-up and should come before any stream capture; calls
+ * that overlap on the GPU share the array and race. */
+int p3g_coset_lde_noalloc(const uint64_t *d_in, uint64_t height, uint64_t width, uint32_t log_blowup, uint64_t shift,
+                          uint64_t *d_out, void *stream);
+uint64_t p3g_coset_lde_noalloc_max_words(void);
+
 /* ------------------------------------------------- caller-side helpers */
 /* generate_keccak_trace (p3-miden-lifted-examples/src/keccak.rs:54-56):
  * 2^log_height x 2633, n_perms * 24 <= 2^log_height. */

@@ -37,7 +37,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return OUT
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", str(OUT), str(CSRC / "p3g_all.cu"), "-lcudart"]
+    cmd = [nvcc, *NVCC_FLAGS, "-o", str(OUT), str(CSRC / "p3g_all.cu"), str(CSRC / "lde_noalloc.cu"), "-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

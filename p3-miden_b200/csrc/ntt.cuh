@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(256) ntt_pass_kernel(const __grid_constant__ P
 // Multiply row k, column col of a row-major matrix by col_base[col/2]^k
 // (quotient chunk de-shifting, quotient.rs:484-497). col_base holds one
 // value per EF column.
-__global__ void scale_rows_by_colpow_kernel(uint64_t *m, uint64_t h, uint64_t w, const uint64_t *col_base_pows_lo,
+static __global__ void scale_rows_by_colpow_kernel(uint64_t *m, uint64_t h, uint64_t w, const uint64_t *col_base_pows_lo,
                                             const uint64_t *col_base_pows_hi, uint32_t lo_bits, uint64_t hi_len) {
     uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= h * w) return;
