@@ -126,7 +126,7 @@ __global__ void permute_batch_kernel(uint64_t *st, uint64_t n) {
     for (int k = 0; k < 12; k++) s[k] = st[i * 12 + k];
     p2_permute_dev(s);
 #pragma unroll
-    for (int k = 0; k < 12; k++) st[i * 12 + k] = s[k];
+    for (int k = 0; k < 12; k++) st[i * 12 + k] = p2w::canon(s[k]);
 }
 }  // namespace p3g
 

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ 
             p2_permute_dev(s);
         }
 #pragma unroll
-        for (int i = 0; i < 4; i++) a.digests[4 * g + i] = s[i];
+        for (int i = 0; i < 4; i++) a.digests[4 * g + i] = p2w::canon(s[i]);
     }
 }
 
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(128) leaf_hash_kernel(const uint64_t *evals, u
         p2_permute_dev(s);
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) digests[4 * k + i] = s[i];
+    for (int i = 0; i < 4; i++) digests[4 * k + i] = p2w::canon(s[i]);
 }
 
 // Proof-of-work search over witnesses [base, base + count): the challenger
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(128) grind_kernel(const __grid_constant__ Grin
         for (uint32_t i = 0; i < a.n_pending; i++) s[i] = a.pending[i];
         s[a.n_pending] = w;
         p2_permute_dev(s);
-        if ((s[7] & mask) == 0) atomicMin(a.found, (unsigned long long)w);
+        if ((p2w::canon(s[7]) & mask) == 0) atomicMin(a.found, (unsigned long long)w);
     }
 }
 

@@ -22,22 +22,106 @@ __constant__ uint64_t c_p2[p2::N_PARAMS];
 // that kernels stay small enough for the instruction cache (the fully
 // unrolled form stalled on instruction fetch). Rounds 0-3 and 26-29 are
 // external, 4-25 internal; constants come from the __constant__ table.
+//
+// Arithmetic is lazy: state words are kept weakly reduced (any value below
+// 2^64 congruent mod p); the linear layers accumulate in 96 bits and reduce
+// once per output; s*mu + sum is reduced once from 128 bits. Callers
+// canonicalise words that leave the permutation (p2w::canon).
+namespace p2w {
+constexpr uint64_t EPS = 0xFFFFFFFFull;
+struct W {  // lo + hi * 2^64
+    uint64_t lo;
+    uint32_t hi;
+};
+__device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo) {
+    uint64_t hh = hi >> 32, hl = hi & EPS;
+    uint64_t t = lo - hh;
+    if (lo < hh) t -= EPS;
+    uint64_t u = hl * EPS;
+    uint64_t r = t + u;
+    if (r < u) r += EPS;
+    return r;
+}
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce128(__umul64hi(a, b), a * b); }
+__device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= gl::P ? a - gl::P : a; }
+// weak + canonical: one wrap at most
+__device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t c) {
+    uint64_t s = a + c;
+    if (s < c) s += EPS;
+    return s;
+}
+__device__ __forceinline__ W wide(uint64_t a) { return W{a, 0}; }
+__device__ __forceinline__ W wadd(W a, W b) {
+    W r;
+    r.lo = a.lo + b.lo;
+    r.hi = a.hi + b.hi + (r.lo < a.lo ? 1u : 0u);
+    return r;
+}
+__device__ __forceinline__ W wadd1(W a, uint64_t b) {
+    W r;
+    r.lo = a.lo + b;
+    r.hi = a.hi + (r.lo < b ? 1u : 0u);
+    return r;
+}
+__device__ __forceinline__ W wdbl(uint64_t a) { return W{a << 1, (uint32_t)(a >> 63)}; }
+// lo + hi * 2^64 with hi < 2^32: lo + hi * EPS, one wrap at most
+__device__ __forceinline__ uint64_t wreduce(W a) {
+    uint64_t u = (uint64_t)a.hi * EPS;
+    uint64_t r = a.lo + u;
+    if (r < u) r += EPS;
+    return r;
+}
+__device__ __forceinline__ uint64_t sbox(uint64_t x) {
+    uint64_t x2 = mul(x, x), x4 = mul(x2, x2), x3 = mul(x2, x);
+    return mul(x4, x3);
+}
+// circ(2*M4, M4, M4), M4 = circ(2,3,1,1): 96-bit accumulation, one reduction per output
+__device__ __forceinline__ void ext_linear(uint64_t *s) {
+    W y[12];
+#pragma unroll
+    for (int c = 0; c < 12; c += 4) {
+        uint64_t x0 = s[c], x1 = s[c + 1], x2 = s[c + 2], x3 = s[c + 3];
+        W t01 = wadd1(wide(x0), x1), t23 = wadd1(wide(x2), x3);
+        W t0123 = wadd(t01, t23);
+        W t01123 = wadd1(t0123, x1), t01233 = wadd1(t0123, x3);
+        y[c + 0] = wadd(t01123, t01);           // 2x0 + 3x1 + x2 + x3
+        y[c + 1] = wadd(t01123, wdbl(x2));      // x0 + 2x1 + 3x2 + x3
+        y[c + 2] = wadd(t01233, t23);           // x0 + x1 + 2x2 + 3x3
+        y[c + 3] = wadd(t01233, wdbl(x0));      // 3x0 + x1 + x2 + 2x3
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        W t = wadd(wadd(y[k], y[k + 4]), y[k + 8]);
+        s[k] = wreduce(wadd(y[k], t));
+        s[k + 4] = wreduce(wadd(y[k + 4], t));
+        s[k + 8] = wreduce(wadd(y[k + 8], t));
+    }
+}
+}  // namespace p2w
+
 __device__ __forceinline__ void p2_permute_dev(uint64_t *s) {
-    p2::ext_linear(s);
+    p2w::ext_linear(s);
 #pragma unroll 1
     for (int r = 0; r < 30; r++) {
         if (r < 4 || r >= 26) {
             const int off = r < 4 ? p2::OFF_INIT + 12 * r : p2::OFF_TERM + 12 * (r - 26);
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = p2::sbox(gl::add(s[i], c_p2[off + i]));
-            p2::ext_linear(s);
+            for (int i = 0; i < 12; i++) s[i] = p2w::sbox(p2w::add_c(s[i], c_p2[off + i]));
+            p2w::ext_linear(s);
         } else {
-            s[0] = p2::sbox(gl::add(s[0], c_p2[p2::OFF_INT + r - 4]));
-            uint64_t sum = s[0];
+            s[0] = p2w::sbox(p2w::add_c(s[0], c_p2[p2::OFF_INT + r - 4]));
+            p2w::W acc = p2w::wide(s[0]);
 #pragma unroll
-            for (int i = 1; i < 12; i++) sum = gl::add(sum, s[i]);
+            for (int i = 1; i < 12; i++) acc = p2w::wadd1(acc, s[i]);
+            const uint64_t sum = p2w::wreduce(acc);
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl::add(gl::mul(s[i], c_p2[p2::OFF_DIAG + i]), sum);
+            for (int i = 0; i < 12; i++) {
+                const uint64_t d = c_p2[p2::OFF_DIAG + i];
+                uint64_t lo = s[i] * d, hi = __umul64hi(s[i], d);
+                lo += sum;
+                hi += (lo < sum) ? 1 : 0;  // no overflow: hi <= 2^64 - 2 for a 64x64 product
+                s[i] = p2w::reduce128(hi, lo);
+            }
         }
     }
 }
@@ -88,7 +172,7 @@ __global__ void __launch_bounds__(128) leaf_class_kernel(const __grid_constant__
     for (int m = 0; m < a.n_mats; m++) absorb_row(s, a.data[m] + j * a.width[m], a.width[m]);
     if (a.digests_out) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) a.digests_out[j * 4 + i] = s[i];
+        for (int i = 0; i < 4; i++) a.digests_out[j * 4 + i] = p2w::canon(s[i]);
     } else {
 #pragma unroll
         for (int i = 0; i < 12; i++) a.states_out[j * 12 + i] = s[i];
@@ -105,7 +189,7 @@ __device__ __forceinline__ void compress2(const uint64_t *l, const uint64_t *r, 
     }
     p2_permute_dev(s);
 #pragma unroll
-    for (int i = 0; i < 4; i++) out[i] = s[i];
+    for (int i = 0; i < 4; i++) out[i] = p2w::canon(s[i]);
 }
 
 // One block compresses 2*blockDim.x digests of layer `l_in` through `levels`

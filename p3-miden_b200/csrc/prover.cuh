@@ -229,7 +229,20 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         a.consts = d_consts.p;
         a.acc = acc.p;
         if (I.air == AIR_CUBIC) L(quot::cubic_eval_kernel, blocks_for(qh * 32, 256), 256, 0, a);
-        else L(quot::keccak_eval_kernel, blocks_for(qh, 128), 128, 0, a);
+        else {
+            static bool attr = false;
+            if (!attr) {
+                CK(cudaFuncSetAttribute(quot::keccak_eval_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)quot::KEC_SMEM));
+                attr = true;
+            }
+            int dev_sms = 148;
+            CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx.device));
+            uint64_t blocks = std::min<uint64_t>(qh, (uint64_t)dev_sms * 3);
+            uint64_t ppb = (qh + blocks - 1) / blocks;
+            blocks = (qh + ppb - 1) / ppb;
+            L(quot::keccak_eval_block_kernel, (unsigned)blocks, quot::KEC_THREADS, quot::KEC_SMEM, a, ppb);
+        }
         ctx.sync();  // keep d_ap / d_consts alive until the kernel ran
     }
     // ---- 6. divide by Z_H on the max quotient coset
@@ -361,7 +374,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             g.base = base;
             g.count = batch;
             g.found = (unsigned long long *)fb.p;
-            L(fri::grind_kernel, 148 * 8, 128, 0, g);
+            L(fri::grind_kernel, 148 * 2, 128, 0, g);
             ctx.d2h(ctx.stage(1), fb.p, 1);
             ctx.sync();
             found = ctx.pinned[0];

@@ -92,105 +92,172 @@ __device__ __forceinline__ uint64_t kxor3(uint64_t a, uint64_t b, uint64_t c) { 
 __device__ __forceinline__ uint64_t kandn(uint64_t a, uint64_t b) { return gl::mul(gl::sub(1, a), b); }
 __device__ __forceinline__ uint64_t kbool(uint64_t a) { return gl::mul(a, gl::sub(a, 1)); }
 
-// All constraints of one row pair in emission order; the same list as the
-// oracle's restatement of the KeccakAir arithmetization.
-__device__ void keccak_constraints(const uint64_t *L, const uint64_t *N, uint64_t first, uint64_t trans, Fold &f) {
-    f.emit(gl::mul(first, gl::sub(__ldg(L + KC_STEP), 1)));
-    for (int i = 1; i < 24; i++) f.emit(gl::mul(first, __ldg(L + KC_STEP + i)));
-    for (int i = 0; i < 24; i++)
-        f.emit(gl::mul(trans, gl::sub(__ldg(N + KC_STEP + (i + 1) % 24), __ldg(L + KC_STEP + i))));
-    const uint64_t first_step = __ldg(L + KC_STEP), not_final = gl::sub(1, __ldg(L + KC_STEP + 23));
-    for (int o = 0; o < 100; o++) f.emit(gl::mul(first_step, gl::sub(__ldg(L + KC_PRE + o), __ldg(L + KC_A + o))));
-    const uint64_t ex = __ldg(L + KC_EXPORT);
-    f.emit(kbool(ex));
-    f.emit(gl::mul(not_final, ex));
-    const uint64_t nf_t = gl::mul(not_final, trans);
-    for (int o = 0; o < 100; o++) f.emit(gl::mul(nf_t, gl::sub(__ldg(L + KC_PRE + o), __ldg(N + KC_PRE + o))));
-    for (int x = 0; x < 5; x++)
-        for (int z = 0; z < 64; z++) {
-            uint64_t cxz = __ldg(L + KC_C + x * 64 + z);
-            f.emit(kbool(cxz));
-            uint64_t v = kxor3(cxz, __ldg(L + KC_C + ((x + 4) % 5) * 64 + z), __ldg(L + KC_C + ((x + 1) % 5) * 64 + (z + 63) % 64));
-            f.emit(gl::sub(__ldg(L + KC_CP + x * 64 + z), v));
-        }
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t acc = 0;
-                for (int z = l * 16 + 15; z >= l * 16; z--) {
-                    uint64_t ap = __ldg(L + KC_AP + (y * 5 + x) * 64 + z);
-                    f.emit(kbool(ap));
-                    acc = gl::add(gl::dbl(acc), kxor3(ap, __ldg(L + KC_C + x * 64 + z), __ldg(L + KC_CP + x * 64 + z)));
-                }
-                f.emit(gl::sub(acc, __ldg(L + KC_A + (y * 5 + x) * 4 + l)));
-            }
-    for (int x = 0; x < 5; x++)
-        for (int z = 0; z < 64; z++) {
-            uint64_t s = 0;
-            for (int y = 0; y < 5; y++) s = gl::add(s, __ldg(L + KC_AP + (y * 5 + x) * 64 + z));
-            uint64_t d = gl::sub(s, __ldg(L + KC_CP + x * 64 + z));
-            f.emit(gl::mul(gl::mul(d, gl::sub(d, 2)), gl::sub(d, 4)));
-        }
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t acc = 0;
-                for (int z = l * 16 + 15; z >= l * 16; z--) {
-                    uint64_t b[3];
-#pragma unroll
-                    for (int u = 0; u < 3; u++) {
-                        int bx = (x + u) % 5, ax = (bx + 3 * y) % 5;
-                        int rot = c_keccak_rot[ax * 5 + bx];
-                        b[u] = __ldg(L + KC_AP + (bx * 5 + ax) * 64 + (z + 64 - rot) % 64);
-                    }
-                    acc = gl::add(gl::dbl(acc), kxor2(b[0], kandn(b[1], b[2])));
-                }
-                f.emit(gl::sub(acc, __ldg(L + KC_APP + (y * 5 + x) * 4 + l)));
-            }
-    for (int l = 0; l < 4; l++) {
+// Constraint indices (emission order of the AIR's eval; 3182 in total):
+//   0..23     first-row flags      24..47  flag rotation     48..147 preimage == a
+//   148, 149  export               150..249 preimage continuity
+//   250..889  (x,z): bool c, xor c2 (interleaved)
+//   890..2589 a limbs: per (y,x,l) 16 bools (z descending) + the limb equation
+//   2590..2909 (x,z): sum_y a1 - c2 in {0,2,4}
+//   2910..3009 a2 limbs          3010..3077 a2[0][0] bits + limbs
+//   3078..3081 a3[0][0] limbs    3082..3181 output == next input (x outer)
+// (c2 = C', a1 = A', a2 = A'', a3 = A''' in the Keccak-f round notation.)
+constexpr int KEC_TASKS = 878;  // 200 heavy limb tasks, 8 small, 320 (x,z), 350 light
+
+struct KFold {
+    uint64_t c0 = 0, c1 = 0;
+    const uint64_t *ap;
+    __device__ __forceinline__ explicit KFold(const uint64_t *a) : ap(a) {}
+    __device__ __forceinline__ void emit(int k, uint64_t v) {
+        c0 = gl::add(c0, gl::mul(v, __ldg(ap + 2 * k)));
+        c1 = gl::add(c1, gl::mul(v, __ldg(ap + 2 * k + 1)));
+    }
+};
+
+__device__ __forceinline__ uint64_t kbit_b(const uint64_t *L, int bx, int by, int z) {
+    int ax = (bx + 3 * by) % 5;
+    int rot = c_keccak_rot[ax * 5 + bx];
+    return L[KC_AP + (bx * 5 + ax) * 64 + ((z + 64 - rot) & 63)];
+}
+
+// one task of one point; L, N in shared memory
+__device__ void keccak_task(int t, const uint64_t *L, const uint64_t *N, uint64_t first, uint64_t trans, KFold &f) {
+    const uint64_t not_final = gl::sub(1, L[KC_STEP + 23]);
+    if (t < 100) {  // A limbs from xor(A1, C, C2), with the bools of A1
+        int o = t, y = o / 20, x = (o / 4) % 5, l = o % 4;
+        int base = 890 + 17 * o;
         uint64_t acc = 0;
         for (int z = l * 16 + 15; z >= l * 16; z--) {
-            uint64_t bit = __ldg(L + KC_APP00 + z);
-            f.emit(kbool(bit));
+            uint64_t ap = L[KC_AP + (y * 5 + x) * 64 + z];
+            f.emit(base + (l * 16 + 15 - z), kbool(ap));
+            acc = gl::add(gl::dbl(acc), kxor3(ap, L[KC_C + x * 64 + z], L[KC_CP + x * 64 + z]));
+        }
+        f.emit(base + 16, gl::sub(acc, L[KC_A + o]));
+    } else if (t < 200) {  // A2 limbs: xor(B, andn(B[x+1], B[x+2]))
+        int o = t - 100, y = o / 20, x = (o / 4) % 5, l = o % 4;
+        uint64_t acc = 0;
+        for (int z = l * 16 + 15; z >= l * 16; z--) {
+            uint64_t b0 = kbit_b(L, x, y, z), b1 = kbit_b(L, (x + 1) % 5, y, z), b2 = kbit_b(L, (x + 2) % 5, y, z);
+            acc = gl::add(gl::dbl(acc), kxor2(b0, kandn(b1, b2)));
+        }
+        f.emit(2910 + o, gl::sub(acc, L[KC_APP + o]));
+    } else if (t < 204) {  // A2[0][0] bits
+        int l = t - 200, base = 3010 + 17 * l;
+        uint64_t acc = 0;
+        for (int z = l * 16 + 15; z >= l * 16; z--) {
+            uint64_t bit = L[KC_APP00 + z];
+            f.emit(base + (l * 16 + 15 - z), kbool(bit));
             acc = gl::add(gl::dbl(acc), bit);
         }
-        f.emit(gl::sub(acc, __ldg(L + KC_APP + l)));
-    }
-    for (int l = 0; l < 4; l++) {
+        f.emit(base + 16, gl::sub(acc, L[KC_APP + l]));
+    } else if (t < 208) {  // A3[0][0] = A2[0][0] xor RC
+        int l = t - 204;
         uint64_t acc = 0;
         for (int z = l * 16 + 15; z >= l * 16; z--) {
             uint64_t rcb = 0;
             for (int r = 0; r < 24; r++)
-                if ((c_keccak_rc[r] >> z) & 1) rcb = gl::add(rcb, __ldg(L + KC_STEP + r));
-            acc = gl::add(gl::dbl(acc), kxor2(__ldg(L + KC_APP00 + z), rcb));
+                if ((c_keccak_rc[r] >> z) & 1) rcb = gl::add(rcb, L[KC_STEP + r]);
+            acc = gl::add(gl::dbl(acc), kxor2(L[KC_APP00 + z], rcb));
         }
-        f.emit(gl::sub(acc, __ldg(L + KC_APPP00 + l)));
+        f.emit(3078 + l, gl::sub(acc, L[KC_APPP00 + l]));
+    } else if (t < 528) {  // (x, z): bool C, C2 xor, A1 column sum
+        int i = t - 208, x = i / 64, z = i % 64;
+        uint64_t cxz = L[KC_C + i];
+        f.emit(250 + 2 * i, kbool(cxz));
+        uint64_t v = kxor3(cxz, L[KC_C + ((x + 4) % 5) * 64 + z], L[KC_C + ((x + 1) % 5) * 64 + ((z + 63) & 63)]);
+        uint64_t cp = L[KC_CP + i];
+        f.emit(251 + 2 * i, gl::sub(cp, v));
+        uint64_t sm = 0;
+        for (int y = 0; y < 5; y++) sm = gl::add(sm, L[KC_AP + (y * 5 + x) * 64 + z]);
+        uint64_t d = gl::sub(sm, cp);
+        f.emit(2590 + i, gl::mul(gl::mul(d, gl::sub(d, 2)), gl::sub(d, 4)));
+    } else if (t < 552) {  // first-row flags
+        int i = t - 528;
+        f.emit(i, gl::mul(first, i == 0 ? gl::sub(L[KC_STEP], 1) : L[KC_STEP + i]));
+    } else if (t < 576) {  // flag rotation
+        int i = t - 552;
+        f.emit(24 + i, gl::mul(trans, gl::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
+    } else if (t < 676) {  // first step: preimage == a
+        int o = t - 576;
+        f.emit(48 + o, gl::mul(L[KC_STEP], gl::sub(L[KC_PRE + o], L[KC_A + o])));
+    } else if (t < 678) {  // export
+        uint64_t ex = L[KC_EXPORT];
+        if (t == 676) f.emit(148, kbool(ex));
+        else f.emit(149, gl::mul(not_final, ex));
+    } else if (t < 778) {  // preimage continuity
+        int o = t - 678;
+        f.emit(150 + o, gl::mul(gl::mul(not_final, trans), gl::sub(L[KC_PRE + o], N[KC_PRE + o])));
+    } else {  // round output == next round input (x outer, y inner)
+        int i = t - 778, x = i / 20, y = (i / 4) % 5, l = i % 4;
+        uint64_t outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
+        f.emit(3082 + i, gl::mul(gl::mul(not_final, trans), gl::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
     }
-    for (int x = 0; x < 5; x++)
-        for (int y = 0; y < 5; y++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t outv = (x == 0 && y == 0) ? __ldg(L + KC_APPP00 + l) : __ldg(L + KC_APP + (y * 5 + x) * 4 + l);
-                f.emit(gl::mul(nf_t, gl::sub(outv, __ldg(N + KC_A + (y * 5 + x) * 4 + l))));
-            }
 }
 
-// One thread per quotient point.
-__global__ void __launch_bounds__(128) keccak_eval_kernel(const __grid_constant__ EvalArgs a) {
-    const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Persistent blocks over contiguous point ranges. Rows are staged in a ring
+// of 3 shared-memory slots: point m needs rows m and m + 2 (D = 2), so each
+// LDE row is read from HBM once per block range. Selectors for the next 256
+// points are computed cooperatively (one inversion per point).
+constexpr int KEC_THREADS = 256;
+__global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __grid_constant__ EvalArgs a,
+                                                                         uint64_t points_per_block) {
+    extern __shared__ uint64_t sm[];
+    uint64_t *ring = sm;                    // 3 x 2633
+    uint64_t *sel = sm + 3 * KC_NCOLS;      // 256 x {first, trans}
+    uint64_t *red = sel + 2 * KEC_THREADS;  // 8 warps x 2
     const uint64_t qh = 1ull << a.log_qh;
-    if (m >= qh) return;
-    const uint64_t *L = a.lde + gl::bitrev(m, a.log_qh) * a.w;
-    const uint64_t *N = a.lde + gl::bitrev((m + a.D) & (qh - 1), a.log_qh) * a.w;
-    uint64_t x = point_x(a, m);
-    uint64_t zh = a.zh[m & (a.D - 1)];
-    uint64_t first = gl::mul(zh, gl::inv(gl::sub(x, 1)));
-    uint64_t trans = gl::sub(x, a.omega_h_inv);
-    Fold f(a.alpha_pows);
-    keccak_constraints(L, N, first, trans, f);
-    uint64_t *o = a.acc + 2 * m;
-    o[0] = gl::add(o[0], f.c0);
-    o[1] = gl::add(o[1], f.c1);
+    const uint64_t m0 = (uint64_t)blockIdx.x * points_per_block;
+    if (m0 >= qh) return;
+    const uint64_t m1 = min(qh, m0 + points_per_block);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    auto load_row = [&](uint64_t m, int slot) {
+        const uint64_t *src = a.lde + gl::bitrev(m & (qh - 1), a.log_qh) * a.w;
+        uint64_t *dst = ring + slot * KC_NCOLS;
+        for (int c = tid; c < KC_NCOLS; c += KEC_THREADS) dst[c] = __ldg(src + c);
+    };
+    load_row(m0, (int)(m0 % 3));
+    load_row(m0 + 1, (int)((m0 + 1) % 3));
+    for (uint64_t m = m0; m < m1; m++) {
+        const uint64_t j = m - m0;
+        if ((j & (KEC_THREADS - 1)) == 0) {
+            uint64_t pm = m + tid;
+            if (pm < m1) {
+                uint64_t x = point_x(a, pm);
+                sel[2 * tid] = gl::mul(a.zh[pm & (a.D - 1)], gl::inv(gl::sub(x, 1)));
+                sel[2 * tid + 1] = gl::sub(x, a.omega_h_inv);
+            }
+        }
+        load_row(m + 2, (int)((m + 2) % 3));
+        __syncthreads();
+        const uint64_t *L = ring + (m % 3) * KC_NCOLS;
+        const uint64_t *N = ring + ((m + 2) % 3) * KC_NCOLS;
+        const uint64_t first = sel[2 * (j & (KEC_THREADS - 1))], trans = sel[2 * (j & (KEC_THREADS - 1)) + 1];
+        KFold f(a.alpha_pows);
+        for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task(t, L, N, first, trans, f);
+        uint64_t c0 = f.c0, c1 = f.c1;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            c0 = gl::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
+            c1 = gl::add(c1, __shfl_xor_sync(0xffffffffu, c1, off));
+        }
+        if (lane == 0) {
+            red[2 * wid] = c0;
+            red[2 * wid + 1] = c1;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < KEC_THREADS / 32; w++) {
+                c0 = gl::add(c0, red[2 * w]);
+                c1 = gl::add(c1, red[2 * w + 1]);
+            }
+            uint64_t *o = a.acc + 2 * m;
+            o[0] = gl::add(o[0], c0);
+            o[1] = gl::add(o[1], c1);
+        }
+        // slot (m % 3) is overwritten by row m + 3 in the next iteration
+        __syncthreads();
+    }
 }
+constexpr size_t KEC_SMEM = (3 * KC_NCOLS + 2 * KEC_THREADS + 16) * 8;
 
 // acc[0..old) *= beta (EF); then acc[i] = acc[i mod old] for i in [old, new)
 __global__ void scale_ef_kernel(uint64_t *acc, uint64_t n, gl::ef beta) {

@@ -35,6 +35,9 @@ def test_poseidon2_permutation_matches_oracle(product, gpu_ctx):
     rng = np.random.default_rng(5)
     st = rng.integers(0, P, size=(300, 12), dtype=np.uint64)
     st[0] = 0
+    st[1] = P - 1  # every word at the top of the field: exercises every wrap
+    st[2, ::2] = P - 1
+    st[3] = np.arange(12, dtype=np.uint64) * np.uint64(0xFFFFFFFF)
     want = np.stack([O.permute(pp, s) for s in st])
     got = product.to_host(product.poseidon2_permute_batch(gpu_ctx, product.to_device(st)))
     assert np.array_equal(got, want)
