@@ -50,7 +50,50 @@ GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
     if (r >= P) r -= P;
     return r;
 }
-GL_HD uint64_t mul(uint64_t a, uint64_t b) { return reduce128(mulhi(a, b), a * b); }
+#if defined(__CUDA_ARCH__)
+// 64x64 -> 128 product by 32-bit partial products on carry chains, then the
+// reduction 2^64 = 2^32 - 1, 2^96 = -1 on the same chains. The result is
+// weakly reduced: below 2^64 and congruent mod p (not necessarily < p).
+__device__ __forceinline__ uint64_t mul_weak(uint64_t a, uint64_t b) {
+    uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    uint32_t r0, r1, r2, r3, t, ul, uh;
+    asm("mul.lo.u32 %0, %7, %9;\n\t"
+        "mul.hi.u32 %1, %7, %9;\n\t"
+        "mad.lo.cc.u32 %1, %7, %10, %1;\n\t"
+        "madc.hi.u32 %2, %7, %10, 0;\n\t"
+        "mad.lo.cc.u32 %1, %8, %9, %1;\n\t"
+        "madc.hi.cc.u32 %2, %8, %9, %2;\n\t"
+        "madc.hi.u32 %3, %8, %10, 0;\n\t"
+        "mad.lo.cc.u32 %2, %8, %10, %2;\n\t"
+        "addc.u32 %3, %3, 0;\n\t"
+        // (r1:r0) - r3, on borrow subtract eps
+        "sub.cc.u32 %0, %0, %3;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 %4, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, %4;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        // + r2 * eps = (r2 << 32) - r2, on carry add eps
+        "sub.cc.u32 %5, 0, %2;\n\t"
+        "subc.u32 %6, %2, 0;\n\t"
+        "add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.u32 %4, 0, 0;\n\t"
+        "neg.s32 %4, %4;\n\t"
+        "add.cc.u32 %0, %0, %4;\n\t"
+        "addc.u32 %1, %1, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3), "=&r"(t), "=&r"(ul), "=&r"(uh)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    return ((uint64_t)r1 << 32) | r0;
+}
+#endif
+GL_HD uint64_t mul(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    uint64_t r = mul_weak(a, b);
+    return r >= P ? r - P : r;
+#else
+    return reduce128(mulhi(a, b), a * b);
+#endif
+}
 GL_HD uint64_t sqr(uint64_t a) { return mul(a, a); }
 GL_HD uint64_t pow(uint64_t b, uint64_t e) {
     uint64_t r = 1;

@@ -42,7 +42,7 @@ __device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo) {
     if (r < u) r += EPS;
     return r;
 }
-__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return reduce128(__umul64hi(a, b), a * b); }
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return gl::mul_weak(a, b); }
 __device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= gl::P ? a - gl::P : a; }
 // weak + canonical: one wrap at most
 __device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t c) {
