@@ -50,7 +50,7 @@ GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
     if (r >= P) r -= P;
     return r;
 }
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDACC__)
 // 64x64 -> 128 product by 32-bit partial products on carry chains, then the
 // reduction 2^64 = 2^32 - 1, 2^96 = -1 on the same chains. The result is
 // weakly reduced: below 2^64 and congruent mod p (not necessarily < p).
