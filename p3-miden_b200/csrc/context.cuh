@@ -194,8 +194,30 @@ inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     CK(cudaGetLastError());
     ctx.launches++;
 }
+template <int C, bool DIF>
+inline void launch_pass_r8(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
+    uint32_t k = a.bhi - a.blo;
+    dim3 grid((unsigned)((a.w + C - 1) / C), (unsigned)(h >> k));
+    unsigned threads = (1u << (k - 3)) * C;
+    size_t smem = ((size_t(1) << k) * C + (size_t(1) << k) + 16) * 8;
+    static bool attr_set = false;
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(ntt::ntt_pass_r8_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (1024 * C + 1024 + 16) * 8));
+        attr_set = true;
+    }
+    ntt::ntt_pass_r8_kernel<C, DIF><<<grid, threads, smem, ctx.stream>>>(a);
+    CK(cudaGetLastError());
+    ctx.launches++;
+}
 template <bool DIF>
 inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
+    if (a.bhi - a.blo >= 3 && (h >> (a.bhi - a.blo)) <= 65535) {  // radix-8 register passes
+        if (a.w <= 2) launch_pass_r8<2, DIF>(ctx, a, h);
+        else if (a.w <= 4) launch_pass_r8<4, DIF>(ctx, a, h);
+        else launch_pass_r8<8, DIF>(ctx, a, h);
+        return;
+    }
     if (a.w <= 2) launch_pass<2, DIF>(ctx, a, h);
     else if (a.w <= 4) launch_pass<4, DIF>(ctx, a, h);
     else launch_pass<8, DIF>(ctx, a, h);

@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(256) colsum_kernel(const uint64_t *M, uint64_t
                                                      uint64_t rows_per_chunk, uint64_t *partial) {
     __shared__ uint64_t red[8][32][4];
     const int cl = threadIdx.x & 31, rl = threadIdx.x >> 5;
-    const uint64_t col = (uint64_t)blockIdx.y * 32 + cl;
-    const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_chunk;
+    // grid: x = column tile (fastest), y = row chunk
+    const uint64_t col = (uint64_t)blockIdx.x * 32 + cl;
+    const uint64_t r0 = (uint64_t)blockIdx.y * rows_per_chunk;
     const uint64_t r1 = min(d, r0 + rows_per_chunk);
     uint64_t s[4] = {0, 0, 0, 0};
     if (col < w) {
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(256) colsum_kernel(const uint64_t *M, uint64_t
 #pragma unroll
             for (int k = 0; k < 4; k++) s[k] = gl::add(s[k], red[r][cl][k]);
 #pragma unroll
-        for (int k = 0; k < 4; k++) partial[(blockIdx.x * w + col) * 4 + k] = s[k];
+        for (int k = 0; k < 4; k++) partial[(blockIdx.y * w + col) * 4 + k] = s[k];
     }
 }
 // out[col][0..4) = s_j * sum_chunk partial[chunk][col]

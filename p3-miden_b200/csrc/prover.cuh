@@ -333,7 +333,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
             n_chunks = (dm + rpc - 1) / rpc;
             DBuf part = ctx.alloc(n_chunks * m->w * 4);
-            L(deep::colsum_kernel, dim3((unsigned)n_chunks, (unsigned)col_tiles), 256, 0, m->d, m->w, dm,
+            L(deep::colsum_kernel, dim3((unsigned)col_tiles, (unsigned)n_chunks), 256, 0, m->d, m->w, dm,
               weights[dm].p, rpc, part.p);
             L(deep::colsum_finish_kernel, blocks_for(m->w, 128), 128, 0, part.p, n_chunks, m->w, sj[0], sj[1],
               evals.p + 4 * off);
