@@ -370,3 +370,139 @@ def generate_cubic_trace(log_h: int, width: int, seed: int, out: np.ndarray | No
         out = np.empty((1 << log_h, width), dtype=np.uint64)
     _check(lib().p3g_cubic_trace(log_h, width, seed, _ptr(k), out.ctypes.data_as(u64p)))
     return k, out
+
+
+# ---------------------------------------------------- batched / serving
+class JobC(C.Structure):
+    _fields_ = [("pcs", PcsParamsC), ("instances", C.POINTER(InstanceC)), ("n_instances", C.c_uint64),
+                ("arrival_s", C.c_double)]
+
+
+class JobResultC(C.Structure):
+    _fields_ = [("status", C.c_int32), ("pad", C.c_int32), ("proof", ProofC),
+                ("submit_s", C.c_double), ("start_s", C.c_double), ("end_s", C.c_double)]
+
+
+@dataclass
+class Job:
+    pcs: PcsParams
+    instances: list  # list[AirWitness]
+    arrival_s: float = 0.0
+
+
+@dataclass
+class JobResult:
+    status: int
+    output: StarkOutput | None
+    submit_s: float
+    start_s: float
+    end_s: float
+
+    @property
+    def latency_s(self) -> float:
+        return self.end_s - self.submit_s
+
+
+def _instances_c(instances, keep):
+    arr = (InstanceC * max(1, len(instances)))()
+    for i, w in enumerate(instances):
+        t = w.trace
+        if isinstance(t, np.ndarray):
+            t = np.ascontiguousarray(t, dtype=np.uint64)
+            ptr, on_dev = t.ctypes.data, 0
+        else:
+            ptr, on_dev = t.data_ptr(), int(t.is_cuda)
+        keep.append(t)
+        h, wd = t.shape
+        c = np.ascontiguousarray(w.consts if w.consts is not None else np.zeros(0), dtype=np.uint64)
+        keep.append(c)
+        arr[i] = InstanceC(w.air, on_dev, h, wd, C.cast(C.c_void_p(ptr), u64p),
+                           c.ctypes.data_as(u64p) if c.size else None, c.size)
+    keep.append(arr)
+    return arr
+
+
+def _result_from_c(r: JobResultC) -> JobResult:
+    out = None
+    if r.status == OK:
+        p = r.proof
+        fields = np.ctypeslib.as_array(p.fields, shape=(p.n_fields,)).copy()
+        commits = np.ctypeslib.as_array(p.commits, shape=(p.n_commits * 4,)).reshape(-1, 4).copy()
+        out = StarkOutput(np.array(p.digest[:], dtype=np.uint64), TranscriptData(fields, commits),
+                          list(p.stage_ms[:len(STAGES)]), int(p.gpu_launches), int(p.h2d_bytes),
+                          int(p.d2h_bytes), float(p.stage_ms[11]))
+        lib().p3g_proof_free(C.byref(r.proof))
+    return JobResult(int(r.status), out, r.submit_s, r.start_s, r.end_s)
+
+
+class ProofServer:
+    """Batched / continuous-batching prover: n_workers concurrent proofs on one
+    device, admitted by estimated HBM footprint against hbm_budget bytes."""
+
+    def __init__(self, device: int = 0, n_workers: int = 4, hbm_budget: int = 150 * 10**9,
+                 poseidon2_params: np.ndarray | None = None):
+        L = lib()
+        vp = C.c_void_p
+        for name, res, args in [
+            ("p3g_server_create", C.c_int, [C.c_int, u64p, C.c_uint32, C.c_uint64, C.POINTER(vp)]),
+            ("p3g_server_destroy", None, [vp]),
+            ("p3g_server_submit", C.c_int, [vp, C.POINTER(JobC), u64p]),
+            ("p3g_server_wait", C.c_int, [vp, C.c_uint64, C.POINTER(JobResultC)]),
+            ("p3g_server_run", C.c_int, [vp, C.POINTER(JobC), C.c_uint64, C.POINTER(JobResultC)]),
+            ("p3g_server_peak_admitted_bytes", C.c_uint64, [vp]),
+            ("p3g_job_footprint_bytes", C.c_uint64, [C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64]),
+        ]:
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        params = default_poseidon2_params() if poseidon2_params is None else np.ascontiguousarray(poseidon2_params, dtype=np.uint64)
+        self._h = C.c_void_p()
+        _check(L.p3g_server_create(device, _ptr(params), n_workers, int(hbm_budget), C.byref(self._h)))
+        self.n_workers = n_workers
+        self._pending = {}
+
+    def run(self, jobs: list[Job]) -> list[JobResult]:
+        """Submit every job at its arrival time (seconds from now) and wait for all."""
+        keep = []
+        arr = (JobC * max(1, len(jobs)))()
+        for i, j in enumerate(jobs):
+            ins = _instances_c(j.instances, keep)
+            arr[i] = JobC(j.pcs.as_c(), ins, len(j.instances), float(j.arrival_s))
+        res = (JobResultC * max(1, len(jobs)))()
+        _check(lib().p3g_server_run(self._h, arr, len(jobs), res))
+        return [_result_from_c(res[i]) for i in range(len(jobs))]
+
+    def submit(self, job: Job) -> int:
+        keep = []
+        ins = _instances_c(job.instances, keep)
+        jc = JobC(job.pcs.as_c(), ins, len(job.instances), 0.0)
+        t = C.c_uint64()
+        _check(lib().p3g_server_submit(self._h, C.byref(jc), C.byref(t)))
+        self._pending[t.value] = keep
+        return t.value
+
+    def wait(self, ticket: int) -> JobResult:
+        r = JobResultC()
+        lib().p3g_server_wait(self._h, ticket, C.byref(r))
+        self._pending.pop(ticket, None)
+        return _result_from_c(r)
+
+    def peak_admitted_bytes(self) -> int:
+        return int(lib().p3g_server_peak_admitted_bytes(self._h))
+
+    @staticmethod
+    def footprint_bytes(pcs: PcsParams, instances) -> int:
+        keep = []
+        ins = _instances_c(instances, keep)
+        pc = pcs.as_c()
+        return int(lib().p3g_job_footprint_bytes(C.byref(pc), ins, len(instances)))
+
+    def close(self):
+        if self._h:
+            lib().p3g_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -32,6 +32,16 @@ struct p3g_proof_c {
 
 namespace p3g {
 // Upload the Keccak round constants and rho offsets used by the constraint kernel.
+inline void upload_keccak_tables();
+inline void ensure_keccak_tables(int device) {
+    static std::mutex mu;
+    static bool done[64] = {false};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device >= 0 && device < 64 && !done[device]) {
+        upload_keccak_tables();
+        done[device] = true;
+    }
+}
 inline void upload_keccak_tables() {
     const keccak::Tables &T = keccak::tables();
     int rot[25];
@@ -85,11 +95,7 @@ P3G_API int p3g_prove(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instanc
     }
     try {
         CK(cudaSetDevice(x->c.device));
-        static bool tables = false;
-        if (!tables) {
-            p3g::upload_keccak_tables();
-            tables = true;
-        }
+        p3g::ensure_keccak_tables(x->c.device);
         std::vector<p3g::Instance> ins(n);
         for (uint64_t i = 0; i < n; i++)
             ins[i] = {inst[i].air, inst[i].trace_on_device, inst[i].height, inst[i].width, inst[i].trace, inst[i].consts,

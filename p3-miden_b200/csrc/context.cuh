@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -184,12 +185,11 @@ inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     uint32_t k = a.bhi - a.blo;
     dim3 grid((unsigned)(h >> k), (unsigned)((a.w + C - 1) / C));
     size_t smem = ((size_t(1) << k) * C + 512 + 16) * 8;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
         CK(cudaFuncSetAttribute(ntt::ntt_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (1024 * C + 512 + 16) * 8));
-        attr_set = true;
-    }
+    });
     ntt::ntt_pass_kernel<C, DIF><<<grid, 256, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;
@@ -200,12 +200,11 @@ inline void launch_pass_r8(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     dim3 grid((unsigned)((a.w + C - 1) / C), (unsigned)(h >> k));
     unsigned threads = (1u << (k - 3)) * C;
     size_t smem = ((size_t(1) << k) * C + (size_t(1) << k) + 16) * 8;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
         CK(cudaFuncSetAttribute(ntt::ntt_pass_r8_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (1024 * C + 1024 + 16) * 8));
-        attr_set = true;
-    }
+    });
     ntt::ntt_pass_r8_kernel<C, DIF><<<grid, threads, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;

@@ -230,12 +230,11 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         a.acc = acc.p;
         if (I.air == AIR_CUBIC) L(quot::cubic_eval_kernel, blocks_for(qh * 32, 256), 256, 0, a);
         else {
-            static bool attr = false;
-            if (!attr) {
+            static std::once_flag attr_once;
+            std::call_once(attr_once, [] {
                 CK(cudaFuncSetAttribute(quot::keccak_eval_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)quot::KEC_SMEM));
-                attr = true;
-            }
+            });
             int dev_sms = 148;
             CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx.device));
             uint64_t blocks = std::min<uint64_t>(qh, (uint64_t)dev_sms * 3);
@@ -422,11 +421,11 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             const uint64_t *cf = d_coef.p + 2 * off;
             if (m->w >= 16) {
                 size_t smem = 16 * m->w;
-                static bool attr = false;
-                if (!attr) {
-                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-                    attr = true;
-                }
+                static std::once_flag attr_once;
+                std::call_once(attr_once, [] {
+                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            200 * 1024));
+                });
                 unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(m->h * 32, 256), 148 * 16);
                 L(deep::rowdot_warp_kernel, grid, 256, smem, m->d, m->h, m->w, cf, dots[mi].p);
             } else {

@@ -101,7 +101,7 @@ __device__ __forceinline__ uint64_t kbool(uint64_t a) { return gl::mul(a, gl::su
 //   2910..3009 a2 limbs          3010..3077 a2[0][0] bits + limbs
 //   3078..3081 a3[0][0] limbs    3082..3181 output == next input (x outer)
 // (c2 = C', a1 = A', a2 = A'', a3 = A''' in the Keccak-f round notation.)
-constexpr int KEC_TASKS = 878;  // 200 heavy limb tasks, 8 small, 320 (x,z), 350 light
+constexpr int KEC_TASKS = 1502;  // 832 quarter-limb tasks, 320 (x,z), 350 light
 
 struct KFold {
     uint64_t c0 = 0, c1 = 0;
@@ -119,48 +119,55 @@ __device__ __forceinline__ uint64_t kbit_b(const uint64_t *L, int bx, int by, in
     return L[KC_AP + (bx * 5 + ax) * 64 + ((z + 64 - rot) & 63)];
 }
 
-// one task of one point; L, N in shared memory
+// one task of one point; L, N in shared memory. Limb equations are linear in
+// their bits, so a 16-bit limb is split into four 4-bit tasks that each add
+// alpha^k * (their part of the limb) to the fold; part 0 also subtracts
+// alpha^k * limb. All tasks then cost about the same.
 __device__ void keccak_task(int t, const uint64_t *L, const uint64_t *N, uint64_t first, uint64_t trans, KFold &f) {
     const uint64_t not_final = gl::sub(1, L[KC_STEP + 23]);
-    if (t < 100) {  // A limbs from xor(A1, C, C2), with the bools of A1
-        int o = t, y = o / 20, x = (o / 4) % 5, l = o % 4;
+    if (t < 400) {  // A limbs from xor(A1, C, C2), with the bools of A1
+        int o = t >> 2, part = t & 3, y = o / 20, x = (o / 4) % 5, l = o % 4;
         int base = 890 + 17 * o;
         uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
+        for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
             uint64_t ap = L[KC_AP + (y * 5 + x) * 64 + z];
             f.emit(base + (l * 16 + 15 - z), kbool(ap));
             acc = gl::add(gl::dbl(acc), kxor3(ap, L[KC_C + x * 64 + z], L[KC_CP + x * 64 + z]));
         }
-        f.emit(base + 16, gl::sub(acc, L[KC_A + o]));
-    } else if (t < 200) {  // A2 limbs: xor(B, andn(B[x+1], B[x+2]))
-        int o = t - 100, y = o / 20, x = (o / 4) % 5, l = o % 4;
+        acc = gl::mul(acc, 1ull << (4 * part));
+        f.emit(base + 16, part == 0 ? gl::sub(acc, L[KC_A + o]) : acc);
+    } else if (t < 800) {  // A2 limbs: xor(B, andn(B[x+1], B[x+2]))
+        int o = (t - 400) >> 2, part = t & 3, y = o / 20, x = (o / 4) % 5, l = o % 4;
         uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
+        for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
             uint64_t b0 = kbit_b(L, x, y, z), b1 = kbit_b(L, (x + 1) % 5, y, z), b2 = kbit_b(L, (x + 2) % 5, y, z);
             acc = gl::add(gl::dbl(acc), kxor2(b0, kandn(b1, b2)));
         }
-        f.emit(2910 + o, gl::sub(acc, L[KC_APP + o]));
-    } else if (t < 204) {  // A2[0][0] bits
-        int l = t - 200, base = 3010 + 17 * l;
+        acc = gl::mul(acc, 1ull << (4 * part));
+        f.emit(2910 + o, part == 0 ? gl::sub(acc, L[KC_APP + o]) : acc);
+    } else if (t < 816) {  // A2[0][0] bits
+        int l = (t - 800) >> 2, part = t & 3, base = 3010 + 17 * l;
         uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
+        for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
             uint64_t bit = L[KC_APP00 + z];
             f.emit(base + (l * 16 + 15 - z), kbool(bit));
             acc = gl::add(gl::dbl(acc), bit);
         }
-        f.emit(base + 16, gl::sub(acc, L[KC_APP + l]));
-    } else if (t < 208) {  // A3[0][0] = A2[0][0] xor RC
-        int l = t - 204;
+        acc = gl::mul(acc, 1ull << (4 * part));
+        f.emit(base + 16, part == 0 ? gl::sub(acc, L[KC_APP + l]) : acc);
+    } else if (t < 832) {  // A3[0][0] = A2[0][0] xor RC
+        int l = (t - 816) >> 2, part = t & 3;
         uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
+        for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
             uint64_t rcb = 0;
             for (int r = 0; r < 24; r++)
                 if ((c_keccak_rc[r] >> z) & 1) rcb = gl::add(rcb, L[KC_STEP + r]);
             acc = gl::add(gl::dbl(acc), kxor2(L[KC_APP00 + z], rcb));
         }
-        f.emit(3078 + l, gl::sub(acc, L[KC_APPP00 + l]));
-    } else if (t < 528) {  // (x, z): bool C, C2 xor, A1 column sum
-        int i = t - 208, x = i / 64, z = i % 64;
+        acc = gl::mul(acc, 1ull << (4 * part));
+        f.emit(3078 + l, part == 0 ? gl::sub(acc, L[KC_APPP00 + l]) : acc);
+    } else if (t < 1152) {  // (x, z): bool C, C2 xor, A1 column sum
+        int i = t - 832, x = i / 64, z = i % 64;
         uint64_t cxz = L[KC_C + i];
         f.emit(250 + 2 * i, kbool(cxz));
         uint64_t v = kxor3(cxz, L[KC_C + ((x + 4) % 5) * 64 + z], L[KC_C + ((x + 1) % 5) * 64 + ((z + 63) & 63)]);
@@ -170,24 +177,24 @@ __device__ void keccak_task(int t, const uint64_t *L, const uint64_t *N, uint64_
         for (int y = 0; y < 5; y++) sm = gl::add(sm, L[KC_AP + (y * 5 + x) * 64 + z]);
         uint64_t d = gl::sub(sm, cp);
         f.emit(2590 + i, gl::mul(gl::mul(d, gl::sub(d, 2)), gl::sub(d, 4)));
-    } else if (t < 552) {  // first-row flags
-        int i = t - 528;
+    } else if (t < 1176) {  // first-row flags
+        int i = t - 1152;
         f.emit(i, gl::mul(first, i == 0 ? gl::sub(L[KC_STEP], 1) : L[KC_STEP + i]));
-    } else if (t < 576) {  // flag rotation
-        int i = t - 552;
+    } else if (t < 1200) {  // flag rotation
+        int i = t - 1176;
         f.emit(24 + i, gl::mul(trans, gl::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
-    } else if (t < 676) {  // first step: preimage == a
-        int o = t - 576;
+    } else if (t < 1300) {  // first step: preimage == a
+        int o = t - 1200;
         f.emit(48 + o, gl::mul(L[KC_STEP], gl::sub(L[KC_PRE + o], L[KC_A + o])));
-    } else if (t < 678) {  // export
+    } else if (t < 1302) {  // export
         uint64_t ex = L[KC_EXPORT];
-        if (t == 676) f.emit(148, kbool(ex));
+        if (t == 1300) f.emit(148, kbool(ex));
         else f.emit(149, gl::mul(not_final, ex));
-    } else if (t < 778) {  // preimage continuity
-        int o = t - 678;
+    } else if (t < 1402) {  // preimage continuity
+        int o = t - 1302;
         f.emit(150 + o, gl::mul(gl::mul(not_final, trans), gl::sub(L[KC_PRE + o], N[KC_PRE + o])));
     } else {  // round output == next round input (x outer, y inner)
-        int i = t - 778, x = i / 20, y = (i / 4) % 5, l = i % 4;
+        int i = t - 1402, x = i / 20, y = (i / 4) % 5, l = i % 4;
         uint64_t outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
         f.emit(3082 + i, gl::mul(gl::mul(not_final, trans), gl::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
     }

@@ -1,0 +1,178 @@
+// Batched and served proving: a pool of workers on one device, each with its
+// own context (stream, twiddle cache), pulling jobs from one queue.
+//
+// Jobs are admitted in arrival order while their estimated HBM footprint
+// fits in the budget still free (a job is always admitted when nothing else
+// runs, so an oversized job cannot starve). A worker keeps its job's LDEs,
+// trees and FRI layers on the device for the whole proof; the device
+// interleaves the kernels of up to n_workers proofs, and one proof's host
+// work (transcript, challenges) overlaps the others' device work.
+// A failing job (validation or device error) reports its own status; the
+// other jobs are unaffected.
+#pragma once
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+
+#include "prover.cuh"
+
+namespace p3g {
+
+// Upper bound of the device bytes prove() allocates for a job.
+inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, size_t n) {
+    const uint64_t B = 1ull << pcs.log_blowup, D = 2;
+    uint64_t words = 0, max_hw = 0, hmax = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t hw = inst[i].height * inst[i].width;
+        if (!inst[i].trace_on_device) words += hw;  // uploaded trace
+        words += hw * B;                             // main LDE
+        words += inst[i].height * 2 * (B + 1);       // aux trace + LDE
+        max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, 2));
+        hmax = std::max(hmax, inst[i].height);
+    }
+    max_hw = std::max(max_hw, hmax * 2 * D);
+    const uint64_t nl = hmax * B;
+    words += max_hw;             // iNTT scratch
+    words += 2 * hmax * D;       // quotient accumulator
+    words += nl * 2 * D;         // quotient LDE
+    words += 4 * nl;             // DEEP point quotients
+    words += 4 * nl * 4;         // tree digest layers (3 trees + FRI), upper bound
+    words += 2 * nl * 3;         // DEEP row dots, layer, FRI layers
+    words += 4 * nl / B;         // barycentric weights
+    return words * 8 + (64ull << 20);  // plus tables and slack
+}
+
+struct ServerJob {
+    PcsParams pcs;
+    std::vector<Instance> inst;
+    double arrival_s = 0;  // seconds after serve() starts
+    // results
+    int status = -1;
+    ProofOut out;
+    double submit_s = 0, start_s = 0, end_s = 0;
+    std::string error;
+};
+
+class Server {
+   public:
+    Server(int device, const uint64_t *p2, uint32_t n_workers, uint64_t hbm_budget)
+        : device_(device), budget_(hbm_budget) {
+        CK(cudaSetDevice(device));
+        for (uint32_t w = 0; w < n_workers; w++) {
+            auto c = std::make_unique<Ctx>();
+            c->device = device;
+            CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            memcpy(c->p2, p2, sizeof(c->p2));
+            ctxs_.push_back(std::move(c));
+        }
+        CK(cudaMemcpyToSymbol(c_p2, p2, p2::N_PARAMS * 8));
+        t0_ = std::chrono::steady_clock::now();
+        for (uint32_t w = 0; w < n_workers; w++) workers_.emplace_back([this, w] { worker(w); });
+    }
+    ~Server() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : workers_) t.join();
+        for (auto &c : ctxs_) {
+            cudaStreamSynchronize(c->stream);
+            c->tw.clear();
+            c->t1024.reset();
+            cudaStreamSynchronize(c->stream);
+            if (c->pinned) cudaFreeHost(c->pinned);
+            cudaStreamDestroy(c->stream);
+            c->stream = nullptr;
+        }
+    }
+    double now_s() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+    }
+    // Enqueue a job; the caller keeps `job` (and its traces) alive until done.
+    void submit(ServerJob *job) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job->submit_s = now_s();
+            job->status = -1;
+            queue_.push_back(job);
+            pending_++;
+        }
+        cv_.notify_all();
+    }
+    void wait(ServerJob *job) {
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return job->status >= 0; });
+    }
+    void wait_all() {
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+    uint64_t peak_bytes() const { return peak_; }
+
+   private:
+    void worker(uint32_t w) {
+        cudaSetDevice(device_);
+        Ctx &ctx = *ctxs_[w];
+        for (;;) {
+            ServerJob *job = nullptr;
+            uint64_t fp = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] {
+                    if (stop_) return true;
+                    if (queue_.empty()) return false;
+                    uint64_t f = job_footprint_bytes(queue_.front()->pcs, queue_.front()->inst.data(),
+                                                     queue_.front()->inst.size());
+                    return in_use_ == 0 || in_use_ + f <= budget_;
+                });
+                if (stop_ && queue_.empty()) return;
+                if (queue_.empty()) continue;
+                job = queue_.front();
+                queue_.pop_front();
+                fp = job_footprint_bytes(job->pcs, job->inst.data(), job->inst.size());
+                in_use_ += fp;
+                peak_ = std::max(peak_, in_use_);
+            }
+            job->start_s = now_s();
+            int st = OK;
+            try {
+                prove(ctx, job->pcs, job->inst.data(), job->inst.size(), job->out);
+            } catch (const CudaError &e) {
+                st = e.status;
+                job->error = e.what;
+                cudaStreamSynchronize(ctx.stream);
+                cudaGetLastError();
+            } catch (const std::bad_alloc &) {
+                st = ERR_OOM;
+                job->error = "host allocation failed";
+            }
+            job->end_s = now_s();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                in_use_ -= fp;
+                job->status = st;
+                pending_--;
+            }
+            cv_.notify_all();
+            done_cv_.notify_all();
+        }
+    }
+
+    int device_;
+    uint64_t budget_;
+    std::vector<std::unique_ptr<Ctx>> ctxs_;
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::deque<ServerJob *> queue_;
+    uint64_t in_use_ = 0, peak_ = 0;
+    uint64_t pending_ = 0;
+    bool stop_ = false;
+    std::chrono::steady_clock::time_point t0_;
+};
+
+}  // namespace p3g
