@@ -51,14 +51,8 @@ P3G_API int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_
 P3G_API void p3g_ctx_destroy(p3g_ctx *x) {
     if (!x) return;
     cudaSetDevice(x->c.device);
-    cudaStreamSynchronize(x->c.stream);
-    // every stream-ordered buffer the context owns is freed before its stream
-    x->c.tw.clear();
-    x->c.t1024.reset();
-    cudaStreamSynchronize(x->c.stream);
-    if (x->c.pinned) cudaFreeHost(x->c.pinned);
-    cudaStreamDestroy(x->c.stream);
-    x->c.stream = nullptr;
+    // every stream-ordered buffer the context owns is freed before its streams
+    x->c.release();
     delete x;
 }
 

@@ -86,6 +86,27 @@ struct Ctx {
     size_t pinned_words = 0;
     uint64_t launches = 0;       // kernels launched by this context
     std::unique_ptr<Tw1024> t1024;
+    cudaStream_t lde_stream = nullptr, copy_stream = nullptr;  // main-commit pipeline
+
+    void pipeline_streams() {
+        if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
+        if (!copy_stream) CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    }
+    // free stream-ordered buffers, then the streams (used at teardown)
+    void release() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (lde_stream) cudaStreamSynchronize(lde_stream);
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
+        tw.clear();
+        t1024.reset();
+        if (stream) cudaStreamSynchronize(stream);
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        if (lde_stream) cudaStreamDestroy(lde_stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (stream) cudaStreamDestroy(stream);
+        lde_stream = copy_stream = stream = nullptr;
+    }
 
     const Tw1024 &tw1024() {
         if (!t1024) {
@@ -222,91 +243,125 @@ inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
     else launch_pass<8, DIF>(ctx, a, h);
 }
 
-// Bit-reversed coset LDE: in (h x w, row stride ld_in) -> out ((h<<lb) x w,
-// stride w). tmp must hold h*w words. If col_bases is non-empty, coefficient
-// k of base column col is additionally multiplied by col_bases[col/2]^k.
-inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h, uint64_t w, uint32_t log_blowup,
-                      uint64_t shift, uint64_t *d_out, uint64_t *d_tmp, const std::vector<uint64_t> &col_bases = {}) {
-    if (w == 0) return;
-    const uint32_t L = log2u(h);
-    const uint64_t B = 1ull << log_blowup;
-    const TwTables &tw = ctx.twiddles(L);
-    auto sizes = pass_sizes(L);
-    // inverse transform (DIT, ascending bit ranges)
-    {
-        uint32_t blo = 0;
-        for (size_t pi = 0; pi < sizes.size(); pi++) {
-            ntt::PassArgs a{};
-            a.src = pi == 0 ? d_in : d_tmp;
-            a.ld_src = pi == 0 ? ld_in : w;
-            a.dst = d_tmp;
-            a.ld_dst = w;
-            a.w = w;
-            a.L = L;
-            a.blo = blo;
-            a.bhi = blo + sizes[pi];
-            a.src_bitrev = pi == 0;
-            a.tw = ntt::PowTab{tw.inv_lo.p, tw.inv_hi.p, tw.lo_bits};
-            a.tw1024 = ctx.tw1024().inv.p;
-            a.has_scale = 0;
-            launch_pass_any<false>(ctx, a, h);
-            blo = a.bhi;
-        }
-    }
+// Bit-reversed coset LDE of an h x w matrix, split into a plan (tables on
+// the device; synchronises the context stream once) and launches (no host
+// synchronisation, any stream), so that column slabs of one trace can be
+// transformed while earlier slabs are hashed.
+struct LdePlan {
+    uint32_t L = 0, log_blowup = 0;
+    uint64_t h = 0;
+    std::vector<uint32_t> sizes;
+    const TwTables *tw = nullptr;
+    uint32_t scale_lo_bits = 0;
+    std::vector<DBuf> scale;  // per coset: lo table (with 1/h folded in), hi table
     DBuf colpow_lo, colpow_hi;
+    uint32_t colpow_lo_bits = 0;
+    uint64_t colpow_hi_len = 0;
+};
+
+// col_bases: if non-empty, coefficient k of base column col is also
+// multiplied by col_bases[col/2]^k (quotient chunks).
+inline LdePlan lde_plan(Ctx &ctx, uint64_t h, uint32_t log_blowup, uint64_t shift,
+                        const std::vector<uint64_t> &col_bases = {}) {
+    LdePlan p;
+    p.L = log2u(h);
+    p.h = h;
+    p.log_blowup = log_blowup;
+    p.tw = &ctx.twiddles(p.L);
+    p.sizes = pass_sizes(p.L);
+    p.scale_lo_bits = p.L < 12 ? p.L : 12;
+    const uint64_t wb = gl::root(p.L + log_blowup);
+    const uint64_t hinv = gl::inv(h % gl::P);
+    std::vector<uint64_t> lo, hi;
+    uint64_t sk = shift;
+    for (uint64_t k = 0; k < (1ull << log_blowup); k++) {
+        pow_table(sk, p.L, p.scale_lo_bits, lo, hi);
+        for (auto &v : lo) v = gl::mul(v, hinv);  // the inverse transform's 1/h
+        p.scale.push_back(ctx.upload(lo));
+        p.scale.push_back(ctx.upload(hi));
+        sk = gl::mul(sk, wb);
+    }
     if (!col_bases.empty()) {
-        uint32_t lo_bits = L < 10 ? L : 10;
-        size_t nlo = 1ull << lo_bits, nhi = 1ull << (L - lo_bits);
-        std::vector<uint64_t> all_lo, all_hi, lo, hi;
+        p.colpow_lo_bits = p.L < 10 ? p.L : 10;
+        p.colpow_hi_len = 1ull << (p.L - p.colpow_lo_bits);
+        std::vector<uint64_t> all_lo, all_hi;
         for (uint64_t cb : col_bases) {
-            pow_table(cb, L, lo_bits, lo, hi);
+            pow_table(cb, p.L, p.colpow_lo_bits, lo, hi);
             all_lo.insert(all_lo.end(), lo.begin(), lo.end());
             all_hi.insert(all_hi.end(), hi.begin(), hi.end());
         }
-        colpow_lo = ctx.upload(all_lo);
-        colpow_hi = ctx.upload(all_hi);
+        p.colpow_lo = ctx.upload(all_lo);
+        p.colpow_hi = ctx.upload(all_hi);
+    }
+    (void)ctx.tw1024();
+    return p;
+}
+
+// in: h x w (row stride ld_in) -> out: (h << log_blowup) x w (row stride
+// ld_out); tmp holds h * w words.
+inline void lde_run(Ctx &ctx, const LdePlan &p, const uint64_t *d_in, uint64_t ld_in, uint64_t w, uint64_t *d_out,
+                    uint64_t ld_out, uint64_t *d_tmp, cudaStream_t stream) {
+    if (w == 0) return;
+    cudaStream_t saved = ctx.stream;
+    ctx.stream = stream;  // launch helpers use ctx.stream
+    const uint32_t L = p.L;
+    const uint64_t h = p.h;
+    uint32_t blo = 0;
+    for (size_t pi = 0; pi < p.sizes.size(); pi++) {  // inverse transform (DIT, ascending bits)
+        ntt::PassArgs a{};
+        a.src = pi == 0 ? d_in : d_tmp;
+        a.ld_src = pi == 0 ? ld_in : w;
+        a.dst = d_tmp;
+        a.ld_dst = w;
+        a.w = w;
+        a.L = L;
+        a.blo = blo;
+        a.bhi = blo + p.sizes[pi];
+        a.src_bitrev = pi == 0;
+        a.tw = ntt::PowTab{p.tw->inv_lo.p, p.tw->inv_hi.p, p.tw->lo_bits};
+        a.tw1024 = ctx.t1024->inv.p;
+        a.has_scale = 0;
+        launch_pass_any<false>(ctx, a, h);
+        blo = a.bhi;
+    }
+    if (p.colpow_lo.p) {
         uint64_t n = h * w;
         ntt::scale_rows_by_colpow_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(
-            d_tmp, h, w, colpow_lo.p, colpow_hi.p, lo_bits, nhi);
+            d_tmp, h, w, p.colpow_lo.p, p.colpow_hi.p, p.colpow_lo_bits, p.colpow_hi_len);
         CK(cudaGetLastError());
         ctx.launches++;
-        (void)nlo;
     }
-    // forward transform per coset (DIF, descending bit ranges)
-    const uint64_t wb = gl::root(L + log_blowup);
-    const uint64_t hinv = gl::inv(h % gl::P);
-    uint32_t lo_bits = L < 12 ? L : 12;
-    std::vector<uint64_t> lo, hi;
-    std::vector<DBuf> keep;
-    uint64_t sk = shift;
-    for (uint64_t k = 0; k < B; k++) {
-        pow_table(sk, L, lo_bits, lo, hi);
-        for (auto &v : lo) v = gl::mul(v, hinv);  // the inverse transform's 1/h
-        DBuf dlo = ctx.upload(lo), dhi = ctx.upload(hi);
-        uint64_t *blk = d_out + gl::bitrev(k, log_blowup) * h * w;
+    for (uint64_t k = 0; k < (1ull << p.log_blowup); k++) {  // forward per coset (DIF, descending bits)
+        uint64_t *blk = d_out + gl::bitrev(k, p.log_blowup) * h * ld_out;
         uint32_t bhi = L;
-        for (size_t pi = 0; pi < sizes.size(); pi++) {
+        for (size_t pi = 0; pi < p.sizes.size(); pi++) {
             ntt::PassArgs a{};
             a.src = pi == 0 ? d_tmp : blk;
-            a.ld_src = w;
+            a.ld_src = pi == 0 ? w : ld_out;
             a.dst = blk;
-            a.ld_dst = w;
+            a.ld_dst = ld_out;
             a.w = w;
             a.L = L;
             a.bhi = bhi;
-            a.blo = bhi - sizes[pi];
+            a.blo = bhi - p.sizes[pi];
             a.src_bitrev = 0;
-            a.tw = ntt::PowTab{tw.fwd_lo.p, tw.fwd_hi.p, tw.lo_bits};
-            a.tw1024 = ctx.tw1024().fwd.p;
+            a.tw = ntt::PowTab{p.tw->fwd_lo.p, p.tw->fwd_hi.p, p.tw->lo_bits};
+            a.tw1024 = ctx.t1024->fwd.p;
             a.has_scale = pi == 0;
-            a.scale = ntt::PowTab{dlo.p, dhi.p, lo_bits};
+            a.scale = ntt::PowTab{p.scale[2 * k].p, p.scale[2 * k + 1].p, p.scale_lo_bits};
             launch_pass_any<true>(ctx, a, h);
             bhi = a.blo;
         }
-        keep.push_back(std::move(dlo));
-        keep.push_back(std::move(dhi));
-        sk = gl::mul(sk, wb);
     }
+    ctx.stream = saved;
+}
+
+// One-shot form on the context stream.
+inline void coset_lde(Ctx &ctx, const uint64_t *d_in, uint64_t ld_in, uint64_t h, uint64_t w, uint32_t log_blowup,
+                      uint64_t shift, uint64_t *d_out, uint64_t *d_tmp, const std::vector<uint64_t> &col_bases = {}) {
+    if (w == 0) return;
+    LdePlan p = lde_plan(ctx, h, log_blowup, shift, col_bases);
+    lde_run(ctx, p, d_in, ld_in, w, d_out, w, d_tmp, ctx.stream);
 }
 
 // ------------------------------------------------------------------ trees
@@ -374,6 +429,7 @@ inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t
         for (int m = 0; m < a.n_mats; m++) {
             a.data[m] = mats[launches[li].idx[m]].d;
             a.width[m] = mats[launches[li].idx[m]].w;
+            a.ld[m] = mats[launches[li].idx[m]].w;
         }
         a.log_h = log2u(launches[li].h);
         a.prev = prev;

@@ -133,6 +133,7 @@ constexpr int MAX_MATS = 8;
 struct ClassArgs {
     const uint64_t *data[MAX_MATS];
     uint64_t width[MAX_MATS];
+    uint64_t ld[MAX_MATS];  // row stride in words (>= width; a column slab of a wider matrix)
     int n_mats;
     uint32_t log_h;         // height of this class
     const uint64_t *prev;   // states of the previous class (12 words each), or null
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128) leaf_class_kernel(const __grid_constant__
 #pragma unroll
         for (int i = 0; i < 12; i++) s[i] = 0;
     }
-    for (int m = 0; m < a.n_mats; m++) absorb_row(s, a.data[m] + j * a.width[m], a.width[m]);
+    for (int m = 0; m < a.n_mats; m++) absorb_row(s, a.data[m] + j * a.ld[m], a.width[m]);
     if (a.digests_out) {
 #pragma unroll
         for (int i = 0; i < 4; i++) a.digests_out[j * 4 + i] = p2w::canon(s[i]);

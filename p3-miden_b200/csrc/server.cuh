@@ -79,15 +79,7 @@ class Server {
         }
         cv_.notify_all();
         for (auto &t : workers_) t.join();
-        for (auto &c : ctxs_) {
-            cudaStreamSynchronize(c->stream);
-            c->tw.clear();
-            c->t1024.reset();
-            cudaStreamSynchronize(c->stream);
-            if (c->pinned) cudaFreeHost(c->pinned);
-            cudaStreamDestroy(c->stream);
-            c->stream = nullptr;
-        }
+        for (auto &c : ctxs_) c->release();
     }
     double now_s() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
