@@ -37,6 +37,11 @@ PCS = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bi
            deep_pow_bits=0, num_queries=100, query_pow_bits=0)
 WORKLOAD = "keccak-f1600 AIR, 10922 perms -> 2^18 x 2633 Goldilocks trace, lifted STARK (Poseidon2-12 LMCS)"
 METRIC = "proofs/s"
+# DRAM bytes per algorithmic byte of the main-trace LDE, from the ncu capture
+# of every NTT launch of a 2^15-row LDE (dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the launches, divided by 8*w*N*(1+B));
+# traffic grows in proportion to the rows, so it scales to 2^18.
+LDE_TRAFFIC_PER_ALG_BYTE = 3.88
 
 
 def load_product():
@@ -274,7 +279,7 @@ def run_gpu(args):
         "dominant_stage": P.STAGES[dominant],
         "roofline": {"kernel": "coset LDE of the main trace (radix-8 NTT passes, column slabs)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": lde_bytes * 6 / 3 * 4 / 4 if False else None,
+                     "traffic": LDE_TRAFFIC_PER_ALG_BYTE * lde_bytes if LDE_TRAFFIC_PER_ALG_BYTE else None,
                      "algorithmic_bytes": lde_bytes, "kernel_ms": lde_ms,
                      "peak_source": "measured" if "hbm_gbs" in pk else "fallback"},
         "hash": {"kernel": "LMCS leaf sponge (Poseidon2-12)", "perms": perms,

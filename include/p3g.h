@@ -144,6 +144,43 @@ int p3g_coset_lde_noalloc(const uint64_t *d_in, uint64_t height, uint64_t width,
                           uint64_t *d_out, void *stream);
 uint64_t p3g_coset_lde_noalloc_max_words(void);
 
+/* ------------------------------------------- batched and served proving */
+/* No counterpart in the reference: a job queue in front of p3g_prove
+ * (prove_multi, p3-miden-lifted-stark/src/prover/mod.rs:223). n_workers
+ * workers on one device, each with its own stream and context, prove jobs
+ * concurrently; a job is admitted, in arrival order, when its device
+ * footprint (p3g_job_footprint_bytes) fits in what is left of
+ * hbm_budget_bytes, or when nothing else runs. Each job's proof is the one
+ * p3g_prove returns for it alone. Traces are borrowed until the job is
+ * awaited. */
+typedef struct p3g_server p3g_server;
+typedef struct {
+    p3g_pcs_params pcs;
+    const p3g_instance *instances;
+    uint64_t n_instances;
+    double arrival_s;  /* p3g_server_run: submit this many seconds after the call starts */
+} p3g_job;
+typedef struct {
+    int32_t status;    /* the job's own status; other jobs are unaffected by it */
+    int32_t pad;
+    p3g_proof proof;   /* valid when status == P3G_OK; release with p3g_proof_free */
+    double submit_s, start_s, end_s;
+} p3g_job_result;
+
+int p3g_server_create(int device, const uint64_t *poseidon2_params130, uint32_t n_workers,
+                      uint64_t hbm_budget_bytes, p3g_server **out);
+/* Waits for every submitted job, then releases the workers. */
+void p3g_server_destroy(p3g_server *srv);
+int p3g_server_submit(p3g_server *srv, const p3g_job *job, uint64_t *ticket);
+/* Blocks until the ticket's job ends; returns its status. */
+int p3g_server_wait(p3g_server *srv, uint64_t ticket, p3g_job_result *out);
+/* Submits each job at its arrival time, then waits for all; results[i]
+ * belongs to jobs[i]. Returns P3G_OK unless an argument is invalid. */
+int p3g_server_run(p3g_server *srv, const p3g_job *jobs, uint64_t n, p3g_job_result *results);
+uint64_t p3g_server_peak_admitted_bytes(const p3g_server *srv);
+/* Upper bound of the device bytes p3g_prove allocates for these instances. */
+uint64_t p3g_job_footprint_bytes(const p3g_pcs_params *pcs, const p3g_instance *instances, uint64_t n);
+
 /* ------------------------------------------------- caller-side helpers */
 /* generate_keccak_trace (p3-miden-lifted-examples/src/keccak.rs:54-56):
  * 2^log_height x 2633, n_perms * 24 <= 2^log_height. */
