@@ -13,6 +13,7 @@
 
 #include "gl.cuh"
 #include "merkle.cuh"
+#include "lde.cuh"
 #include "ntt.cuh"
 #include "poseidon2.cuh"
 
@@ -72,9 +73,6 @@ struct TwTables {
     DBuf fwd_lo, fwd_hi, inv_lo, inv_hi;
     uint32_t lo_bits;
 };
-struct Tw1024 {
-    DBuf fwd, inv;  // w_1024^j and w_1024^-j, j < 512
-};
 
 struct Ctx {
     int device = 0;
@@ -85,7 +83,6 @@ struct Ctx {
     uint64_t *pinned = nullptr;  // small pinned staging area
     size_t pinned_words = 0;
     uint64_t launches = 0;       // kernels launched by this context
-    std::unique_ptr<Tw1024> t1024;
     cudaStream_t lde_stream = nullptr, copy_stream = nullptr;  // main-commit pipeline
 
     void pipeline_streams() {
@@ -98,7 +95,6 @@ struct Ctx {
         if (lde_stream) cudaStreamSynchronize(lde_stream);
         if (copy_stream) cudaStreamSynchronize(copy_stream);
         tw.clear();
-        t1024.reset();
         if (stream) cudaStreamSynchronize(stream);
         if (pinned) cudaFreeHost(pinned);
         pinned = nullptr;
@@ -106,18 +102,6 @@ struct Ctx {
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
         lde_stream = copy_stream = stream = nullptr;
-    }
-
-    const Tw1024 &tw1024() {
-        if (!t1024) {
-            t1024 = std::make_unique<Tw1024>();
-            uint64_t w = gl::root(10), wi = gl::inv(w), x = 1, y = 1;
-            std::vector<uint64_t> a(512), b(512);
-            for (int j = 0; j < 512; j++) a[j] = x, b[j] = y, x = gl::mul(x, w), y = gl::mul(y, wi);
-            t1024->fwd = upload(a);
-            t1024->inv = upload(b);
-        }
-        return *t1024;
     }
 
     DBuf alloc(size_t words) {
@@ -201,48 +185,6 @@ inline std::vector<uint32_t> pass_sizes(uint32_t L) {
     return v;
 }
 
-template <int C, bool DIF>
-inline void launch_pass(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
-    uint32_t k = a.bhi - a.blo;
-    dim3 grid((unsigned)(h >> k), (unsigned)((a.w + C - 1) / C));
-    size_t smem = ((size_t(1) << k) * C + 512 + 16) * 8;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(ntt::ntt_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (1024 * C + 512 + 16) * 8));
-    });
-    ntt::ntt_pass_kernel<C, DIF><<<grid, 256, smem, ctx.stream>>>(a);
-    CK(cudaGetLastError());
-    ctx.launches++;
-}
-template <int C, bool DIF>
-inline void launch_pass_r8(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
-    uint32_t k = a.bhi - a.blo;
-    dim3 grid((unsigned)((a.w + C - 1) / C), (unsigned)(h >> k));
-    unsigned threads = (1u << (k - 3)) * C;
-    size_t smem = ((size_t(1) << k) * C + (size_t(1) << k) + 16) * 8;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(ntt::ntt_pass_r8_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (1024 * C + 1024 + 16) * 8));
-    });
-    ntt::ntt_pass_r8_kernel<C, DIF><<<grid, threads, smem, ctx.stream>>>(a);
-    CK(cudaGetLastError());
-    ctx.launches++;
-}
-template <bool DIF>
-inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
-    if (a.bhi - a.blo >= 3 && (h >> (a.bhi - a.blo)) <= 65535) {  // radix-8 register passes
-        if (a.w <= 2) launch_pass_r8<2, DIF>(ctx, a, h);
-        else if (a.w <= 4) launch_pass_r8<4, DIF>(ctx, a, h);
-        else launch_pass_r8<8, DIF>(ctx, a, h);
-        return;
-    }
-    if (a.w <= 2) launch_pass<2, DIF>(ctx, a, h);
-    else if (a.w <= 4) launch_pass<4, DIF>(ctx, a, h);
-    else launch_pass<8, DIF>(ctx, a, h);
-}
-
 // Bit-reversed coset LDE of an h x w matrix, split into a plan (tables on
 // the device; synchronises the context stream once) and launches (no host
 // synchronisation, any stream), so that column slabs of one trace can be
@@ -250,10 +192,11 @@ inline void launch_pass_any(Ctx &ctx, const ntt::PassArgs &a, uint64_t h) {
 struct LdePlan {
     uint32_t L = 0, log_blowup = 0;
     uint64_t h = 0;
-    std::vector<uint32_t> sizes;
+    std::vector<uint32_t> sizes;  // bit ranges, ascending
     const TwTables *tw = nullptr;
     uint32_t scale_lo_bits = 0;
-    std::vector<DBuf> scale;  // per coset: lo table (with 1/h folded in), hi table
+    uint64_t scale_hi_len = 0;
+    DBuf scale_lo, scale_hi;  // every coset's two-level table of (s*w_{hB}^c)^i / h
     DBuf colpow_lo, colpow_hi;
     uint32_t colpow_lo_bits = 0;
     uint64_t colpow_hi_len = 0;
@@ -272,19 +215,22 @@ inline LdePlan lde_plan(Ctx &ctx, uint64_t h, uint32_t log_blowup, uint64_t shif
     p.scale_lo_bits = p.L < 12 ? p.L : 12;
     const uint64_t wb = gl::root(p.L + log_blowup);
     const uint64_t hinv = gl::inv(h % gl::P);
-    std::vector<uint64_t> lo, hi;
+    std::vector<uint64_t> lo, hi, all_lo, all_hi;
     uint64_t sk = shift;
     for (uint64_t k = 0; k < (1ull << log_blowup); k++) {
         pow_table(sk, p.L, p.scale_lo_bits, lo, hi);
         for (auto &v : lo) v = gl::mul(v, hinv);  // the inverse transform's 1/h
-        p.scale.push_back(ctx.upload(lo));
-        p.scale.push_back(ctx.upload(hi));
+        all_lo.insert(all_lo.end(), lo.begin(), lo.end());
+        all_hi.insert(all_hi.end(), hi.begin(), hi.end());
+        p.scale_hi_len = hi.size();
         sk = gl::mul(sk, wb);
     }
+    p.scale_lo = ctx.upload(all_lo);
+    p.scale_hi = ctx.upload(all_hi);
     if (!col_bases.empty()) {
         p.colpow_lo_bits = p.L < 10 ? p.L : 10;
         p.colpow_hi_len = 1ull << (p.L - p.colpow_lo_bits);
-        std::vector<uint64_t> all_lo, all_hi;
+        all_lo.clear(), all_hi.clear();
         for (uint64_t cb : col_bases) {
             pow_table(cb, p.L, p.colpow_lo_bits, lo, hi);
             all_lo.insert(all_lo.end(), lo.begin(), lo.end());
@@ -293,65 +239,115 @@ inline LdePlan lde_plan(Ctx &ctx, uint64_t h, uint32_t log_blowup, uint64_t shif
         p.colpow_lo = ctx.upload(all_lo);
         p.colpow_hi = ctx.upload(all_hi);
     }
-    (void)ctx.tw1024();
     return p;
 }
 
+template <int C, bool DIF>
+inline void launch_lde_pass(Ctx &ctx, const lde::PassArgs &a, uint64_t groups, unsigned n_blocks_y) {
+    const uint32_t G = 1u << a.k;
+    const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
+    const size_t smem = ((size_t)G * C + G) * 8;
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
+        CK(cudaFuncSetAttribute(lde::lde_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (1024 * C + 1024) * 8));
+    });
+    lde::lde_pass_kernel<C, DIF><<<dim3((unsigned)(groups * a.n_tiles), n_blocks_y), threads, smem, ctx.stream>>>(a);
+    CK(cudaGetLastError());
+    ctx.launches++;
+}
+template <int C>
+inline void launch_lde_fused(Ctx &ctx, const lde::FusedArgs &a, uint64_t groups) {
+    const uint32_t G = 1u << a.k;
+    const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
+    const size_t smem = (2 * (size_t)G * C + 3 * (size_t)G) * 8;
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
+        CK(cudaFuncSetAttribute(lde::lde_fused_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (2 * 1024 * C + 3 * 1024) * 8));
+    });
+    lde::lde_fused_kernel<C><<<(unsigned)(groups * a.n_tiles), threads, smem, ctx.stream>>>(a);
+    CK(cudaGetLastError());
+    ctx.launches++;
+}
+template <bool DIF>
+inline void launch_lde_pass_any(Ctx &ctx, uint32_t C, const lde::PassArgs &a, uint64_t groups, unsigned ny) {
+    if (C == 2) launch_lde_pass<2, DIF>(ctx, a, groups, ny);
+    else if (C == 4) launch_lde_pass<4, DIF>(ctx, a, groups, ny);
+    else launch_lde_pass<8, DIF>(ctx, a, groups, ny);
+}
+
 // in: h x w (row stride ld_in) -> out: (h << log_blowup) x w (row stride
-// ld_out); tmp holds h * w words.
+// ld_out); tmp holds h * w words (used when h > 2^10).
 inline void lde_run(Ctx &ctx, const LdePlan &p, const uint64_t *d_in, uint64_t ld_in, uint64_t w, uint64_t *d_out,
                     uint64_t ld_out, uint64_t *d_tmp, cudaStream_t stream) {
     if (w == 0) return;
     cudaStream_t saved = ctx.stream;
     ctx.stream = stream;  // launch helpers use ctx.stream
-    const uint32_t L = p.L;
+    const uint32_t L = p.L, n = (uint32_t)p.sizes.size();
     const uint64_t h = p.h;
-    uint32_t blo = 0;
-    for (size_t pi = 0; pi < p.sizes.size(); pi++) {  // inverse transform (DIT, ascending bits)
-        ntt::PassArgs a{};
-        a.src = pi == 0 ? d_in : d_tmp;
-        a.ld_src = pi == 0 ? ld_in : w;
+    const uint32_t C = w <= 2 ? 2 : w <= 4 ? 4 : 8;
+    const uint32_t n_tiles = (uint32_t)((w + C - 1) / C);
+    const ntt::PowTab inv{p.tw->inv_lo.p, p.tw->inv_hi.p, p.tw->lo_bits};
+    const ntt::PowTab fwd{p.tw->fwd_lo.p, p.tw->fwd_hi.p, p.tw->lo_bits};
+    std::vector<uint32_t> blo(n, 0);
+    for (uint32_t i = 1; i < n; i++) blo[i] = blo[i - 1] + p.sizes[i - 1];
+    for (uint32_t i = 0; i + 1 < n; i++) {  // inverse transform, low ranges
+        lde::PassArgs a{};
+        a.src = i == 0 ? d_in : d_tmp;
+        a.ld_src = i == 0 ? ld_in : w;
         a.dst = d_tmp;
         a.ld_dst = w;
         a.w = w;
         a.L = L;
-        a.blo = blo;
-        a.bhi = blo + p.sizes[pi];
-        a.src_bitrev = pi == 0;
-        a.tw = ntt::PowTab{p.tw->inv_lo.p, p.tw->inv_hi.p, p.tw->lo_bits};
-        a.tw1024 = ctx.t1024->inv.p;
-        a.has_scale = 0;
-        launch_pass_any<false>(ctx, a, h);
-        blo = a.bhi;
+        a.blo = blo[i];
+        a.k = p.sizes[i];
+        a.n_tiles = n_tiles;
+        a.src_bitrev = i == 0;
+        a.root = inv;
+        launch_lde_pass_any<false>(ctx, C, a, h >> a.k, 1);
     }
-    if (p.colpow_lo.p) {
-        uint64_t n = h * w;
-        ntt::scale_rows_by_colpow_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(
-            d_tmp, h, w, p.colpow_lo.p, p.colpow_hi.p, p.colpow_lo_bits, p.colpow_hi_len);
-        CK(cudaGetLastError());
-        ctx.launches++;
+    {  // top range: inverse, then every coset's scale and forward range
+        lde::FusedArgs f{};
+        f.src = n == 1 ? d_in : d_tmp;
+        f.ld_src = n == 1 ? ld_in : w;
+        f.src_bitrev = n == 1;
+        f.dst = d_out;
+        f.ld_dst = ld_out;
+        f.w = w;
+        f.L = L;
+        f.blo = blo[n - 1];
+        f.k = p.sizes[n - 1];
+        f.n_tiles = n_tiles;
+        f.log_cosets = p.log_blowup;
+        f.inv_root = inv;
+        f.fwd_root = fwd;
+        f.scale_lo = p.scale_lo.p;
+        f.scale_hi = p.scale_hi.p;
+        f.scale_lo_bits = p.scale_lo_bits;
+        f.scale_hi_len = p.scale_hi_len;
+        f.cp_lo = p.colpow_lo.p;
+        f.cp_hi = p.colpow_hi.p;
+        f.cp_lo_bits = p.colpow_lo_bits;
+        f.cp_hi_len = p.colpow_hi_len;
+        if (C == 2) launch_lde_fused<2>(ctx, f, h >> f.k);
+        else if (C == 4) launch_lde_fused<4>(ctx, f, h >> f.k);
+        else launch_lde_fused<8>(ctx, f, h >> f.k);
     }
-    for (uint64_t k = 0; k < (1ull << p.log_blowup); k++) {  // forward per coset (DIF, descending bits)
-        uint64_t *blk = d_out + gl::bitrev(k, p.log_blowup) * h * ld_out;
-        uint32_t bhi = L;
-        for (size_t pi = 0; pi < p.sizes.size(); pi++) {
-            ntt::PassArgs a{};
-            a.src = pi == 0 ? d_tmp : blk;
-            a.ld_src = pi == 0 ? w : ld_out;
-            a.dst = blk;
-            a.ld_dst = ld_out;
-            a.w = w;
-            a.L = L;
-            a.bhi = bhi;
-            a.blo = bhi - p.sizes[pi];
-            a.src_bitrev = 0;
-            a.tw = ntt::PowTab{p.tw->fwd_lo.p, p.tw->fwd_hi.p, p.tw->lo_bits};
-            a.tw1024 = ctx.t1024->fwd.p;
-            a.has_scale = pi == 0;
-            a.scale = ntt::PowTab{p.scale[2 * k].p, p.scale[2 * k + 1].p, p.scale_lo_bits};
-            launch_pass_any<true>(ctx, a, h);
-            bhi = a.blo;
-        }
+    for (int i = (int)n - 2; i >= 0; i--) {  // forward transform, low ranges, every coset
+        lde::PassArgs a{};
+        a.src = d_out;
+        a.dst = d_out;
+        a.ld_src = a.ld_dst = ld_out;
+        a.src_blk = a.dst_blk = h * ld_out;
+        a.w = w;
+        a.L = L;
+        a.blo = blo[i];
+        a.k = p.sizes[i];
+        a.n_tiles = n_tiles;
+        a.src_bitrev = 0;
+        a.root = fwd;
+        launch_lde_pass_any<true>(ctx, C, a, h >> a.k, 1u << p.log_blowup);
     }
     ctx.stream = saved;
 }

@@ -83,16 +83,17 @@ __global__ void __launch_bounds__(256) colsum_kernel(const uint64_t *M, uint64_t
     const uint64_t col = (uint64_t)blockIdx.x * 32 + cl;
     const uint64_t r0 = (uint64_t)blockIdx.y * rows_per_chunk;
     const uint64_t r1 = min(d, r0 + rows_per_chunk);
-    uint64_t s[4] = {0, 0, 0, 0};
+    gl::Acc acc[4];
     if (col < w) {
         for (uint64_t i = r0 + rl; i < r1; i += 8) {
             uint64_t v = __ldg(M + i * w + col);
 #pragma unroll
-            for (int k = 0; k < 4; k++) s[k] = gl::add(s[k], gl::mul(v, __ldg(W + 4 * i + k)));
+            for (int k = 0; k < 4; k++) acc[k].mac(v, __ldg(W + 4 * i + k));
         }
     }
+    uint64_t s[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) red[rl][cl][k] = s[k];
+    for (int k = 0; k < 4; k++) red[rl][cl][k] = s[k] = acc[k].reduce();
     __syncthreads();
     if (rl == 0 && col < w) {
         for (int r = 1; r < 8; r++)
@@ -129,12 +130,13 @@ __global__ void __launch_bounds__(256) rowdot_warp_kernel(const uint64_t *M, uin
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < h; i += warps) {
         const uint64_t *row = M + i * w;
-        uint64_t c0 = 0, c1 = 0;
+        gl::Acc a0, a1;
         for (uint64_t col = lane; col < w; col += 32) {
             uint64_t v = __ldg(row + col);
-            c0 = gl::add(c0, gl::mul(v, sc[2 * col]));
-            c1 = gl::add(c1, gl::mul(v, sc[2 * col + 1]));
+            a0.mac(v, sc[2 * col]);
+            a1.mac(v, sc[2 * col + 1]);
         }
+        uint64_t c0 = a0.reduce(), c1 = a1.reduce();
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
             c0 = gl::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
@@ -151,14 +153,14 @@ __global__ void rowdot_thread_kernel(const uint64_t *M, uint64_t h, uint64_t w, 
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= h) return;
     const uint64_t *row = M + i * w;
-    uint64_t c0 = 0, c1 = 0;
+    gl::Acc a0, a1;
     for (uint64_t col = 0; col < w; col++) {
         uint64_t v = __ldg(row + col);
-        c0 = gl::add(c0, gl::mul(v, __ldg(coef + 2 * col)));
-        c1 = gl::add(c1, gl::mul(v, __ldg(coef + 2 * col + 1)));
+        a0.mac(v, __ldg(coef + 2 * col));
+        a1.mac(v, __ldg(coef + 2 * col + 1));
     }
-    dots[2 * i] = c0;
-    dots[2 * i + 1] = c1;
+    dots[2 * i] = a0.reduce();
+    dots[2 * i + 1] = a1.reduce();
 }
 
 constexpr int MAX_DOTS = 24;

@@ -19,15 +19,70 @@ constexpr uint64_t EPS = 0xFFFFFFFFULL;  // 2^64 mod p
 constexpr uint64_t W = 7;                // EF non-residue
 constexpr uint64_t GEN = 7;              // multiplicative generator
 
+#if defined(__CUDACC__)
+// Device forms on 32-bit carry chains: no 64-bit compares or selects on the
+// carries. Inputs and outputs as the host forms below.
+__device__ __forceinline__ uint64_t add_dev(uint64_t a, uint64_t b) {  // a, b < p
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 t0, t1, c;\n\t.reg .pred q;\n\t"
+        "add.cc.u32 %0, %2, %4;\n\t"
+        "addc.cc.u32 %1, %3, %5;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "add.cc.u32 t0, %0, 0xFFFFFFFF;\n\t"  // sum + eps = sum - p (mod 2^64)
+        "addc.cc.u32 t1, %1, 0;\n\t"
+        "addc.u32 c, c, 0;\n\t"                // sum >= 2^64 or sum >= p (never both)
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.b32 %0, t0, %0, q;\n\t"
+        "selp.b32 %1, t1, %1, q;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+// b < p: a - b mod p, below p when a < p, below 2^64 (weak) when a < 2^64
+__device__ __forceinline__ uint64_t sub_dev(uint64_t a, uint64_t b) {
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32 m, 0, 0;\n\t"    // borrow: 0xFFFFFFFF = eps
+        "sub.cc.u32 %0, %0, m;\n\t"  // a - b + 2^64 - eps = a - b + p
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+// x < 2^64 -> x mod p (x >= p iff x + eps carries)
+__device__ __forceinline__ uint64_t canon_dev(uint64_t x) {
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 t0, t1, c;\n\t.reg .pred q;\n\t"
+        "add.cc.u32 t0, %2, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 t1, %3, 0;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.b32 %0, t0, %2, q;\n\t"
+        "selp.b32 %1, t1, %3, q;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+#endif
 GL_HD uint64_t add(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return add_dev(a, b);
+#else
     uint64_t r = a + b;
     if (r < a || r >= P) r -= P;
     return r;
+#endif
 }
 GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return sub_dev(a, b);
+#else
     uint64_t r = a - b;
     if (a < b) r += P;
     return r;
+#endif
 }
 GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
 GL_HD uint64_t dbl(uint64_t a) { return add(a, a); }
@@ -51,45 +106,102 @@ GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
     return r;
 }
 #if defined(__CUDACC__)
-// 64x64 -> 128 product by 32-bit partial products on carry chains, then the
-// reduction 2^64 = 2^32 - 1, 2^96 = -1 on the same chains. The result is
-// weakly reduced: below 2^64 and congruent mod p (not necessarily < p).
-__device__ __forceinline__ uint64_t mul_weak(uint64_t a, uint64_t b) {
-    uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-    uint32_t r0, r1, r2, r3, t, ul, uh;
-    asm("mul.lo.u32 %0, %7, %9;\n\t"
-        "mul.hi.u32 %1, %7, %9;\n\t"
-        "mad.lo.cc.u32 %1, %7, %10, %1;\n\t"
-        "madc.hi.u32 %2, %7, %10, 0;\n\t"
-        "mad.lo.cc.u32 %1, %8, %9, %1;\n\t"
-        "madc.hi.cc.u32 %2, %8, %9, %2;\n\t"
-        "madc.hi.u32 %3, %8, %10, 0;\n\t"
-        "mad.lo.cc.u32 %2, %8, %10, %2;\n\t"
-        "addc.u32 %3, %3, 0;\n\t"
-        // (r1:r0) - r3, on borrow subtract eps
-        "sub.cc.u32 %0, %0, %3;\n\t"
-        "subc.cc.u32 %1, %1, 0;\n\t"
-        "subc.u32 %4, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, %4;\n\t"
+// r0 + r1*2^32 + r2*2^64 + r3*2^96 -> a value below 2^64 congruent mod p
+// (weakly reduced), with 2^64 = 2^32 - 1 and 2^96 = -1: (r1:r0) - r3 + r2*eps.
+__device__ __forceinline__ uint64_t reduce4_dev(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+    uint32_t o0, o1;
+    asm("{\n\t.reg .u32 m, u0, u1;\n\t"
+        "sub.cc.u32 %0, %2, %5;\n\t"
+        "subc.cc.u32 %1, %3, 0;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"  // on borrow subtract eps
         "subc.u32 %1, %1, 0;\n\t"
-        // + r2 * eps = (r2 << 32) - r2, on carry add eps
-        "sub.cc.u32 %5, 0, %2;\n\t"
-        "subc.u32 %6, %2, 0;\n\t"
-        "add.cc.u32 %0, %0, %5;\n\t"
-        "addc.cc.u32 %1, %1, %6;\n\t"
-        "addc.u32 %4, 0, 0;\n\t"
-        "neg.s32 %4, %4;\n\t"
-        "add.cc.u32 %0, %0, %4;\n\t"
-        "addc.u32 %1, %1, 0;"
-        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3), "=&r"(t), "=&r"(ul), "=&r"(uh)
-        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-    return ((uint64_t)r1 << 32) | r0;
+        "sub.cc.u32 u0, 0, %4;\n\t"   // r2*eps = (r2 << 32) - r2
+        "subc.u32 u1, %4, 0;\n\t"
+        "add.cc.u32 %0, %0, u0;\n\t"
+        "addc.cc.u32 %1, %1, u1;\n\t"
+        "addc.u32 m, 0, 0;\n\t"
+        "neg.s32 m, m;\n\t"            // on carry add eps
+        "add.cc.u32 %0, %0, m;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(o0), "=&r"(o1)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    return ((uint64_t)o1 << 32) | o0;
 }
+// 64x64 -> 128 product by 32-bit partial products on carry chains.
+__device__ __forceinline__ void mul128_dev(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2,
+                                           uint32_t &r3) {
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+}
+// a*b for a, b < 2^64, weakly reduced.
+__device__ __forceinline__ uint64_t mul_weak(uint64_t a, uint64_t b) {
+    uint32_t r0, r1, r2, r3;
+    mul128_dev(a, b, r0, r1, r2, r3);
+    return reduce4_dev(r0, r1, r2, r3);
+}
+// a*b + c for a, b, c < 2^64 (below 2^128), weakly reduced.
+__device__ __forceinline__ uint64_t mul_add_weak(uint64_t a, uint64_t b, uint64_t c) {
+    uint32_t r0, r1, r2, r3;
+    mul128_dev(a, b, r0, r1, r2, r3);
+    asm("add.cc.u32 %0, %0, %4;\n\t"
+        "addc.cc.u32 %1, %1, %5;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
+        : "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
+    return reduce4_dev(r0, r1, r2, r3);
+}
+#endif
+#if defined(__CUDACC__)
+// Lazy sum of products: sum a_i * b_i held in 160 bits (r4 counts the
+// overflows past 2^128, so up to 2^32 products), reduced once.
+struct Acc {
+    uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
+    __device__ __forceinline__ void mac(uint64_t a, uint64_t b) {  // += a*b, a, b < 2^64
+        asm("mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
+            "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
+            "madc.lo.cc.u32 %2, %6, %8, %2;\n\t"
+            "madc.hi.cc.u32 %3, %6, %8, %3;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            "mad.lo.cc.u32 %1, %5, %8, %1;\n\t"
+            "madc.hi.cc.u32 %2, %5, %8, %2;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            "mad.lo.cc.u32 %1, %6, %7, %1;\n\t"
+            "madc.hi.cc.u32 %2, %6, %7, %2;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.u32 %4, %4, 0;"
+            : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(r4)
+            : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    }
+    __device__ __forceinline__ void add(uint64_t a) {  // += a, a < 2^64
+        asm("add.cc.u32 %0, %0, %5;\n\t"
+            "addc.cc.u32 %1, %1, %6;\n\t"
+            "addc.cc.u32 %2, %2, 0;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.u32 %4, %4, 0;"
+            : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(r4)
+            : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)));
+    }
+    // canonical value: 2^128 = -2^32 (mod p), and r4 * 2^32 < p
+    __device__ __forceinline__ uint64_t reduce() const {
+        return sub_dev(canon_dev(reduce4_dev(r0, r1, r2, r3)), (uint64_t)r4 << 32);
+    }
+};
 #endif
 GL_HD uint64_t mul(uint64_t a, uint64_t b) {
 #if defined(__CUDA_ARCH__)
-    uint64_t r = mul_weak(a, b);
-    return r >= P ? r - P : r;
+    return canon_dev(mul_weak(a, b));
 #else
     return reduce128(mulhi(a, b), a * b);
 #endif

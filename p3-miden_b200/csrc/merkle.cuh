@@ -33,43 +33,58 @@ struct W {  // lo + hi * 2^64
     uint64_t lo;
     uint32_t hi;
 };
-__device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo) {
-    uint64_t hh = hi >> 32, hl = hi & EPS;
-    uint64_t t = lo - hh;
-    if (lo < hh) t -= EPS;
-    uint64_t u = hl * EPS;
-    uint64_t r = t + u;
-    if (r < u) r += EPS;
-    return r;
-}
 __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return gl::mul_weak(a, b); }
-__device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= gl::P ? a - gl::P : a; }
-// weak + canonical: one wrap at most
+__device__ __forceinline__ uint64_t canon(uint64_t a) { return gl::canon_dev(a); }
+// weak + canonical: one wrap at most (a + c - 2^64 + eps < 2^64)
 __device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t c) {
-    uint64_t s = a + c;
-    if (s < c) s += EPS;
-    return s;
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 k;\n\t"
+        "add.cc.u32 %0, %2, %4;\n\t"
+        "addc.cc.u32 %1, %3, %5;\n\t"
+        "addc.u32 k, 0, 0;\n\t"
+        "neg.s32 k, k;\n\t"
+        "add.cc.u32 %0, %0, k;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
 }
 __device__ __forceinline__ W wide(uint64_t a) { return W{a, 0}; }
 __device__ __forceinline__ W wadd(W a, W b) {
-    W r;
-    r.lo = a.lo + b.lo;
-    r.hi = a.hi + b.hi + (r.lo < a.lo ? 1u : 0u);
-    return r;
+    uint32_t r0, r1, h;
+    asm("add.cc.u32 %0, %3, %6;\n\t"
+        "addc.cc.u32 %1, %4, %7;\n\t"
+        "addc.u32 %2, %5, %8;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(h)
+        : "r"((uint32_t)a.lo), "r"((uint32_t)(a.lo >> 32)), "r"(a.hi), "r"((uint32_t)b.lo),
+          "r"((uint32_t)(b.lo >> 32)), "r"(b.hi));
+    return W{((uint64_t)r1 << 32) | r0, h};
 }
 __device__ __forceinline__ W wadd1(W a, uint64_t b) {
-    W r;
-    r.lo = a.lo + b;
-    r.hi = a.hi + (r.lo < b ? 1u : 0u);
-    return r;
+    uint32_t r0, r1, h;
+    asm("add.cc.u32 %0, %3, %6;\n\t"
+        "addc.cc.u32 %1, %4, %7;\n\t"
+        "addc.u32 %2, %5, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(h)
+        : "r"((uint32_t)a.lo), "r"((uint32_t)(a.lo >> 32)), "r"(a.hi), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return W{((uint64_t)r1 << 32) | r0, h};
 }
-__device__ __forceinline__ W wdbl(uint64_t a) { return W{a << 1, (uint32_t)(a >> 63)}; }
-// lo + hi * 2^64 with hi < 2^32: lo + hi * EPS, one wrap at most
+__device__ __forceinline__ W wdbl(uint64_t a) { return wadd1(wide(a), a); }
+// lo + hi * 2^64 with hi < 2^32: lo + hi * eps, one wrap at most
 __device__ __forceinline__ uint64_t wreduce(W a) {
-    uint64_t u = (uint64_t)a.hi * EPS;
-    uint64_t r = a.lo + u;
-    if (r < u) r += EPS;
-    return r;
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 u0, u1, c;\n\t"
+        "sub.cc.u32 u0, 0, %4;\n\t"  // hi*eps = (hi << 32) - hi
+        "subc.u32 u1, %4, 0;\n\t"
+        "add.cc.u32 %0, %2, u0;\n\t"
+        "addc.cc.u32 %1, %3, u1;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"          // on carry add eps
+        "add.cc.u32 %0, %0, c;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)a.lo), "r"((uint32_t)(a.lo >> 32)), "r"(a.hi));
+    return ((uint64_t)r1 << 32) | r0;
 }
 __device__ __forceinline__ uint64_t sbox(uint64_t x) {
     uint64_t x2 = mul(x, x), x4 = mul(x2, x2), x3 = mul(x2, x);
@@ -115,13 +130,7 @@ __device__ __forceinline__ void p2_permute_dev(uint64_t *s) {
             for (int i = 1; i < 12; i++) acc = p2w::wadd1(acc, s[i]);
             const uint64_t sum = p2w::wreduce(acc);
 #pragma unroll
-            for (int i = 0; i < 12; i++) {
-                const uint64_t d = c_p2[p2::OFF_DIAG + i];
-                uint64_t lo = s[i] * d, hi = __umul64hi(s[i], d);
-                lo += sum;
-                hi += (lo < sum) ? 1 : 0;  // no overflow: hi <= 2^64 - 2 for a 64x64 product
-                s[i] = p2w::reduce128(hi, lo);
-            }
+            for (int i = 0; i < 12; i++) s[i] = gl::mul_add_weak(s[i], c_p2[p2::OFF_DIAG + i], sum);
         }
     }
 }

@@ -57,15 +57,16 @@ __global__ void __launch_bounds__(256) cubic_eval_kernel(const __grid_constant__
     const uint64_t m = warp;
     const uint64_t *L = a.lde + gl::bitrev(m, a.log_qh) * a.w;
     const uint64_t *N = a.lde + gl::bitrev((m + a.D) & (qh - 1), a.log_qh) * a.w;
-    uint64_t c0 = 0, c1 = 0;
+    gl::Acc a0, a1;
     for (uint64_t i = lane; i < a.w; i += 32) {
         uint64_t x = __ldg(L + i);
         uint64_t y = __ldg(L + (i + 1 == a.w ? 0 : i + 1));
         uint64_t rhs = gl::add(gl::add(gl::mul(gl::sqr(x), x), y), __ldg(a.consts + i));
         uint64_t v = gl::sub(__ldg(N + i), rhs);
-        c0 = gl::add(c0, gl::mul(v, __ldg(a.alpha_pows + 2 * i)));
-        c1 = gl::add(c1, gl::mul(v, __ldg(a.alpha_pows + 2 * i + 1)));
+        a0.mac(v, __ldg(a.alpha_pows + 2 * i));
+        a1.mac(v, __ldg(a.alpha_pows + 2 * i + 1));
     }
+    uint64_t c0 = a0.reduce(), c1 = a1.reduce();
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
         c0 = gl::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
@@ -104,12 +105,12 @@ __device__ __forceinline__ uint64_t kbool(uint64_t a) { return gl::mul(a, gl::su
 constexpr int KEC_TASKS = 1502;  // 832 quarter-limb tasks, 320 (x,z), 350 light
 
 struct KFold {
-    uint64_t c0 = 0, c1 = 0;
+    gl::Acc c0, c1;  // lazy sums of v * alpha^(K-1-k), reduced once per point
     const uint64_t *ap;
     __device__ __forceinline__ explicit KFold(const uint64_t *a) : ap(a) {}
     __device__ __forceinline__ void emit(int k, uint64_t v) {
-        c0 = gl::add(c0, gl::mul(v, __ldg(ap + 2 * k)));
-        c1 = gl::add(c1, gl::mul(v, __ldg(ap + 2 * k + 1)));
+        c0.mac(v, __ldg(ap + 2 * k));
+        c1.mac(v, __ldg(ap + 2 * k + 1));
     }
 };
 
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
         const uint64_t first = sel[2 * (j & (KEC_THREADS - 1))], trans = sel[2 * (j & (KEC_THREADS - 1)) + 1];
         KFold f(a.alpha_pows);
         for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task(t, L, N, first, trans, f);
-        uint64_t c0 = f.c0, c1 = f.c1;
+        uint64_t c0 = f.c0.reduce(), c1 = f.c1.reduce();
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
             c0 = gl::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
