@@ -26,7 +26,7 @@ struct Challenger {
     void duplex() {
         for (int i = 0; i < n_in; i++) state[i] = in[i];
         n_in = 0;
-        p2::permute(state, p2);
+        p2::host::permute(state, p2);
         for (int i = 0; i < 8; i++) out[i] = state[i];
         n_out = 8;
     }
