@@ -37,11 +37,16 @@ PCS = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bi
            deep_pow_bits=0, num_queries=100, query_pow_bits=0)
 WORKLOAD = "keccak-f1600 AIR, 10922 perms -> 2^18 x 2633 Goldilocks trace, lifted STARK (Poseidon2-12 LMCS)"
 METRIC = "proofs/s"
-# DRAM bytes per algorithmic byte of the main-trace LDE, from the ncu capture
-# of every NTT launch of a 2^15-row LDE (dram__bytes_read.sum +
-# dram__bytes_write.sum summed over the launches, divided by 8*w*N*(1+B));
-# traffic grows in proportion to the rows, so it scales to 2^18.
-LDE_TRAFFIC_PER_ALG_BYTE = 3.88
+# DRAM bytes per algorithmic byte, from ncu captures of one full-size column
+# slab (2^18 x 336 through the LDE, 2^19 leaves through the sponge): the sum of
+# dram__bytes_read.sum + dram__bytes_write.sum over the slab's launches divided
+# by the slab's algorithmic bytes; the slabs of the 2^18 x 2633 trace are alike.
+LDE_TRAFFIC_PER_ALG_BYTE = 2.93
+HASH_TRAFFIC_PER_ALG_BYTE = 1.02
+# Binding resource of the two kernels, from the same captures (ncu
+# sm__inst_executed_pipe_alu / smsp__issue_active, % of peak).
+HASH_BINDING = "integer ALU pipe: 72.6 % of peak, issue 70.2 % (ncu, full-size slab)"
+LDE_BINDING = "integer ALU pipe: 63-72 % of peak, issue 56-67 % (ncu, full-size slab)"
 
 
 def load_product():
@@ -254,16 +259,22 @@ def run_gpu(args):
             pg.destroy_process_group()
         return 0
 
-    # roofline of the coset-LDE (HBM-bound): 8*w*N*(1+B) algorithmic bytes
     stages_ms = stages / args.steps
     pk = peaks()
     hbm_peak = pk.get("hbm_gbs", 6650.0)
     w = P.KECCAK_NUM_COLS
     B = 1 << PCS["log_blowup"]
+    n_lde = (1 << LOG_H) * B
+    # dominant kernel: the LMCS leaf sponge ("main tree" stage, which also holds
+    # the compress kernels); it reads every LDE word once
+    tree_ms = float(stages_ms[1])
+    hash_bytes = 8 * w * n_lde
+    hash_gbs = hash_bytes / (tree_ms * 1e-3) / 1e9
+    perms = n_lde * ((w + 7) // 8) + n_lde - 1
+    # coset LDE: 8*w*N*(1+B) algorithmic bytes over the LDE kernels' event time
     lde_bytes = 8 * w * (1 << LOG_H) * (1 + B)
-    lde_ms = float(np.mean(lde_k))  # LDE kernels only, CUDA events on their stream
-    achieved = lde_bytes / (lde_ms * 1e-3) / 1e9
-    perms = (1 << (LOG_H + PCS["log_blowup"])) * ((w + 7) // 8) + (1 << (LOG_H + PCS["log_blowup"])) - 1
+    lde_ms = float(np.mean(lde_k))
+    lde_gbs = lde_bytes / (lde_ms * 1e-3) / 1e9
     dominant = int(np.argmax(stages_ms))
     clk = clocks.summary()
     line = {
@@ -277,13 +288,17 @@ def run_gpu(args):
                        "wall_per_step": wall / args.steps * 1e3},
         "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages_ms)},
         "dominant_stage": P.STAGES[dominant],
-        "roofline": {"kernel": "coset LDE of the main trace (radix-8 NTT passes, column slabs)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": LDE_TRAFFIC_PER_ALG_BYTE * lde_bytes if LDE_TRAFFIC_PER_ALG_BYTE else None,
-                     "algorithmic_bytes": lde_bytes, "kernel_ms": lde_ms,
-                     "peak_source": "measured" if "hbm_gbs" in pk else "fallback"},
-        "hash": {"kernel": "LMCS leaf sponge (Poseidon2-12)", "perms": perms,
-                 "perms_per_s": perms / (stages_ms[1] * 1e-3)},
+        "roofline": {"kernel": "merkle::leaf_class_kernel (LMCS leaf sponge, Poseidon2-12)", "bound": "hbm",
+                     "achieved": hash_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": hash_gbs / hbm_peak,
+                     "traffic": HASH_TRAFFIC_PER_ALG_BYTE * hash_bytes, "algorithmic_bytes": hash_bytes,
+                     "kernel_ms": tree_ms, "peak_source": "measured" if "hbm_gbs" in pk else "fallback",
+                     "binding_resource": HASH_BINDING},
+        "lde": {"kernel": "lde::lde_pass_kernel + lde::lde_fused_kernel (coset LDE, 3 trips x 8 slabs)",
+                "bound": "hbm", "achieved": lde_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": lde_gbs / hbm_peak,
+                "traffic": LDE_TRAFFIC_PER_ALG_BYTE * lde_bytes, "algorithmic_bytes": lde_bytes, "kernel_ms": lde_ms,
+                "binding_resource": LDE_BINDING},
+        "hash": {"kernel": "LMCS leaf sponge + compress (Poseidon2-12)", "perms": perms,
+                 "perms_per_s": perms / (tree_ms * 1e-3)},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_time / args.steps * 1e3},
         "gpu_launches": launches,
@@ -303,6 +318,67 @@ def run_gpu(args):
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------ other named configurations
+LIFTED_PCS = dict(log_blowup=3, log_folding_arity=2, log_final_degree=0, folding_pow_bits=16,
+                  deep_pow_bits=0, num_queries=100, query_pow_bits=0)
+SMALL_PCS = PCS
+
+
+def time_proofs(P, ctx, pcs, wits, steps, warmup, dev):
+    """Device-timed prove_multi on resident witnesses: per-proof ms, stage ms, last output."""
+    import torch
+    for _ in range(warmup):
+        out = P.prove_multi(ctx, pcs, wits)
+    ref = out.digest.copy()
+    torch.cuda.synchronize(dev)
+    lat, stages, launches = [], np.zeros(len(P.STAGES)), 0
+    with ClockSampler(dev) as clocks:
+        for _ in range(steps):
+            out = P.prove_multi(ctx, pcs, wits)
+            lat.append(out.device_ms)
+            stages += np.array(out.stage_ms)
+            launches += out.gpu_launches
+            assert np.array_equal(out.digest, ref), "non-deterministic proof"
+    return lat, stages / steps, launches, out, clocks.summary()
+
+
+def run_named(args):
+    """Config 1 (Keccak, 42 permutations, 2^10 rows: latency) or config 3
+    (three cubic-AIR traces 2^20 x 64, 2^16 x 256, 2^12 x 1024 lifted to
+    2^20, log_blowup 3, FRI arity 4)."""
+    import torch
+    dev = 0
+    torch.cuda.set_device(dev)
+    P = load_product()
+    ctx = P.Context(dev)
+    if args.workload == "small":
+        inputs = P.keccak_inputs(1, 42)
+        t = P.generate_keccak_trace(inputs)
+        wits = [P.AirWitness(P.AIR_KECCAK, torch.from_numpy(t.view(np.int64)).to(f"cuda:{dev}"))]
+        pcs_d, name = SMALL_PCS, "keccak-f1600 AIR, 42 perms -> 2^10 x 2633 trace, lifted STARK (Poseidon2-12 LMCS)"
+    else:
+        wits = []
+        for i, (lh, w) in enumerate([(12, 1024), (16, 256), (20, 64)]):  # ascending heights
+            k, t = P.generate_cubic_trace(lh, w, 300 + i)
+            wits.append(P.AirWitness(P.AIR_CUBIC, torch.from_numpy(t.view(np.int64)).to(f"cuda:{dev}"), k))
+        pcs_d, name = LIFTED_PCS, "cubic AIR x3 (2^12 x 1024, 2^16 x 256, 2^20 x 64) lifted to 2^20, log_blowup 3, arity 4"
+    torch.cuda.synchronize(dev)
+    lat, stages, launches, out, clk = time_proofs(P, ctx, P.PcsParams(**pcs_d), wits, args.steps, args.warmup, dev)
+    line = {
+        "metric": "proofs/s", "value": len(lat) / (sum(lat) / 1e3), "unit": "proofs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(lat)), "higher_is_better": True,
+        "dtype": "u64 (Goldilocks, exact)", "data": "synthetic (seeded traces), resident in HBM",
+        "config": {"workload": name, "pcs": pcs_d, "timing": "CUDA events on the prover stream"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages)},
+        "gpu_launches": launches, "clocks": clk,
+        "proof_bytes": int(out.proof.fields.nbytes + out.proof.commitments.nbytes),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
     return 0
 
 
@@ -428,8 +504,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--log-h", type=int, default=18,
                     help="trace height (log2); 18 is the measured workload, smaller values are profiling cases")
-    ap.add_argument("--workload", default="keccak", choices=["keccak", "batch", "serve"],
-                    help="keccak: the plain prover at scale (headline); batch: 64-proof uneven mix; serve: Poisson stream")
+    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve"],
+                    help="keccak: the plain prover at scale (headline); small: 42-permutation Keccak proof; "
+                         "lifted: three cubic traces lifted to 2^20; batch: 64-proof uneven mix; serve: Poisson stream")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--pool", type=int, default=32)
@@ -443,6 +520,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload in ("small", "lifted"):
+        return run_named(args)
     global LOG_H, N_PERMS
     if args.log_h != LOG_H:
         LOG_H = args.log_h
