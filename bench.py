@@ -382,6 +382,44 @@ def run_named(args):
     return 0
 
 
+def run_slab(args):
+    """One full-size column slab of the headline workload through the public
+    LDE and LMCS entry points (2^18 x 336 seeded words, log_blowup 1, then the
+    2^19-leaf tree): the launch shapes of one of the 8 main-trace slabs, for
+    kernel-level profiling."""
+    import torch
+    dev = 0
+    torch.cuda.set_device(dev)
+    P = load_product()
+    ctx = P.Context(dev)
+    h, w = 1 << LOG_H, 336
+    m = np.random.default_rng(1).integers(0, P.P, size=(h, w), dtype=np.uint64)
+    d = P.to_device(m, dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    lde_ms, tree_ms = [], []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        ev[0].record()
+        out = P.coset_lde(ctx, d, PCS["log_blowup"], 7)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            lde_ms.append(ev[0].elapsed_time(ev[1]))
+        ev[0].record()
+        root = P.LmcsTree(ctx, [out], 8).root()
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            tree_ms.append(ev[0].elapsed_time(ev[1]))
+    print(json.dumps({"workload": f"column slab 2^{LOG_H} x {w}, log_blowup {PCS['log_blowup']}",
+                      "lde_ms": float(np.median(lde_ms)), "tree_ms": float(np.median(tree_ms)),
+                      "root": [int(x) for x in root],
+                      "timing": "CUDA events on the current stream around each synchronous call (includes host set-up)"}),
+          flush=True)
+    ctx.close()
+    return 0
+
+
 # ------------------------------------------------- batched and serving
 MIX_PCS = dict(log_blowup=3, log_folding_arity=1, log_final_degree=0, folding_pow_bits=16,
                deep_pow_bits=0, num_queries=100, query_pow_bits=0)
@@ -504,9 +542,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--log-h", type=int, default=18,
                     help="trace height (log2); 18 is the measured workload, smaller values are profiling cases")
-    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve"],
+    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve", "slab"],
                     help="keccak: the plain prover at scale (headline); small: 42-permutation Keccak proof; "
-                         "lifted: three cubic traces lifted to 2^20; batch: 64-proof uneven mix; serve: Poisson stream")
+                         "lifted: three cubic traces lifted to 2^20; batch: 64-proof uneven mix; serve: Poisson stream; "
+                         "slab: one 2^18 x 336 column slab through the LDE and the tree (kernel profiling)")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--pool", type=int, default=32)
@@ -528,6 +567,8 @@ def main():
         N_PERMS = (1 << LOG_H) // 24
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "slab":
+        return run_slab(args)
     return run_gpu(args)
 
 
