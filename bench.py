@@ -109,7 +109,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -118,36 +118,49 @@ def dist_setup():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=None)
+        # short timeout: a rank that never arrives ends the others' next collective with an error
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
 
+def _scalar(v: float, dev):
+    import torch
+    return torch.tensor([v], dtype=torch.float64, device="cpu" if dev is None else f"cuda:{dev}")
+
+
 def barrier(pg, dev):
+    """All ranks meet; dev None means a CPU (gloo) group."""
     if pg is not None:
-        import torch
-        t = torch.zeros(1, device=f"cuda:{dev}")
+        t = _scalar(0.0, dev)
         pg.all_reduce(t)
-        torch.cuda.synchronize(dev)
+        if dev is not None:
+            import torch
+            torch.cuda.synchronize(dev)
 
 
-def max_over_ranks(pg, v: float, dev: int) -> float:
+def max_over_ranks(pg, v: float, dev) -> float:
     if pg is None:
         return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{dev}")
+    t = _scalar(v, dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
-def sum_over_ranks(pg, v: float, dev: int) -> float:
+def sum_over_ranks(pg, v: float, dev) -> float:
     if pg is None:
         return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{dev}")
+    t = _scalar(v, dev)
     pg.all_reduce(t)
     return float(t.item())
+
+
+def aggregate(pg, proofs: float, device_s: float, dev):
+    """Replica aggregation: whole-job proofs/s = proofs of all ranks / the
+    slowest rank's device time (weak scaling, no data-path collective)."""
+    t = max_over_ranks(pg, device_s, dev)
+    total = sum_over_ranks(pg, proofs, dev)
+    return total / t, t, total
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -173,8 +186,8 @@ def cpu_sample_rate(log_h_sample: int, threads: int, reps: int):
 
 
 def run_reference(args):
-    world, rank, local, pg = dist_setup()
-    if rank != 0:
+    # CPU-only arm with no collectives: under torchrun, rank 0 alone runs and prints
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     threads = os.cpu_count() or 1
     log_s = int(os.environ.get("P3G_CPU_SAMPLE_LOG_H", "12"))
@@ -235,9 +248,7 @@ def run_gpu(args):
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - t0
     barrier(pg, dev)
-    dev_time = max_over_ranks(pg, sum(lat) / 1e3, dev)
-    total_proofs = sum_over_ranks(pg, float(args.steps), dev)
-    value = total_proofs / dev_time
+    value, dev_time, total_proofs = aggregate(pg, float(args.steps), sum(lat) / 1e3, dev)
 
     # ---- end-to-end arm: host (pinned) trace in, proof bytes out, per step
     for _ in range(max(1, args.warmup // 2)):
