@@ -107,23 +107,24 @@ GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
 }
 #if defined(__CUDACC__)
 // r0 + r1*2^32 + r2*2^64 + r3*2^96 -> a value below 2^64 congruent mod p
-// (weakly reduced), with 2^64 = 2^32 - 1 and 2^96 = -1: (r1:r0) - r3 + r2*eps.
+// (weakly reduced). With 2^64 = 2^32 - 1 and 2^96 = -1 the value is
+// V = r0 + 2^32 (r1 + r2) - (r2 + r3), in (-2^33, 2^65 + 2^32): one carry
+// chain forms (r1 + r2 : r0) - (r2 + r3) mod 2^64 and k = carry - borrow in
+// {-1, 0, 1}, then k * eps (2^64 = eps) is added; neither direction wraps again.
 __device__ __forceinline__ uint64_t reduce4_dev(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
     uint32_t o0, o1;
-    asm("{\n\t.reg .u32 m, u0, u1;\n\t"
-        "sub.cc.u32 %0, %2, %5;\n\t"
-        "subc.cc.u32 %1, %3, 0;\n\t"
-        "subc.u32 m, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, m;\n\t"  // on borrow subtract eps
-        "subc.u32 %1, %1, 0;\n\t"
-        "sub.cc.u32 u0, 0, %4;\n\t"   // r2*eps = (r2 << 32) - r2
-        "subc.u32 u1, %4, 0;\n\t"
-        "add.cc.u32 %0, %0, u0;\n\t"
-        "addc.cc.u32 %1, %1, u1;\n\t"
-        "addc.u32 m, 0, 0;\n\t"
-        "neg.s32 m, m;\n\t"            // on carry add eps
-        "add.cc.u32 %0, %0, m;\n\t"
-        "addc.u32 %1, %1, 0;\n\t}"
+    asm("{\n\t.reg .u32 s0, s1, h, c, k;\n\t"
+        "add.cc.u32 s0, %4, %5;\n\t"  // s = r2 + r3 (33 bits)
+        "addc.u32 s1, 0, 0;\n\t"
+        "add.cc.u32 h, %3, %4;\n\t"   // h = r1 + r2, carry c
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 %0, %2, s0;\n\t"  // (h:r0) - (s1:s0), borrow b
+        "subc.cc.u32 %1, h, s1;\n\t"
+        "subc.u32 k, c, 0;\n\t"       // k = c - b
+        "neg.s32 s0, k;\n\t"          // k * eps = (k >> 31 : -k)
+        "shr.s32 s1, k, 31;\n\t"
+        "add.cc.u32 %0, %0, s0;\n\t"
+        "addc.u32 %1, %1, s1;\n\t}"
         : "=&r"(o0), "=&r"(o1)
         : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
     return ((uint64_t)o1 << 32) | o0;
