@@ -393,6 +393,40 @@ inline void finish_tree(Ctx &ctx, Tree &t) {
     memcpy(t.root, ctx.pinned, 32);
 }
 
+// LMCS tree of matrices that are identically zero (the dummy aux traces).
+// Every leaf absorbs the same zero rows (one zero-padded 8-word chunk per 8
+// columns of each matrix, overwrite mode), so layer 0 is one digest c_0
+// repeated and layer l + 1 is c_{l+1} = compress(c_l, c_l). The depth + 1
+// digests are computed on the host and written into the usual layer buffer,
+// so openings read it like any other tree; the result equals build_tree's.
+inline void build_zero_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t alignment) {
+    t.mats = mats;
+    t.alignment = alignment ? alignment : 1;
+    t.H = mats.back().h;
+    t.depth = log2u(t.H);
+    t.layers = ctx.alloc((2 * t.H - 1) * 4);
+    uint64_t s[12] = {0};
+    for (const Mat &m : mats)
+        for (uint64_t i = 0; i < m.w; i += 8) {
+            for (int j = 0; j < 8; j++) s[j] = 0;
+            p2::host::permute(s, ctx.p2);
+        }
+    std::vector<uint64_t> c(4 * (t.depth + 1));
+    for (int j = 0; j < 4; j++) c[j] = s[j];
+    for (uint32_t l = 0; l < t.depth; l++) {
+        uint64_t u[12] = {0};
+        for (int j = 0; j < 4; j++) u[j] = u[4 + j] = c[4 * l + j];
+        p2::host::permute(u, ctx.p2);
+        for (int j = 0; j < 4; j++) c[4 * (l + 1) + j] = u[j];
+    }
+    DBuf dc = ctx.upload(c);
+    const uint64_t n = 2 * t.H - 1;
+    merkle::fill_const_layers_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(t.layers.p, t.H, t.depth, dc.p);
+    CK(cudaGetLastError());
+    ctx.launches++;
+    memcpy(t.root, &c[4 * t.depth], 32);
+}
+
 inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t alignment) {
     t.mats = mats;
     t.alignment = alignment ? alignment : 1;

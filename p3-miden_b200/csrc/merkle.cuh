@@ -241,4 +241,16 @@ __global__ void __launch_bounds__(256) compress_kernel(uint64_t *layers, uint64_
     }
 }
 
+// Digest layers of a tree whose layer l holds one digest c_l repeated:
+// digest g (0 <= g < 2H - 1) belongs to layer l with H >> l = 2^(ceil(log2(2H - g)) - 1).
+__global__ void fill_const_layers_kernel(uint64_t *layers, uint64_t H, uint32_t depth, const uint64_t *c) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= 2 * H - 1) return;
+    const uint64_t r1 = 2 * H - g;  // >= 2
+    const uint32_t lg = 64 - __clzll(r1 - 1);
+    const uint32_t l = depth - (lg - 1);
+#pragma unroll
+    for (int k = 0; k < 4; k++) layers[4 * g + k] = c[4 * l + k];
+}
+
 }  // namespace merkle

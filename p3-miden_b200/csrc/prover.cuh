@@ -281,19 +281,20 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     CK(cudaEventRecord(ev[2], ctx.stream));
 
     // ---- 2. randomness (max num_randomness over the AIRs = 1) and the
-    // 1-column zero aux traces flattened to 2 base columns
+    // dummy aux traces: one EF column of zeros, flattened to 2 base columns
+    // (p3-miden-lifted-examples/src/lib.rs:93-103). The LDE of a zero trace
+    // on any coset is zero, and its tree has one digest per layer
+    // (build_zero_tree): both are produced exactly, without transforms or
+    // per-leaf hashing.
     (void)tr.ch.sample_ef();
     for (size_t i = 0; i < n_inst; i++) {
         uint64_t h = inst[i].height;
-        DBuf z = ctx.alloc(h * 2);
-        CK(cudaMemsetAsync(z.p, 0, h * 16, ctx.stream));
         aux_lde[i] = ctx.alloc((h << lb) * 2);
-        uint64_t shift = gl::exp2k(gl::GEN, log_max_h - log2u(h));
-        coset_lde(ctx, z.p, 2, h, 2, lb, shift, aux_lde[i].p, tmp.p);
+        CK(cudaMemsetAsync(aux_lde[i].p, 0, (h << lb) * 16, ctx.stream));
         aux_mats.push_back({aux_lde[i].p, h << lb, 2});
     }
     Tree aux_tree;
-    build_tree(ctx, aux_tree, aux_mats, 8);
+    build_zero_tree(ctx, aux_tree, aux_mats, 8);
     tr.send_commit(aux_tree.root);
     CK(cudaEventRecord(ev[3], ctx.stream));
 
