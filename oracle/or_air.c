@@ -157,111 +157,34 @@ void or_keccak_trace(const uint64_t *inputs25, size_t n_perms, size_t log_h, uin
     }
 }
 
-/* Constraint helpers, as polynomials in arbitrary field values */
-static inline uint64_t xor2(uint64_t a, uint64_t b) { return or_sub(or_add(a, b), or_add(or_mul(a, b), or_mul(a, b))); }
-static inline uint64_t xor3(uint64_t a, uint64_t b, uint64_t c) { return xor2(a, xor2(b, c)); }
-static inline uint64_t andn(uint64_t a, uint64_t b) { return or_mul(or_sub(1, a), b); }
-static inline uint64_t isbool(uint64_t a) { return or_mul(a, or_sub(a, 1)); }
-
-static size_t keccak_eval(const uint64_t *L, const uint64_t *N, const uint64_t sel[3], uint64_t *out) {
-    keccak_tables();
-    size_t k = 0;
-    uint64_t first = sel[0], trans = sel[2];
-#define EMIT(v) (out ? (out[k] = (v)) : 0, k++)
-    /* round flags */
-    EMIT(or_mul(first, or_sub(L[KC_STEP], 1)));
-    for (int i = 1; i < 24; i++) EMIT(or_mul(first, L[KC_STEP + i]));
-    for (int i = 0; i < 24; i++) EMIT(or_mul(trans, or_sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
-    uint64_t first_step = L[KC_STEP], not_final = or_sub(1, L[KC_STEP + 23]);
-    /* first step: preimage == a */
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                int o = (y * 5 + x) * 4 + l;
-                EMIT(or_mul(first_step, or_sub(L[KC_PRE + o], L[KC_A + o])));
-            }
-    EMIT(isbool(L[KC_EXPORT]));
-    EMIT(or_mul(not_final, L[KC_EXPORT]));
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                int o = (y * 5 + x) * 4 + l;
-                EMIT(or_mul(not_final, or_mul(trans, or_sub(L[KC_PRE + o], N[KC_PRE + o]))));
-            }
-    /* C'[x,z] = xor(C[x,z], C[x-1,z], C[x+1,z-1]) */
-    for (int x = 0; x < 5; x++)
-        for (int z = 0; z < 64; z++) {
-            EMIT(isbool(L[KC_C + x * 64 + z]));
-            uint64_t v = xor3(L[KC_C + x * 64 + z], L[KC_C + ((x + 4) % 5) * 64 + z],
-                              L[KC_C + ((x + 1) % 5) * 64 + (z + 63) % 64]);
-            EMIT(or_sub(L[KC_CP + x * 64 + z], v));
-        }
-    /* A = xor(A', C, C') limb-wise */
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t acc = 0;
-                for (int z = l * 16 + 15; z >= l * 16; z--) {
-                    uint64_t ap = L[KC_AP + (y * 5 + x) * 64 + z];
-                    EMIT(isbool(ap));
-                    uint64_t bit = xor3(ap, L[KC_C + x * 64 + z], L[KC_CP + x * 64 + z]);
-                    acc = or_add(or_add(acc, acc), bit);
-                }
-                EMIT(or_sub(acc, L[KC_A + (y * 5 + x) * 4 + l]));
-            }
-    /* sum_y A'[x,y,z] - C'[x,z] in {0, 2, 4} */
-    for (int x = 0; x < 5; x++)
-        for (int z = 0; z < 64; z++) {
-            uint64_t s = 0;
-            for (int y = 0; y < 5; y++) s = or_add(s, L[KC_AP + (y * 5 + x) * 64 + z]);
-            uint64_t d = or_sub(s, L[KC_CP + x * 64 + z]);
-            EMIT(or_mul(or_mul(d, or_sub(d, 2)), or_sub(d, 4)));
-        }
-    /* A''[x,y] = xor(B[x,y], andn(B[x+1,y], B[x+2,y])); B[x,y] bit z is
-     * A'[(x+3y)%5, x] bit (z - r) with r the rho offset of lane ((x+3y)%5, x) */
-#define BBIT(bx, by, bz)                                                                                 \
-    L[KC_AP + ((bx) * 5 + ((bx) + 3 * (by)) % 5) * 64 + ((bz) + 64 - rot_r[((bx) + 3 * (by)) % 5][(bx)]) % 64]
-    for (int y = 0; y < 5; y++)
-        for (int x = 0; x < 5; x++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t acc = 0;
-                for (int z = l * 16 + 15; z >= l * 16; z--) {
-                    uint64_t bit = xor2(BBIT(x, y, z), andn(BBIT((x + 1) % 5, y, z), BBIT((x + 2) % 5, y, z)));
-                    acc = or_add(or_add(acc, acc), bit);
-                }
-                EMIT(or_sub(acc, L[KC_APP + (y * 5 + x) * 4 + l]));
-            }
-#undef BBIT
-    /* A''[0,0] bits */
-    for (int l = 0; l < 4; l++) {
-        uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
-            EMIT(isbool(L[KC_APP00 + z]));
-            acc = or_add(or_add(acc, acc), L[KC_APP00 + z]);
-        }
-        EMIT(or_sub(acc, L[KC_APP + l]));
-    }
-    /* A'''[0,0] = A''[0,0] xor RC, RC bit = sum_r step_flags[r] * RC_r bit */
-    for (int l = 0; l < 4; l++) {
-        uint64_t acc = 0;
-        for (int z = l * 16 + 15; z >= l * 16; z--) {
-            uint64_t rcb = 0;
-            for (int r = 0; r < 24; r++)
-                if ((rc64[r] >> z) & 1) rcb = or_add(rcb, L[KC_STEP + r]);
-            acc = or_add(or_add(acc, acc), xor2(L[KC_APP00 + z], rcb));
-        }
-        EMIT(or_sub(acc, L[KC_APPP00 + l]));
-    }
-    /* round output == next round input, unless final step */
-    for (int x = 0; x < 5; x++)
-        for (int y = 0; y < 5; y++)
-            for (int l = 0; l < 4; l++) {
-                uint64_t outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
-                EMIT(or_mul(trans, or_mul(not_final, or_sub(outv, N[KC_A + (y * 5 + x) * 4 + l]))));
-            }
-#undef EMIT
-    return k;
-}
+/* The constraint list, instantiated over F (quotient domain) and over EF
+ * (the verifier's out-of-domain point). */
+#define KT uint64_t
+#define K_ADD or_add
+#define K_SUB or_sub
+#define K_MUL or_mul
+#define K_C(u) ((uint64_t)(u))
+#define K_FN(name) name
+#include "or_keccak_cons.inc"
+#undef KT
+#undef K_ADD
+#undef K_SUB
+#undef K_MUL
+#undef K_C
+#undef K_FN
+#define KT or_ef
+#define K_ADD or_ef_add
+#define K_SUB or_ef_sub
+#define K_MUL or_ef_mul
+#define K_C(u) or_ef_from((uint64_t)(u))
+#define K_FN(name) name##_ef
+#include "or_keccak_cons.inc"
+#undef KT
+#undef K_ADD
+#undef K_SUB
+#undef K_MUL
+#undef K_C
+#undef K_FN
 
 size_t or_air_num_constraints(int air, size_t width) {
     if (air == OR_AIR_CUBIC) return width;
@@ -288,6 +211,21 @@ void or_air_eval(int air, size_t width, const uint64_t *consts, const uint64_t *
         }
     } else if (air == OR_AIR_KECCAK) {
         keccak_eval(L, N, sel, out);
+    }
+}
+
+/* Constraints of one row pair over EF (the verifier's local/next openings
+ * at z and z*w), in emission order; sel as in or_air_eval. */
+void or_air_eval_ef(int air, size_t width, const uint64_t *consts, const or_ef *L, const or_ef *N, const or_ef sel[3],
+                    or_ef *out) {
+    if (air == OR_AIR_CUBIC) {
+        for (size_t i = 0; i < width; i++) {
+            or_ef x = L[i];
+            or_ef rhs = or_ef_add(or_ef_add(or_ef_mul(or_ef_mul(x, x), x), L[(i + 1) % width]), or_ef_from(consts[i]));
+            out[i] = or_ef_mul(sel[2], or_ef_sub(N[i], rhs));
+        }
+    } else if (air == OR_AIR_KECCAK) {
+        keccak_eval_ef(L, N, sel, out);
     }
 }
 

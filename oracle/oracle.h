@@ -104,6 +104,8 @@ unsigned or_air_log_quotient_degree(int air);
  * sel = {is_first_row, is_last_row, is_transition}. */
 void or_air_eval(int air, size_t width, const uint64_t *consts, const uint64_t *local,
                  const uint64_t *next, const uint64_t sel[3], uint64_t *out);
+void or_air_eval_ef(int air, size_t width, const uint64_t *consts, const or_ef *local, const or_ef *next,
+                    const or_ef sel[3], or_ef *out);
 /* Trace generators (the caller side of the reference path). */
 void or_cubic_trace(size_t log_h, size_t width, uint64_t seed, uint64_t *consts_out, uint64_t *trace_out);
 size_t or_keccak_num_cols(void);
@@ -140,6 +142,25 @@ typedef struct {
 int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
              or_proof *out);
 void or_proof_free(or_proof *p);
+
+/* --------------------------------------------------------------- verifier */
+enum {
+    OR_VERR_SHAPE = 1,   /* instances not ascending / not powers of two, degree > blowup */
+    OR_VERR_OPENING,     /* query index outside the tree */
+    OR_VERR_ROOT,        /* an LMCS opening does not reproduce its commitment */
+    OR_VERR_POW,         /* a proof-of-work witness fails */
+    OR_VERR_DEEP,        /* an evaluation point lies on the LDE domain */
+    OR_VERR_FRI,         /* an FRI row does not contain the folded value */
+    OR_VERR_FINAL,       /* the final polynomial disagrees with the last fold */
+    OR_VERR_QUOTIENT,    /* folded constraints != Q(z) * Z_H(z) */
+    OR_VERR_TRANSCRIPT,  /* transcript too short or not fully consumed */
+    OR_VERR_DIGEST,      /* final challenger state differs from the proof's digest */
+};
+/* Verify a proof (fields, commitments, digest) for the given instances
+ * (air, height, width, consts; traces are not read). 0 = accepted. */
+int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
+              const uint64_t *fields, size_t n_fields, const uint64_t *commits, size_t n_commits,
+              const uint64_t digest[12]);
 /* Stage timers of the last or_prove call (seconds), by stage index. */
 double or_last_stage_seconds(int stage);
 

@@ -126,6 +126,8 @@ def lib():
             ("or_prove", C.c_int, [C.POINTER(P2Params), C.POINTER(PcsParams), C.POINTER(Instance), C.c_size_t, C.POINTER(Proof)]),
             ("or_proof_free", None, [C.POINTER(Proof)]),
             ("or_last_stage_seconds", C.c_double, [C.c_int]),
+            ("or_verify", C.c_int, [C.POINTER(P2Params), C.POINTER(PcsParams), C.POINTER(Instance), C.c_size_t,
+                                    u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
         ]:
             fn = getattr(L, name)
             fn.restype = res
@@ -258,6 +260,30 @@ def prove(pp: P2Params, pcs: dict, instances):
     out["stage_seconds"] = [lib().or_last_stage_seconds(i) for i in range(7)]
     lib().or_proof_free(C.byref(proof))
     return out
+
+
+VERIFY_ERRORS = {0: "accepted", 1: "shape", 2: "opening index", 3: "LMCS root", 4: "proof of work",
+                 5: "DEEP point on domain", 6: "FRI row", 7: "final polynomial", 8: "quotient identity",
+                 9: "transcript length", 10: "digest"}
+
+
+def verify(pp: P2Params, pcs: dict, instances, fields, commits, digest) -> int:
+    """Verifier restatement: instances are (air, height, width, consts|None),
+    in ascending height order; returns 0 when the proof is accepted, else an
+    error code (VERIFY_ERRORS)."""
+    keep = []
+    arr = (Instance * len(instances))()
+    dummy = np.zeros(1, dtype=np.uint64)
+    for i, (air, h, w, consts) in enumerate(instances):
+        c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
+        keep.append(c)
+        arr[i] = Instance(air, h, w, ptr(dummy), ptr(c))
+    f = np.ascontiguousarray(fields, dtype=np.uint64)
+    cm = np.ascontiguousarray(np.asarray(commits, dtype=np.uint64).reshape(-1))
+    d = np.ascontiguousarray(digest, dtype=np.uint64)
+    pr = PcsParams(**pcs)
+    return int(lib().or_verify(C.byref(pp), C.byref(pr), arr, len(instances), ptr(f), f.size,
+                               ptr(cm) if cm.size else ptr(dummy), cm.size // 4, ptr(d)))
 
 
 def set_threads(n: int):

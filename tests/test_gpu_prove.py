@@ -1,5 +1,8 @@
-"""Whole-proof parity: the GPU prover's transcript (fields, commitments,
-digest) is bit-identical to the oracle's on the same traces and parameters."""
+"""Whole-proof parity and acceptance: the GPU prover's transcript (fields,
+commitments, digest) is bit-identical to the oracle's on the same traces and
+parameters, and the verifier restatement (oracle/or_verify.c) accepts it,
+including at the full sizes of the headline and lifted workloads, where only
+the (cheap) verifier runs on the CPU."""
 import numpy as np
 import pytest
 
@@ -12,6 +15,12 @@ def pcs_dict(p):
     return dict(log_blowup=p.log_blowup, log_folding_arity=p.log_folding_arity,
                 log_final_degree=p.log_final_degree, folding_pow_bits=p.folding_pow_bits,
                 deep_pow_bits=p.deep_pow_bits, num_queries=p.num_queries, query_pow_bits=p.query_pow_bits)
+
+
+def check_verifies(gpu, pcs, instances):
+    """instances: (air, height, width, consts|None) in ascending height order."""
+    rc = O.verify(O.default_p2(), pcs_dict(pcs), instances, gpu.proof.fields, gpu.proof.commitments, gpu.digest)
+    assert rc == 0, f"verifier rejected the GPU proof: {O.VERIFY_ERRORS.get(rc, rc)}"
 
 
 def check_same(gpu, orc):
@@ -29,6 +38,7 @@ def test_cubic_single_trace(product, gpu_ctx, arity):
     gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k)])
     orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_CUBIC, t, k)])
     check_same(gpu, orc)
+    check_verifies(gpu, pcs, [(O.AIR_CUBIC, t.shape[0], t.shape[1], k)])
 
 
 def test_cubic_lifted_three_traces(product, gpu_ctx):
@@ -43,6 +53,7 @@ def test_cubic_lifted_three_traces(product, gpu_ctx):
     gpu = product.prove_multi(gpu_ctx, pcs, inst)
     orc = O.prove(O.default_p2(), pcs_dict(pcs), oinst)
     check_same(gpu, orc)
+    check_verifies(gpu, pcs, [(a, t.shape[0], t.shape[1], k) for a, t, k in oinst])
 
 
 def test_keccak_small(product, gpu_ctx):
@@ -52,6 +63,7 @@ def test_keccak_small(product, gpu_ctx):
     gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, t)])
     orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t, None)])
     check_same(gpu, orc)
+    check_verifies(gpu, pcs, [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)])
 
 
 def test_keccak_42_perms_config(product, gpu_ctx):
@@ -64,6 +76,7 @@ def test_keccak_42_perms_config(product, gpu_ctx):
     gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, t)])
     orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t, None)])
     check_same(gpu, orc)
+    check_verifies(gpu, pcs, [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)])
 
 
 def test_device_resident_trace(product, gpu_ctx):
@@ -73,3 +86,31 @@ def test_device_resident_trace(product, gpu_ctx):
     dev = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, product.to_device(t), k)])
     assert np.array_equal(host.proof.fields, dev.proof.fields)
     assert np.array_equal(host.digest, dev.digest)
+
+
+def test_keccak_headline_2e18_verifies(product, gpu_ctx):
+    """The headline workload at full size (10922 permutations, 2^18 x 2633):
+    the GPU proof is accepted by the verifier restatement."""
+    t = product.generate_keccak_trace(product.keccak_inputs(1, 10922))
+    assert t.shape == (1 << 18, 2633)
+    pcs = product.PcsParams(1, 1, 0, 16, 0, 100, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, product.to_device(t))])
+    check_verifies(gpu, pcs, [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)])
+    # a proof for other inputs does not verify against this statement's transcript
+    bad = gpu.proof.fields.copy()
+    bad[len(bad) // 2] ^= 1
+    assert O.verify(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)], bad,
+                    gpu.proof.commitments, gpu.digest) != 0
+
+
+def test_lifted_config_full_size_verifies(product, gpu_ctx):
+    """Three cubic-AIR traces 2^12 x 1024, 2^16 x 256, 2^20 x 64 lifted to
+    2^20, log_blowup 3, FRI arity 4: accepted by the verifier restatement."""
+    inst, meta = [], []
+    for i, (lh, w) in enumerate([(12, 1024), (16, 256), (20, 64)]):
+        k, t = product.generate_cubic_trace(lh, w, 300 + i)
+        inst.append(product.AirWitness(product.AIR_CUBIC, product.to_device(t), k))
+        meta.append((O.AIR_CUBIC, t.shape[0], t.shape[1], k))
+    pcs = product.PcsParams(3, 2, 0, 16, 0, 100, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, inst)
+    check_verifies(gpu, pcs, meta)

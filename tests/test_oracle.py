@@ -164,3 +164,63 @@ def test_oracle_prove_is_deterministic():
     b = O.prove(pp, pcs, [(O.AIR_CUBIC, t, k)])
     assert np.array_equal(a["fields"], b["fields"]) and np.array_equal(a["commits"], b["commits"])
     assert np.array_equal(a["digest"], b["digest"])
+
+
+# ----------------------------------------------------------- verifier
+def _prove_and_meta(pcs, insts):
+    pp = O.default_p2()
+    pr = O.prove(pp, pcs, insts)
+    meta = [(a, t.shape[0], t.shape[1], k) for a, t, k in insts]
+    return pp, pr, meta
+
+
+BASE_PCS = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bits=4, deep_pow_bits=0,
+                num_queries=20, query_pow_bits=0)
+
+
+@pytest.mark.parametrize("log_a,log_b", [(1, 1), (2, 2), (3, 3), (1, 3), (3, 1)])
+def test_verifier_accepts_oracle_proofs(log_a, log_b):
+    """verify_multi restatement (verifier/mod.rs:170-364) accepts the oracle
+    prover's proofs across FRI arities and blowups."""
+    k, t = O.cubic_trace(6, 9, 3)
+    pcs = dict(BASE_PCS, log_folding_arity=log_a, log_blowup=log_b)
+    pp, pr, meta = _prove_and_meta(pcs, [(O.AIR_CUBIC, t, k)])
+    assert O.verify(pp, pcs, meta, pr["fields"], pr["commits"], pr["digest"]) == 0
+
+
+def test_verifier_accepts_lifted_keccak_and_pow():
+    ins = []
+    for lh, w, s in [(3, 20, 1), (5, 9, 2), (7, 5, 3)]:
+        kk, tt = O.cubic_trace(lh, w, s)
+        ins.append((O.AIR_CUBIC, tt, kk))
+    pcs = dict(BASE_PCS, log_blowup=2, log_folding_arity=2, log_final_degree=2, deep_pow_bits=3, query_pow_bits=5)
+    pp, pr, meta = _prove_and_meta(pcs, ins)
+    assert O.verify(pp, pcs, meta, pr["fields"], pr["commits"], pr["digest"]) == 0
+    t = O.keccak_trace(O.keccak_inputs(1, 5), 7)
+    pp, pr, meta = _prove_and_meta(BASE_PCS, [(O.AIR_KECCAK, t, None)])
+    assert O.verify(pp, BASE_PCS, meta, pr["fields"], pr["commits"], pr["digest"]) == 0
+
+
+def test_verifier_rejects_tampering():
+    """Any changed field, commitment or digest, a truncated transcript, or a
+    wrong statement (other AIR constants) is rejected."""
+    k, t = O.cubic_trace(6, 9, 3)
+    pcs = dict(BASE_PCS, folding_pow_bits=0, log_blowup=2, log_folding_arity=2)
+    pp, pr, meta = _prove_and_meta(pcs, [(O.AIR_CUBIC, t, k)])
+    f, c, d = pr["fields"], pr["commits"], pr["digest"]
+    n = len(f)
+    for i in [0, 1, 7, n // 4, n // 2, n - 2, n - 1]:
+        g = f.copy()
+        g[i] = (int(g[i]) + 1) % (2**64 - 2**32 + 1)
+        assert O.verify(pp, pcs, meta, g, c, d) != 0, i
+    for i in range(len(c)):
+        cc = c.copy()
+        cc[i][0] ^= 1
+        assert O.verify(pp, pcs, meta, f, cc, d) != 0, i
+    dd = d.copy()
+    dd[3] ^= 1
+    assert O.verify(pp, pcs, meta, f, c, dd) == 10
+    assert O.verify(pp, pcs, meta, f[:-1], c, d) != 0
+    k2 = k.copy()
+    k2[0] = (int(k2[0]) + 1) % (2**64 - 2**32 + 1)
+    assert O.verify(pp, pcs, [(O.AIR_CUBIC, t.shape[0], t.shape[1], k2)], f, c, d) == 8  # quotient identity
