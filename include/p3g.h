@@ -185,6 +185,14 @@ uint64_t p3g_job_footprint_bytes(const p3g_pcs_params *pcs, const p3g_instance *
 /* generate_keccak_trace (p3-miden-lifted-examples/src/keccak.rs:54-56):
  * 2^log_height x 2633, n_perms * 24 <= 2^log_height. */
 int p3g_keccak_trace(const uint64_t *inputs25, uint64_t n_perms, uint32_t log_height, uint64_t *out);
+/* The same rows generated on the device (generate_trace_rows,
+ * p3-miden-lifted-examples/src/keccak.rs:54-56): d_inputs25 (device,
+ * n_perms x 25) -> d_out (device, 2^log_height x 2633, row-major), on the
+ * context's stream; returns when the trace is written. A caller holding only
+ * the permutation inputs uploads 200 bytes per permutation instead of the
+ * 505 KB of its 24 trace rows. */
+int p3g_keccak_trace_device(p3g_ctx *ctx, const uint64_t *d_inputs25, uint64_t n_perms, uint32_t log_height,
+                            uint64_t *d_out);
 /* SmallRng::seed_from_u64(seed).random::<[u64; 25]>() per permutation
  * (p3-miden-lifted-examples/src/bin/lifted_keccak.rs:167-170) */
 int p3g_keccak_inputs(uint64_t seed, uint64_t n_perms, uint64_t *out25);

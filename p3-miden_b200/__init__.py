@@ -100,6 +100,7 @@ def lib():
             "p3g_prove": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, C.POINTER(ProofC)]),
             "p3g_proof_free": (None, [C.POINTER(ProofC)]),
             "p3g_keccak_trace": (C.c_int, [u64p, C.c_uint64, C.c_uint32, u64p]),
+            "p3g_keccak_trace_device": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
             "p3g_keccak_inputs": (C.c_int, [C.c_uint64, C.c_uint64, u64p]),
             "p3g_cubic_trace": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, u64p, u64p]),
             "p3g_air_num_constraints": (C.c_uint64, [C.c_int32, C.c_uint64]),
@@ -365,6 +366,22 @@ def generate_keccak_trace(inputs: np.ndarray, out: np.ndarray | None = None) -> 
     if out is None:
         out = np.empty((1 << log_h, KECCAK_NUM_COLS), dtype=np.uint64)
     _check(lib().p3g_keccak_trace(_ptr(inputs), n, log_h, out.ctypes.data_as(u64p)))
+    return out
+
+
+def generate_keccak_trace_device(ctx: Context, inputs_dev, log_h: int | None = None, out=None):
+    """generate_trace_rows on the device: inputs_dev is a device tensor of
+    n_perms x 25 words (int64 view); returns a device tensor of
+    2^log_h x 2633 (default: the smallest height that holds the rows)."""
+    import torch
+    n = int(inputs_dev.shape[0])
+    if log_h is None:
+        log_h = max(0, (24 * n - 1).bit_length()) if n else 0
+    if out is None:
+        out = empty_device((1 << log_h, KECCAK_NUM_COLS), ctx.device)
+    torch.cuda.synchronize(ctx.device)
+    ctx.check(lib().p3g_keccak_trace_device(ctx.handle, inputs_dev.data_ptr() if n else None, n, log_h,
+                                            out.data_ptr()))
     return out
 
 

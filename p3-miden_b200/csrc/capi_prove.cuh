@@ -4,6 +4,7 @@
 #include <cstdlib>
 
 #include "capi_stage.cuh"
+#include "trace_gen.cuh"
 #include "prover.cuh"
 #include "traces.cuh"
 
@@ -49,6 +50,8 @@ inline void upload_keccak_tables() {
         for (int y = 0; y < 5; y++) rot[x * 5 + y] = T.rot[x][y];
     CK(cudaMemcpyToSymbol(quot::c_keccak_rc, T.rc, sizeof(T.rc)));
     CK(cudaMemcpyToSymbol(quot::c_keccak_rot, rot, sizeof(rot)));
+    CK(cudaMemcpyToSymbol(tgen::c_rc, T.rc, sizeof(T.rc)));
+    CK(cudaMemcpyToSymbol(tgen::c_rot, rot, sizeof(rot)));
 }
 
 // Validation mirroring prove_multi's checks (prover/mod.rs:238-264,
@@ -144,6 +147,22 @@ P3G_API int p3g_keccak_trace(const uint64_t *inputs25, uint64_t n_perms, uint32_
     if (n_perms * 24 > (1ull << log_height)) return p3g::ERR_INVALID;
     p3g::keccak_trace(inputs25, n_perms, log_height, out);
     return p3g::OK;
+}
+// The same trace generated on the device from device-resident inputs, on the
+// context's stream; returns once the trace is written.
+P3G_API int p3g_keccak_trace_device(p3g_ctx *x, const uint64_t *d_inputs25, uint64_t n_perms, uint32_t log_height,
+                                    uint64_t *d_out) {
+    if (!x || !d_out || (!d_inputs25 && n_perms) || log_height > 30) return p3g::ERR_INVALID;
+    if (n_perms * 24 > (1ull << log_height)) return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        p3g::ensure_keccak_tables(x->c.device);
+        const uint64_t h = 1ull << log_height;
+        tgen::keccak_trace_kernel<<<(unsigned)((h + 23) / 24), 128, 0, x->c.stream>>>(d_inputs25, n_perms, h, d_out);
+        CK(cudaGetLastError());
+        x->c.launches++;
+        x->c.sync();
+    })
 }
 P3G_API int p3g_cubic_trace(uint32_t log_height, uint64_t width, uint64_t seed, uint64_t *consts_out,
                             uint64_t *trace_out) {

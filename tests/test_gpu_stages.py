@@ -65,3 +65,18 @@ def test_lmcs_tree_matches_oracle(product, gpu_ctx, scenario, alignment):
     assert np.array_equal(gt.root(), ot.root())
     for l in range(gt.depth + 1):
         assert np.array_equal(gt.layer(l), ot.layer(l))
+
+
+@pytest.mark.parametrize("n_perms,log_h", [(0, 0), (1, 5), (5, 7), (10, 8), (42, 10), (2730, 16)])
+def test_keccak_trace_device_matches_host(product, gpu_ctx, n_perms, log_h):
+    """Device generate_trace_rows equals the host generator bit for bit,
+    including truncated last permutations and zero padding permutations."""
+    import torch
+    inputs = product.keccak_inputs(9, n_perms)
+    host = np.zeros((1 << log_h, product.KECCAK_NUM_COLS), dtype=np.uint64)
+    product.lib().p3g_keccak_trace(inputs.ctypes.data_as(product.u64p) if n_perms else None, n_perms, log_h,
+                                   host.ctypes.data_as(product.u64p))
+    d_in = product.to_device(inputs.reshape(-1, 25)) if n_perms else torch.empty((0, 25), dtype=torch.int64,
+                                                                                  device="cuda:0")
+    dev = product.generate_keccak_trace_device(gpu_ctx, d_in, log_h)
+    assert np.array_equal(product.to_host(dev), host)
