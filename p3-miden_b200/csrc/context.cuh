@@ -375,8 +375,9 @@ struct Tree {
     uint64_t layer_off(uint32_t l) const { return 2 * H - 2 * (H >> l); }
 };
 
-// Compress layer 0 (already filled) up to the root and fetch the root.
-inline void finish_tree(Ctx &ctx, Tree &t) {
+// Compress layer 0 (already filled) up to the root (kernels only; the root
+// stays on the device); finish_tree also fetches the root.
+inline void compress_layers(Ctx &ctx, Tree &t) {
     uint32_t l = 0;
     while (l < t.depth) {
         uint64_t n_parents = t.H >> (l + 1);
@@ -388,6 +389,9 @@ inline void finish_tree(Ctx &ctx, Tree &t) {
         ctx.launches++;
         l += levels;
     }
+}
+inline void finish_tree(Ctx &ctx, Tree &t) {
+    compress_layers(ctx, t);
     ctx.d2h(ctx.stage(4), t.layers.p + 4 * t.layer_off(t.depth), 4);
     ctx.sync();
     memcpy(t.root, ctx.pinned, 32);

@@ -25,18 +25,19 @@ struct FoldArgs {
     uint32_t log_n0;      // log2 of the root of the s_inv table
     ntt::PowTab w0inv;    // powers of w_{n0}^{-1}
     gl::ef beta;
+    const uint64_t *beta_dev;  // if set, the challenge is read from here (device-side transcript)
     uint64_t winv_a[8];   // w_a^{-t}, t < a
     uint64_t inv_a;       // 1/a
     uint64_t *out;        // n_out EF
     uint64_t *digests;    // (n_out / a) digests of the next round, or null
 };
 
-__device__ __forceinline__ gl::ef fold_one(const FoldArgs &a, uint64_t k) {
+__device__ __forceinline__ gl::ef fold_one(const FoldArgs &a, gl::ef beta, uint64_t k) {
     const uint32_t A = 1u << a.log_a;
     // s_inv = w_{n_in}^{-bitrev_{log n_out}(k)} = w_{n0}^{-(bitrev << (log n0 - log n_in))}
     uint64_t e = gl::bitrev(k, a.log_nin - a.log_a) << (a.log_n0 - a.log_nin);
     uint64_t s_inv = a.w0inv.at(e);
-    gl::ef x = gl::ef_mulf(a.beta, s_inv);
+    gl::ef x = gl::ef_mulf(beta, s_inv);
     const uint64_t *row = a.in + 2 * k * A;
     if (A == 2) {
         gl::ef y0{row[0], row[1]}, y1{row[2], row[3]};
@@ -65,8 +66,9 @@ __global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ 
     if (g * A >= a.n_out) return;
     uint64_t buf[16];
     const uint32_t cnt = (uint32_t)((a.n_out - g * A) < A ? (a.n_out - g * A) : A);
+    const gl::ef beta = a.beta_dev ? gl::ef{a.beta_dev[0], a.beta_dev[1]} : a.beta;
     for (uint32_t u = 0; u < cnt; u++) {
-        gl::ef v = fold_one(a, g * A + u);
+        gl::ef v = fold_one(a, beta, g * A + u);
         a.out[2 * (g * A + u)] = v.c0;
         a.out[2 * (g * A + u) + 1] = v.c1;
         buf[2 * u] = v.c0;
@@ -109,6 +111,60 @@ __global__ void __launch_bounds__(128) leaf_hash_kernel(const uint64_t *evals, u
 // Proof-of-work search over witnesses [base, base + count): the challenger
 // with `n_pending` buffered inputs observes w and samples; success when the
 // sampled word (state[7] after the duplex) has its low `bits` bits zero.
+// Device copy of the host Challenger (transcript.cuh) for the FRI commit
+// loop: the same observe / sample / duplex rules on canonical words, so the
+// state read back after the loop continues the host transcript unchanged.
+struct DevCh {
+    uint64_t state[12], in[8], out[8];
+    int32_t n_in, n_out;
+    int32_t err;  // a grind witness was missing or did not satisfy its bits
+};
+__device__ __forceinline__ void dch_duplex(DevCh *c) {
+    uint64_t s[12];
+    for (int i = 0; i < 12; i++) s[i] = c->state[i];
+    for (int i = 0; i < c->n_in; i++) s[i] = c->in[i];
+    c->n_in = 0;
+    p2_permute_dev(s);
+    for (int i = 0; i < 12; i++) c->state[i] = p2w::canon(s[i]);
+    for (int i = 0; i < 8; i++) c->out[i] = c->state[i];
+    c->n_out = 8;
+}
+__device__ __forceinline__ void dch_observe(DevCh *c, uint64_t x) {
+    c->n_out = 0;
+    c->in[c->n_in++] = x;
+    if (c->n_in == 8) dch_duplex(c);
+}
+__device__ __forceinline__ uint64_t dch_sample(DevCh *c) {
+    if (c->n_in > 0 || c->n_out == 0) dch_duplex(c);
+    return c->out[--c->n_out];
+}
+// send_commit(root): record and observe the four root words (one thread)
+__global__ void fri_observe_root_kernel(DevCh *c, const uint64_t *root, uint64_t *log_root) {
+    if (threadIdx.x || blockIdx.x) return;
+    for (int i = 0; i < 4; i++) {
+        const uint64_t x = root[i];
+        log_root[i] = x;
+        dch_observe(c, x);
+    }
+}
+// grind(bits) with the witness found by grind_kernel, then sample the
+// folding challenge beta (one thread)
+__global__ void fri_after_grind_kernel(DevCh *c, uint32_t bits, const unsigned long long *found, uint64_t *log_w,
+                                       uint64_t *beta_out) {
+    if (threadIdx.x || blockIdx.x) return;
+    if (bits == 0) {
+        *log_w = 0;
+    } else {
+        uint64_t w = *found;
+        if (w == ~0ull) c->err = 1, w = 0;
+        *log_w = w;
+        dch_observe(c, w);
+        if ((dch_sample(c) & ((1ull << bits) - 1)) != 0) c->err = 1;
+    }
+    beta_out[0] = dch_sample(c);
+    beta_out[1] = dch_sample(c);
+}
+
 struct GrindArgs {
     uint64_t state[12];
     uint64_t pending[8];
@@ -117,6 +173,7 @@ struct GrindArgs {
     uint64_t base;
     uint64_t count;
     unsigned long long *found;  // atomicMin target, initialised to ~0
+    const DevCh *ch;            // if set, state and pending inputs are read from this device challenger
 };
 __global__ void __launch_bounds__(128) grind_kernel(const __grid_constant__ GrindArgs a) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -125,10 +182,18 @@ __global__ void __launch_bounds__(128) grind_kernel(const __grid_constant__ Grin
         uint64_t w = a.base + t;
         if (w >= *((volatile unsigned long long *)a.found)) return;
         uint64_t s[12];
+        if (a.ch) {
 #pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = a.state[i];
-        for (uint32_t i = 0; i < a.n_pending; i++) s[i] = a.pending[i];
-        s[a.n_pending] = w;
+            for (int i = 0; i < 12; i++) s[i] = a.ch->state[i];
+            const int np = a.ch->n_in;
+            for (int i = 0; i < np; i++) s[i] = a.ch->in[i];
+            s[np] = w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 12; i++) s[i] = a.state[i];
+            for (uint32_t i = 0; i < a.n_pending; i++) s[i] = a.pending[i];
+            s[a.n_pending] = w;
+        }
         p2_permute_dev(s);
         if ((p2w::canon(s[7]) & mask) == 0) atomicMin(a.found, (unsigned long long)w);
     }

@@ -591,12 +591,47 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         uint64_t wi = gl::inv(gl::root(log_a)), x = 1;
         for (uint64_t t = 0; t < 8; t++) winv_a[t] = x, x = gl::mul(x, wi);
     }
-    while (dom > final_dom) {
+    // The rounds run without host round trips: the challenger lives on the
+    // device for the loop (fri::DevCh). Per round: observe the root, grind,
+    // check the witness and sample beta (one-thread kernels), fold + hash the
+    // next round's leaves, compress. The roots, witnesses and the final
+    // challenger state come back in one copy after the loop.
+    const uint32_t fbits = pcs.folding_pow_bits;
+    const uint64_t n_rounds = rounds;
+    DBuf dch, droots, dwit, dbeta, dfound;
+    if (n_rounds) {
+        fri::DevCh h{};
+        memcpy(h.state, tr.ch.state, sizeof(h.state));
+        memcpy(h.in, tr.ch.in, sizeof(h.in));
+        memcpy(h.out, tr.ch.out, sizeof(h.out));
+        h.n_in = tr.ch.n_in, h.n_out = tr.ch.n_out, h.err = 0;
+        dch = ctx.alloc((sizeof(fri::DevCh) + 7) / 8);
+        uint64_t *st = ctx.stage((sizeof(fri::DevCh) + 7) / 8);
+        memcpy(st, &h, sizeof(h));
+        ctx.h2d(dch.p, st, (sizeof(fri::DevCh) + 7) / 8);
+        droots = ctx.alloc(4 * n_rounds);
+        dwit = ctx.alloc(n_rounds);
+        dbeta = ctx.alloc(2 * n_rounds);
+        dfound = ctx.alloc(n_rounds);
+        CK(cudaMemsetAsync(dfound.p, 0xff, n_rounds * 8, ctx.stream));
+    }
+    fri::DevCh *devch = (fri::DevCh *)dch.p;
+    for (uint64_t r = 0; r < n_rounds; r++) {
         Tree &cur = *next_tree;
-        tr.send_commit(cur.root);
+        L(fri::fri_observe_root_kernel, 1, 32, 0, devch, (const uint64_t *)(cur.layers.p + 4 * cur.layer_off(cur.depth)),
+          droots.p + 4 * r);
         fri_trees.push_back(std::move(next_tree));
-        grind(pcs.folding_pow_bits);
-        const gl::ef fb = tr.ch.sample_ef();
+        if (fbits) {
+            fri::GrindArgs g{};
+            g.bits = fbits;
+            g.base = 0;
+            g.count = 1ull << std::min<uint32_t>(40, fbits + 16);  // ~2^16 times the expected work
+            g.found = (unsigned long long *)(dfound.p + r);
+            g.ch = devch;
+            L(fri::grind_kernel, 148 * 2, 128, 0, g);
+        }
+        L(fri::fri_after_grind_kernel, 1, 32, 0, devch, fbits, (const unsigned long long *)(dfound.p + r), dwit.p + r,
+          dbeta.p + 2 * r);
         const uint64_t nout = dom / arity;
         DBuf out = ctx.alloc(2 * nout);
         fri::FoldArgs fa{};
@@ -606,7 +641,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         fa.log_nin = log2u(dom);
         fa.log_n0 = log_lde;
         fa.w0inv = ntt::PowTab{tw0.inv_lo.p, tw0.inv_hi.p, tw0.lo_bits};
-        fa.beta = fb;
+        fa.beta_dev = dbeta.p + 2 * r;
         memcpy(fa.winv_a, winv_a, sizeof(winv_a));
         fa.inv_a = gl::inv(arity);
         fa.out = out.p;
@@ -623,11 +658,32 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         }
         L(fri::fold_hash_kernel, blocks_for((nout + arity - 1) / arity, 128), 128, 0, fa);
         if (more) {
-            finish_tree(ctx, *nt);
+            compress_layers(ctx, *nt);
             next_tree = std::move(nt);
         }
         fri_layers.push_back(std::move(out));
         dom = nout;
+    }
+    if (n_rounds) {  // the transcript entries of the loop, in order, and the challenger
+        std::vector<uint64_t> roots(4 * n_rounds), wit(n_rounds);
+        ctx.d2h(roots.data(), droots.p, 4 * n_rounds);
+        ctx.d2h(wit.data(), dwit.p, n_rounds);
+        uint64_t *st = ctx.stage((sizeof(fri::DevCh) + 7) / 8);
+        ctx.d2h(st, dch.p, (sizeof(fri::DevCh) + 7) / 8);
+        ctx.sync();
+        fri::DevCh h;
+        memcpy(&h, st, sizeof(h));
+        if (h.err) throw CudaError{ERR_TIMEOUT, "FRI grind: no valid witness within the search bound"};
+        for (uint64_t r = 0; r < n_rounds; r++) {
+            for (int i = 0; i < 4; i++) tr.commits.push_back(roots[4 * r + i]);
+            memcpy(fri_trees[r]->root, &roots[4 * r], 32);
+            tr.fields.push_back(wit[r]);
+        }
+        memcpy(tr.ch.state, h.state, sizeof(h.state));
+        memcpy(tr.ch.in, h.in, sizeof(h.in));
+        memcpy(tr.ch.out, h.out, sizeof(h.out));
+        tr.ch.n_in = h.n_in, tr.ch.n_out = h.n_out;
+        po.d2h += 40 * n_rounds;
     }
     // final polynomial: first final_deg values, bit-reversed, iDFT, descending order
     {
