@@ -1,9 +1,12 @@
 // Batched and served proving: a pool of workers on one device, each with its
 // own context (stream, twiddle cache), pulling jobs from one queue.
 //
-// Jobs are admitted in arrival order while their estimated HBM footprint
-// fits in the budget still free (a job is always admitted when nothing else
-// runs, so an oversized job cannot starve). A worker keeps its job's LDEs,
+// Admission: a job is admitted while its estimated HBM footprint fits in the
+// budget still free (always when nothing else runs, so an oversized job
+// cannot starve), and at most one heavy job (job_is_heavy) runs at a time.
+// Jobs are taken in arrival order, except that light jobs may pass a heavy
+// job that waits for the running heavy one: they fill the GPU time the
+// heavy job leaves idle in its latency-bound phases. A worker keeps its job's LDEs,
 // trees and FRI layers on the device for the whole proof; the device
 // interleaves the kernels of up to n_workers proofs, and one proof's host
 // work (transcript, challenges) overlaps the others' device work.
@@ -43,6 +46,16 @@ inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, 
     words += 2 * nl * 3;         // DEEP row dots, layer, FRI layers
     words += 4 * nl / B;         // barycentric weights
     return words * 8 + (64ull << 20);  // plus tables and slack
+}
+
+// A job is heavy when its LDEs alone hold more than 2^26 words (512 MB):
+// its transforms and hashes fill the GPU, so a second heavy job running at
+// the same time only competes for the same integer pipes and L2.
+constexpr uint64_t kHeavyLdeWords = 1ull << 26;
+inline bool job_is_heavy(const PcsParams &pcs, const Instance *inst, size_t n) {
+    uint64_t words = 0;
+    for (size_t i = 0; i < n; i++) words += (inst[i].height << pcs.log_blowup) * inst[i].width;
+    return words > kHeavyLdeWords;
 }
 
 struct ServerJob {
@@ -112,20 +125,35 @@ class Server {
         for (;;) {
             ServerJob *job = nullptr;
             uint64_t fp = 0;
+            bool heavy = false;
             {
                 std::unique_lock<std::mutex> lk(mu_);
+                // first admissible job in arrival order (see the admission rule above)
+                auto pick = [&]() -> std::deque<ServerJob *>::iterator {
+                    for (auto it = queue_.begin(); it != queue_.end(); ++it) {
+                        ServerJob *j = *it;
+                        const uint64_t f = job_footprint_bytes(j->pcs, j->inst.data(), j->inst.size());
+                        const bool h = job_is_heavy(j->pcs, j->inst.data(), j->inst.size());
+                        const bool fits = in_use_ == 0 || in_use_ + f <= budget_;
+                        if (fits && !(h && heavy_running_)) return it;
+                        if (!fits && !h) break;  // keep arrival order among light jobs when memory is short
+                    }
+                    return queue_.end();
+                };
+                std::deque<ServerJob *>::iterator it;
                 cv_.wait(lk, [&] {
                     if (stop_) return true;
-                    if (queue_.empty()) return false;
-                    uint64_t f = job_footprint_bytes(queue_.front()->pcs, queue_.front()->inst.data(),
-                                                     queue_.front()->inst.size());
-                    return in_use_ == 0 || in_use_ + f <= budget_;
+                    it = pick();
+                    return it != queue_.end();
                 });
                 if (stop_ && queue_.empty()) return;
-                if (queue_.empty()) continue;
-                job = queue_.front();
-                queue_.pop_front();
+                it = pick();
+                if (it == queue_.end()) continue;
+                job = *it;
+                queue_.erase(it);
                 fp = job_footprint_bytes(job->pcs, job->inst.data(), job->inst.size());
+                heavy = job_is_heavy(job->pcs, job->inst.data(), job->inst.size());
+                if (heavy) heavy_running_ = true;
                 in_use_ += fp;
                 peak_ = std::max(peak_, in_use_);
             }
@@ -146,6 +174,7 @@ class Server {
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 in_use_ -= fp;
+                if (heavy) heavy_running_ = false;
                 job->status = st;
                 pending_--;
             }
@@ -162,6 +191,7 @@ class Server {
     std::condition_variable cv_, done_cv_;
     std::deque<ServerJob *> queue_;
     uint64_t in_use_ = 0, peak_ = 0;
+    bool heavy_running_ = false;
     uint64_t pending_ = 0;
     bool stop_ = false;
     std::chrono::steady_clock::time_point t0_;
