@@ -242,31 +242,34 @@ inline LdePlan lde_plan(Ctx &ctx, uint64_t h, uint32_t log_blowup, uint64_t shif
     return p;
 }
 
-template <int C, bool DIF>
+// KT: the range's bit count as a template argument (0 = read at run time);
+// the common 8-column ranges of 7..10 bits get their own instances, whose
+// round loops and index arithmetic fold at compile time.
+template <int C, bool DIF, int KT = 0>
 inline void launch_lde_pass(Ctx &ctx, const lde::PassArgs &a, uint64_t groups, unsigned n_blocks_y) {
     const uint32_t G = 1u << a.k;
     const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
     const size_t smem = ((size_t)G * C + G) * 8;
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(lde::lde_pass_kernel<C, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(lde::lde_pass_kernel<C, DIF, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (1024 * C + 1024) * 8));
     });
-    lde::lde_pass_kernel<C, DIF><<<dim3((unsigned)(groups * a.n_tiles), n_blocks_y), threads, smem, ctx.stream>>>(a);
+    lde::lde_pass_kernel<C, DIF, KT><<<dim3((unsigned)(groups * a.n_tiles), n_blocks_y), threads, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;
 }
-template <int C>
+template <int C, int KT = 0>
 inline void launch_lde_fused(Ctx &ctx, const lde::FusedArgs &a, uint64_t groups) {
     const uint32_t G = 1u << a.k;
     const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
     const size_t smem = (2 * (size_t)G * C + 3 * (size_t)G) * 8;
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(lde::lde_fused_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(lde::lde_fused_kernel<C, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (2 * 1024 * C + 3 * 1024) * 8));
     });
-    lde::lde_fused_kernel<C><<<(unsigned)(groups * a.n_tiles), threads, smem, ctx.stream>>>(a);
+    lde::lde_fused_kernel<C, KT><<<(unsigned)(groups * a.n_tiles), threads, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;
 }
@@ -274,6 +277,10 @@ template <bool DIF>
 inline void launch_lde_pass_any(Ctx &ctx, uint32_t C, const lde::PassArgs &a, uint64_t groups, unsigned ny) {
     if (C == 2) launch_lde_pass<2, DIF>(ctx, a, groups, ny);
     else if (C == 4) launch_lde_pass<4, DIF>(ctx, a, groups, ny);
+    else if (a.k == 7) launch_lde_pass<8, DIF, 7>(ctx, a, groups, ny);
+    else if (a.k == 8) launch_lde_pass<8, DIF, 8>(ctx, a, groups, ny);
+    else if (a.k == 9) launch_lde_pass<8, DIF, 9>(ctx, a, groups, ny);
+    else if (a.k == 10) launch_lde_pass<8, DIF, 10>(ctx, a, groups, ny);
     else launch_lde_pass<8, DIF>(ctx, a, groups, ny);
 }
 
@@ -332,6 +339,10 @@ inline void lde_run(Ctx &ctx, const LdePlan &p, const uint64_t *d_in, uint64_t l
         f.cp_hi_len = p.colpow_hi_len;
         if (C == 2) launch_lde_fused<2>(ctx, f, h >> f.k);
         else if (C == 4) launch_lde_fused<4>(ctx, f, h >> f.k);
+        else if (f.k == 7) launch_lde_fused<8, 7>(ctx, f, h >> f.k);
+        else if (f.k == 8) launch_lde_fused<8, 8>(ctx, f, h >> f.k);
+        else if (f.k == 9) launch_lde_fused<8, 9>(ctx, f, h >> f.k);
+        else if (f.k == 10) launch_lde_fused<8, 10>(ctx, f, h >> f.k);
         else launch_lde_fused<8>(ctx, f, h >> f.k);
     }
     for (int i = (int)n - 2; i >= 0; i--) {  // forward transform, low ranges, every coset

@@ -224,10 +224,13 @@ __device__ __forceinline__ void round(uint64_t *sm, const uint64_t *T, uint32_t 
 
 // All rounds of a k-bit range; every round ends with a block barrier.
 // tw_low: whether the round at bit 0 has a nontrivial table (base_lo != 0).
-template <int C, bool DIF>
-__device__ __forceinline__ void run_rounds(uint64_t *sm, const uint64_t *T, bool tw_low, uint32_t k, uint32_t c,
-                                           uint32_t t, uint32_t TPC) {
+template <int C, bool DIF, int KT = 0>
+__device__ __forceinline__ void run_rounds(uint64_t *sm, const uint64_t *T, bool tw_low, uint32_t k_rt, uint32_t c,
+                                           uint32_t t, uint32_t TPC_rt) {
+    const uint32_t k = KT ? (uint32_t)KT : k_rt;
+    const uint32_t TPC = KT ? (1u << KT) / 8 : TPC_rt;
     const uint32_t nr = (k + 2) / 3;
+#pragma unroll
     for (uint32_t rd = 0; rd < nr; rd++) {
         uint32_t q_lo, r;
         round_bits(DIF, k, rd, q_lo, r);
@@ -277,17 +280,19 @@ __device__ __forceinline__ void group_of(uint64_t g, uint32_t blo, uint32_t k, u
     base_lo = base & (S - 1);
 }
 
-// One range of the inverse (DIF = false) or forward (DIF = true) transform.
-template <int C, bool DIF>
+// One range of the inverse (DIF = false) or forward (DIF = true) transform;
+// KT != 0 fixes the range's bit count at compile time (blockDim = 2^KT / 8 * C).
+template <int C, bool DIF, int KT = 0>
 __global__ void __launch_bounds__(1024) lde_pass_kernel(const __grid_constant__ PassArgs a) {
     extern __shared__ uint64_t sm[];
-    const uint32_t G = 1u << a.k;
+    const uint32_t kk = KT ? (uint32_t)KT : a.k;
+    const uint32_t G = 1u << kk;
     uint64_t *T = sm + (size_t)G * C;
     const uint32_t tile = blockIdx.x % a.n_tiles;
     uint64_t base, base_lo;
-    group_of(blockIdx.x / a.n_tiles, a.blo, a.k, base, base_lo);
+    group_of(blockIdx.x / a.n_tiles, a.blo, kk, base, base_lo);
     const uint64_t col0 = (uint64_t)tile * C;
-    const uint32_t tid = threadIdx.x, c = tid % C, t = tid / C, TPC = blockDim.x / C;
+    const uint32_t tid = threadIdx.x, c = tid % C, t = tid / C, TPC = KT ? G / 8 : blockDim.x / C;
     const bool col_ok = col0 + c < a.w;
     const uint64_t *src = a.src + blockIdx.y * a.src_blk + col0 + c;
     uint64_t *dst = a.dst + blockIdx.y * a.dst_blk + col0 + c;
@@ -296,9 +301,9 @@ __global__ void __launch_bounds__(1024) lde_pass_kernel(const __grid_constant__ 
         const uint64_t row = a.src_bitrev ? gl::bitrev(P, a.L) : P;
         sm[m * C + c] = col_ok ? __ldg(src + row * a.ld_src) : 0;
     }
-    fill_table<DIF>(T, a.k, a.blo, base_lo, a.L, a.root, tid, blockDim.x);
+    fill_table<DIF>(T, kk, a.blo, base_lo, a.L, a.root, tid, blockDim.x);
     __syncthreads();
-    run_rounds<C, DIF>(sm, T, base_lo != 0, a.k, c, t, TPC);
+    run_rounds<C, DIF, KT>(sm, T, base_lo != 0, kk, c, t, TPC);
     if (!col_ok) return;
     for (uint32_t m = t; m < G; m += TPC) {
         const uint64_t P = base + ((uint64_t)m << a.blo);
@@ -308,16 +313,17 @@ __global__ void __launch_bounds__(1024) lde_pass_kernel(const __grid_constant__ 
 
 // The top range: inverse rounds, then per coset the scale and the forward
 // rounds, written to the coset's block of the output.
-template <int C>
+template <int C, int KT = 0>
 __global__ void __launch_bounds__(1024) lde_fused_kernel(const __grid_constant__ FusedArgs a) {
     extern __shared__ uint64_t sm[];
-    const uint32_t G = 1u << a.k;
+    const uint32_t kk = KT ? (uint32_t)KT : a.k;
+    const uint32_t G = 1u << kk;
     uint64_t *A = sm, *Bf = A + (size_t)G * C, *Ti = Bf + (size_t)G * C, *Tf = Ti + G, *sc = Tf + G;
     const uint32_t tile = blockIdx.x % a.n_tiles;
     uint64_t base, base_lo;
-    group_of(blockIdx.x / a.n_tiles, a.blo, a.k, base, base_lo);
+    group_of(blockIdx.x / a.n_tiles, a.blo, kk, base, base_lo);
     const uint64_t col0 = (uint64_t)tile * C;
-    const uint32_t tid = threadIdx.x, c = tid % C, t = tid / C, TPC = blockDim.x / C;
+    const uint32_t tid = threadIdx.x, c = tid % C, t = tid / C, TPC = KT ? G / 8 : blockDim.x / C;
     const uint64_t col = col0 + c;
     const bool col_ok = col < a.w;
     for (uint32_t m = t; m < G; m += TPC) {
@@ -325,10 +331,10 @@ __global__ void __launch_bounds__(1024) lde_fused_kernel(const __grid_constant__
         const uint64_t row = a.src_bitrev ? gl::bitrev(P, a.L) : P;
         A[m * C + c] = col_ok ? __ldg(a.src + row * a.ld_src + col) : 0;
     }
-    fill_table<false>(Ti, a.k, a.blo, base_lo, a.L, a.inv_root, tid, blockDim.x);
-    fill_table<true>(Tf, a.k, a.blo, base_lo, a.L, a.fwd_root, tid, blockDim.x);
+    fill_table<false>(Ti, kk, a.blo, base_lo, a.L, a.inv_root, tid, blockDim.x);
+    fill_table<true>(Tf, kk, a.blo, base_lo, a.L, a.fwd_root, tid, blockDim.x);
     __syncthreads();
-    run_rounds<C, false>(A, Ti, base_lo != 0, a.k, c, t, TPC);
+    run_rounds<C, false, KT>(A, Ti, base_lo != 0, kk, c, t, TPC);
     const uint64_t h = 1ull << a.L;
     const uint32_t B = 1u << a.log_cosets;
     const uint64_t lo_mask = (1ull << a.scale_lo_bits) - 1;
@@ -351,7 +357,7 @@ __global__ void __launch_bounds__(1024) lde_fused_kernel(const __grid_constant__
             Bf[m * C + c] = v;
         }
         __syncthreads();
-        run_rounds<C, true>(Bf, Tf, base_lo != 0, a.k, c, t, TPC);
+        run_rounds<C, true, KT>(Bf, Tf, base_lo != 0, kk, c, t, TPC);
         if (col_ok) {
             uint64_t *dst = a.dst + (uint64_t)gl::bitrev(cs, a.log_cosets) * h * a.ld_dst + col;
             for (uint32_t m = t; m < G; m += TPC) {
