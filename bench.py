@@ -42,11 +42,11 @@ METRIC = "proofs/s"
 # dram__bytes_read.sum + dram__bytes_write.sum over the slab's launches divided
 # by the slab's algorithmic bytes; the slabs of the 2^18 x 2633 trace are alike.
 LDE_TRAFFIC_PER_ALG_BYTE = 2.93
-HASH_TRAFFIC_PER_ALG_BYTE = 1.02
+HASH_TRAFFIC_PER_ALG_BYTE = 1.03
 # Binding resource of the two kernels, from the same captures (ncu
 # sm__inst_executed_pipe_alu / smsp__issue_active, % of peak).
-HASH_BINDING = "integer ALU pipe: 72.6 % of peak, issue 70.2 % (ncu, full-size slab)"
-LDE_BINDING = "integer ALU pipe: 63-72 % of peak, issue 56-67 % (ncu, full-size slab)"
+HASH_BINDING = "integer ALU pipe: 74.9 % of peak, issue 66.7 % (ncu, full-size slab)"
+LDE_BINDING = "integer ALU pipe: 74-80 % of peak, issue 60-68 % (ncu, full-size slab)"
 
 
 def load_product():
