@@ -89,25 +89,6 @@ __global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ 
     }
 }
 
-// leaves of round 0: leaf k absorbs the 2a words of EF values [k*a, k*a + a)
-__global__ void __launch_bounds__(128) leaf_hash_kernel(const uint64_t *evals, uint64_t n_leaves, uint32_t log_a,
-                                                        uint64_t *digests) {
-    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n_leaves) return;
-    const uint32_t W = 2u << log_a;
-    const uint64_t *row = evals + k * W;
-    uint64_t s[12];
-#pragma unroll
-    for (int i = 0; i < 12; i++) s[i] = 0;
-    for (uint32_t i = 0; i < W; i += 8) {
-#pragma unroll
-        for (uint32_t j = 0; j < 8; j++) s[j] = (i + j < W) ? __ldg(row + i + j) : 0;
-        p2_permute_dev(s);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) digests[4 * k + i] = p2w::canon(s[i]);
-}
-
 // Proof-of-work search over witnesses [base, base + count): the challenger
 // with `n_pending` buffered inputs observes w and samples; success when the
 // sampled word (state[7] after the duplex) has its low `bits` bits zero.

@@ -254,7 +254,6 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     using clk = std::chrono::steady_clock;
     Launcher L{ctx};
     const uint32_t lb = pcs.log_blowup;
-    const uint64_t B = 1ull << lb;
     const uint32_t log_max_h = log2u(inst[n_inst - 1].height);
     uint32_t log_qd = 0;
     for (size_t i = 0; i < n_inst; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
