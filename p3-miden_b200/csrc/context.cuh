@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -387,18 +388,36 @@ struct Tree {
 };
 
 // Compress layer 0 (already filled) up to the root (kernels only; the root
-// stays on the device); finish_tree also fetches the root.
+// stays on the device); finish_tree also fetches the root. Levels with at
+// least kWideParents parents run one thread per parent, up to four levels
+// per launch (a block keeps at least a warp's worth of parents per level);
+// levels above 128 parents run one 16-lane group per parent, one launch per
+// level; the last levels (at most 128 parents) run in one cluster launch.
+constexpr uint64_t kWideParents = 8192;
 inline void compress_layers(Ctx &ctx, Tree &t) {
     uint32_t l = 0;
-    while (l < t.depth) {
-        uint64_t n_parents = t.H >> (l + 1);
-        uint32_t blk = (uint32_t)std::min<uint64_t>(256, n_parents);
-        uint32_t levels = std::min<uint32_t>(log2u(blk) + 1, t.depth - l);
-        unsigned grid = (unsigned)(n_parents / blk);
-        merkle::compress_kernel<<<grid, blk, 0, ctx.stream>>>(t.layers.p, t.H, l, levels);
+    while (l < t.depth && (t.H >> (l + 1)) >= kWideParents) {
+        const uint64_t n_parents = t.H >> (l + 1);
+        const uint32_t blk = 256;
+        const uint32_t levels = std::min<uint32_t>({4u, log2u(n_parents) - log2u(kWideParents) + 1, t.depth - l});
+        merkle::compress_kernel<<<(unsigned)(n_parents / blk), blk, 0, ctx.stream>>>(t.layers.p, t.H, l, levels);
         CK(cudaGetLastError());
         ctx.launches++;
         l += levels;
+    }
+    while (l < t.depth && (t.H >> (l + 1)) > 128) {
+        const uint64_t n_parents = t.H >> (l + 1);
+        merkle::compress_level_coop_kernel<<<(unsigned)((n_parents * 16 + 127) / 128), 128, 0, ctx.stream>>>(
+            t.layers.p, t.H, l);
+        CK(cudaGetLastError());
+        ctx.launches++;
+        l++;
+    }
+    if (l < t.depth) {
+        merkle::compress_top_kernel<<<merkle::kTopCtas, merkle::kTopThreads, 0, ctx.stream>>>(t.layers.p, t.H, l,
+                                                                                             t.depth);
+        CK(cudaGetLastError());
+        ctx.launches++;
     }
 }
 inline void finish_tree(Ctx &ctx, Tree &t) {

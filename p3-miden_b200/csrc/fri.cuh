@@ -17,6 +17,8 @@
 
 namespace fri {
 
+__device__ __forceinline__ uint64_t merkle_shfl(uint64_t v, int src) { return p2x::shfl64(v, src); }
+
 struct FoldArgs {
     const uint64_t *in;  // n_in EF
     uint64_t n_out;      // n_in / a
@@ -89,6 +91,40 @@ __global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ 
     }
 }
 
+// The same fold and leaf hash with one 16-lane group per leaf, for rounds
+// with few leaves (latency-bound): lane u < a folds output g*a + u, the leaf
+// words (output i >> 1, component i & 1) are gathered by shuffles, and the
+// group absorbs them (overwrite mode, zero-padded 8-word chunks) with the
+// cooperative permutation.
+__global__ void __launch_bounds__(128) fold_hash_coop_kernel(const __grid_constant__ FoldArgs a) {
+    __shared__ uint64_t sc[p2::N_PARAMS];
+    p2q::stage_consts(sc);
+    const int l = threadIdx.x & 15;
+    const p2x::Lane k = p2x::lane_consts(sc, l);
+    const uint32_t A = 1u << a.log_a;
+    const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const bool ok = g * A < a.n_out;
+    const uint32_t cnt = ok ? (uint32_t)((a.n_out - g * A) < A ? (a.n_out - g * A) : A) : 0;
+    const gl::ef beta = a.beta_dev ? gl::ef{a.beta_dev[0], a.beta_dev[1]} : a.beta;
+    uint64_t c0 = 0, c1 = 0;
+    if ((uint32_t)l < cnt) {
+        const gl::ef v = fold_one(a, beta, g * A + l);
+        a.out[2 * (g * A + l)] = v.c0;
+        a.out[2 * (g * A + l) + 1] = v.c1;
+        c0 = v.c0, c1 = v.c1;
+    }
+    if (!a.digests) return;  // uniform over the grid
+    const uint32_t W = 2 * A;
+    uint64_t x = 0;
+    for (uint32_t i = 0; i < W; i += 8) {
+        const uint32_t idx = i + (l & 7);
+        const uint64_t w0 = merkle_shfl(c0, (int)(idx >> 1) & 15), w1 = merkle_shfl(c1, (int)(idx >> 1) & 15);
+        if (l < 8) x = idx < W ? ((idx & 1) ? w1 : w0) : 0;
+        x = p2x::permute(x, l, sc, k);
+    }
+    if (cnt == A && l < 4) a.digests[4 * g + l] = p2w::canon(x);
+}
+
 // Proof-of-work search over witnesses [base, base + count): the challenger
 // with `n_pending` buffered inputs observes w and samples; success when the
 // sampled word (state[7] after the duplex) has its low `bits` bits zero.
@@ -100,50 +136,92 @@ struct DevCh {
     int32_t n_in, n_out;
     int32_t err;  // a grind witness was missing or did not satisfy its bits
 };
-__device__ __forceinline__ void dch_duplex(DevCh *c) {
-    uint64_t s[12];
-    for (int i = 0; i < 12; i++) s[i] = c->state[i];
-    for (int i = 0; i < c->n_in; i++) s[i] = c->in[i];
-    c->n_in = 0;
-    p2_permute_dev(s);
-    for (int i = 0; i < 12; i++) c->state[i] = p2w::canon(s[i]);
-    for (int i = 0; i < 8; i++) c->out[i] = c->state[i];
-    c->n_out = 8;
-}
-__device__ __forceinline__ void dch_observe(DevCh *c, uint64_t x) {
-    c->n_out = 0;
-    c->in[c->n_in++] = x;
-    if (c->n_in == 8) dch_duplex(c);
-}
-__device__ __forceinline__ uint64_t dch_sample(DevCh *c) {
-    if (c->n_in > 0 || c->n_out == 0) dch_duplex(c);
-    return c->out[--c->n_out];
-}
-// send_commit(root): record and observe the four root words (one thread)
-__global__ void fri_observe_root_kernel(DevCh *c, const uint64_t *root, uint64_t *log_root) {
-    if (threadIdx.x || blockIdx.x) return;
+// Warp-cooperative challenger for the one-warp FRI kernels: the DevCh and
+// the constant table are staged in shared memory (WarpChShared), both 16-lane
+// groups of the warp run the duplex permutation (p2x; the second group
+// duplicates the first), group 0 writes the state back and lane 0 does the
+// counters. The observe / sample / duplex rules are the host Challenger's.
+struct WarpChShared {
+    DevCh c;
+    uint64_t sc[p2::N_PARAMS];
+};
+struct WarpCh {
+    WarpChShared &s;
+    p2x::Lane k;
+    int l;
+    __device__ __forceinline__ WarpCh(WarpChShared &sh, const DevCh *g) : s(sh), l(threadIdx.x & 15) {
+        const uint32_t *src = (const uint32_t *)g;
+        uint32_t *dst = (uint32_t *)&s.c;
+        for (uint32_t i = threadIdx.x; i < sizeof(DevCh) / 4; i += 32) dst[i] = src[i];
+        for (int i = threadIdx.x; i < p2::N_PARAMS; i += 32) s.sc[i] = c_p2[i];
+        __syncwarp();
+        k = p2x::lane_consts(s.sc, l);
+    }
+    __device__ __forceinline__ void store(DevCh *g) {
+        __syncwarp();
+        const uint32_t *src = (const uint32_t *)&s.c;
+        uint32_t *dst = (uint32_t *)g;
+        for (uint32_t i = threadIdx.x; i < sizeof(DevCh) / 4; i += 32) dst[i] = src[i];
+    }
+    __device__ __forceinline__ void duplex() {
+        __syncwarp();
+        uint64_t x = 0;
+        if (l < 12) x = l < s.c.n_in ? s.c.in[l] : s.c.state[l];
+        x = p2w::canon(p2x::permute(x, l, s.sc, k));
+        __syncwarp();
+        if (threadIdx.x < 12) s.c.state[l] = x;
+        if (threadIdx.x < 8) s.c.out[l] = x;
+        if (threadIdx.x == 0) s.c.n_in = 0, s.c.n_out = 8;
+        __syncwarp();
+    }
+    __device__ __forceinline__ void observe(uint64_t x) {
+        __syncwarp();
+        if (threadIdx.x == 0) s.c.n_out = 0, s.c.in[s.c.n_in++] = x;
+        __syncwarp();
+        if (s.c.n_in == 8) duplex();
+    }
+    __device__ __forceinline__ uint64_t sample() {
+        __syncwarp();
+        if (s.c.n_in > 0 || s.c.n_out == 0) duplex();
+        const uint64_t v = s.c.out[s.c.n_out - 1];
+        __syncwarp();
+        if (threadIdx.x == 0) s.c.n_out--;
+        __syncwarp();
+        return v;
+    }
+};
+// send_commit(root): record and observe the four root words (one warp)
+__global__ void __launch_bounds__(32) fri_observe_root_kernel(DevCh *c, const uint64_t *root, uint64_t *log_root) {
+    __shared__ WarpChShared sh;
+    WarpCh w(sh, c);
     for (int i = 0; i < 4; i++) {
         const uint64_t x = root[i];
-        log_root[i] = x;
-        dch_observe(c, x);
+        if (threadIdx.x == 0) log_root[i] = x;
+        w.observe(x);
     }
+    w.store(c);
 }
 // grind(bits) with the witness found by grind_kernel, then sample the
-// folding challenge beta (one thread)
-__global__ void fri_after_grind_kernel(DevCh *c, uint32_t bits, const unsigned long long *found, uint64_t *log_w,
-                                       uint64_t *beta_out) {
-    if (threadIdx.x || blockIdx.x) return;
+// folding challenge beta (one warp)
+__global__ void __launch_bounds__(32) fri_after_grind_kernel(DevCh *c, uint32_t bits, const unsigned long long *found,
+                                                             uint64_t *log_w, uint64_t *beta_out) {
+    __shared__ WarpChShared sh;
+    WarpCh w(sh, c);
     if (bits == 0) {
-        *log_w = 0;
+        if (threadIdx.x == 0) *log_w = 0;
     } else {
-        uint64_t w = *found;
-        if (w == ~0ull) c->err = 1, w = 0;
-        *log_w = w;
-        dch_observe(c, w);
-        if ((dch_sample(c) & ((1ull << bits) - 1)) != 0) c->err = 1;
+        uint64_t x = *found;
+        if (x == ~0ull) {
+            if (threadIdx.x == 0) sh.c.err = 1;
+            x = 0;
+        }
+        if (threadIdx.x == 0) *log_w = x;
+        w.observe(x);
+        if ((w.sample() & ((1ull << bits) - 1)) != 0 && threadIdx.x == 0) sh.c.err = 1;
     }
-    beta_out[0] = dch_sample(c);
-    beta_out[1] = dch_sample(c);
+    const uint64_t b0 = w.sample(), b1 = w.sample();
+    if (threadIdx.x == 0) beta_out[0] = b0, beta_out[1] = b1;
+    w.store(c);
 }
 
 struct GrindArgs {

@@ -655,7 +655,11 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             nt->layers = ctx.alloc((2 * nt->H - 1) * 4);
             fa.digests = nt->layers.p;
         }
-        L(fri::fold_hash_kernel, blocks_for((nout + arity - 1) / arity, 128), 128, 0, fa);
+        const uint64_t n_leaves = (nout + arity - 1) / arity;
+        if (more && n_leaves <= 4096)  // latency-bound: one 16-lane group per leaf
+            L(fri::fold_hash_coop_kernel, blocks_for(n_leaves * 16, 128), 128, 0, fa);
+        else
+            L(fri::fold_hash_kernel, blocks_for(n_leaves, 128), 128, 0, fa);
         if (more) {
             compress_layers(ctx, *nt);
             next_tree = std::move(nt);
