@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(128) fold_hash_kernel(const __grid_constant__ 
 // cooperative permutation.
 __global__ void __launch_bounds__(128) fold_hash_coop_kernel(const __grid_constant__ FoldArgs a) {
     __shared__ uint64_t sc[p2::N_PARAMS];
-    p2q::stage_consts(sc);
+    p2x::stage_consts(sc);
     const int l = threadIdx.x & 15;
     const p2x::Lane k = p2x::lane_consts(sc, l);
     const uint32_t A = 1u << a.log_a;

@@ -135,99 +135,23 @@ __device__ __forceinline__ void p2_permute_dev(uint64_t *s) {
     }
 }
 
-// Permutation shared by 4 lanes, for latency-bound work (a few states at a
-// time). Lane q of a group holds words q, q + 4 and q + 8 (row q of the three
-// M4 blocks), so the cross-block sums of the external layer are local and M4
-// takes three shuffled words per block. In the internal rounds every lane
-// carries a copy z of s_0: the S-box runs on z in all four lanes while the sum
-// R of s_1..s_11 is formed by a local sum of three and two butterfly steps,
-// and s_0 <- (mu_0 + 1) * S(z) + R, so only the S-box and one product lie on
-// the round's critical path. Same lazy arithmetic as p2_permute_dev (results
-// agree mod p). Eight states per warp; all 32 lanes must call it.
-//
-// `sc` is a copy of the constant table in shared memory (stage_consts), read
-// at lane-dependent offsets; `k` holds the lane's diagonal words.
-namespace p2q {
-__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
-    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src, 4);
-    const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src, 4);
-    return ((uint64_t)hi << 32) | lo;
-}
-__device__ __forceinline__ p2w::W shflW_xor(p2w::W v, int m) {
-    const uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)v.lo, m, 4);
-    const uint32_t hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(v.lo >> 32), m, 4);
-    return p2w::W{((uint64_t)hi << 32) | lo, __shfl_xor_sync(0xffffffffu, v.hi, m, 4)};
-}
+
+// Permutation shared by 16 lanes, for latency-bound work (a few states at a
+// time; about a third of the single-thread latency). Lane l < 12 holds word
+// l, lanes 12..15 hold zero between rounds. External rounds run one S-box per
+// lane and move the M4 and cross-block sums through shuffles. In the internal
+// rounds every lane carries a copy z of s_0: the S-box runs on z while the
+// sum R of s_1..s_11 is formed by a 4-step butterfly, and
+// s_0 <- (mu_0 + 1) * S(z) + R, so only the S-box and one product lie on the
+// round's critical path. Same lazy arithmetic as p2_permute_dev (results
+// agree mod p). Two states per warp; all 32 lanes must call it. `sc` is the
+// constant table staged in shared memory (stage_consts).
+namespace p2x {
 // copy the constant table into shared memory (all threads of the block call it)
 __device__ __forceinline__ void stage_consts(uint64_t *sc) {
     for (int i = threadIdx.x; i < p2::N_PARAMS; i += blockDim.x) sc[i] = c_p2[i];
     __syncthreads();
 }
-struct Lane {
-    uint64_t mu[3];  // diagonal words q, q + 4, q + 8
-    uint64_t mu0p1;  // mu_0 + 1 mod p
-};
-__device__ __forceinline__ Lane lane_consts(const uint64_t *sc, int q) {
-    Lane k;
-#pragma unroll
-    for (int c = 0; c < 3; c++) k.mu[c] = sc[p2::OFF_DIAG + 4 * c + q];
-    k.mu0p1 = gl::add_dev(sc[p2::OFF_DIAG], 1);
-    return k;
-}
-__device__ __forceinline__ void ext_linear(uint64_t *a, int q) {
-    using namespace p2w;
-    W y[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const uint64_t x0 = shfl64(a[c], 0), x1 = shfl64(a[c], 1), x2 = shfl64(a[c], 2), x3 = shfl64(a[c], 3);
-        const W t01 = wadd1(wide(x0), x1), t23 = wadd1(wide(x2), x3);
-        const W t0123 = wadd(t01, t23);
-        // M4 row q: 2x0+3x1+x2+x3 | x0+2x1+3x2+x3 | x0+x1+2x2+3x3 | 3x0+x1+x2+2x3
-        const uint64_t e = q < 2 ? x1 : x3;
-        const W f = q == 0 ? t01 : q == 1 ? wdbl(x2) : q == 2 ? t23 : wdbl(x0);
-        y[c] = wadd(wadd1(t0123, e), f);
-    }
-    const W t = wadd(wadd(y[0], y[1]), y[2]);
-#pragma unroll
-    for (int c = 0; c < 3; c++) a[c] = wreduce(wadd(y[c], t));
-}
-__device__ __forceinline__ void ext_rounds(uint64_t *a, int q, const uint64_t *rc) {
-#pragma unroll 1
-    for (int r = 0; r < 4; r++) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) a[c] = p2w::sbox(p2w::add_c(a[c], rc[12 * r + 4 * c + q]));
-        ext_linear(a, q);
-    }
-}
-__device__ __forceinline__ void permute(uint64_t *a, int q, const uint64_t *sc, const Lane &k) {
-    using namespace p2w;
-    ext_linear(a, q);
-    ext_rounds(a, q, sc + p2::OFF_INIT);
-    uint64_t z = shfl64(a[0], 0);
-#pragma unroll 1
-    for (int r = 0; r < 22; r++) {
-        const uint64_t zs = sbox(add_c(z, sc[p2::OFF_INT + r]));
-        W P = wadd1(wadd1(wide(a[1]), a[2]), q ? a[0] : 0);
-        P = wadd(P, shflW_xor(P, 1));
-        P = wadd(P, shflW_xor(P, 2));
-        const uint64_t R = wreduce(P);
-        const uint64_t sum = wreduce(wadd1(P, zs));
-        z = gl::mul_add_weak(zs, k.mu0p1, R);
-#pragma unroll
-        for (int c = 0; c < 3; c++) a[c] = gl::mul_add_weak(a[c], k.mu[c], sum);
-    }
-    if (q == 0) a[0] = z;
-    ext_rounds(a, q, sc + p2::OFF_TERM);
-}
-}  // namespace p2q
-
-// Permutation shared by 16 lanes: lane l < 12 holds word l, lanes 12..15 hold
-// zero between rounds. External rounds run one S-box per lane and move the
-// M4 and cross-block sums through shuffles; internal rounds use the same
-// replicated z = s_0 as p2q, with a 4-step butterfly for the sum of
-// s_1..s_11. Two states per warp; all 32 lanes must call it. `sc` is the
-// shared-memory constant table (p2q::stage_consts).
-namespace p2x {
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
     const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src, 16);
     const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src, 16);
@@ -410,7 +334,7 @@ __device__ __forceinline__ void compress_parent_coop(uint64_t *layers, uint64_t 
 // One level: parents of layer l_in + 1, one 16-lane group each.
 __global__ void __launch_bounds__(128) compress_level_coop_kernel(uint64_t *layers, uint64_t H, uint32_t l_in) {
     __shared__ uint64_t sc[p2::N_PARAMS];
-    p2q::stage_consts(sc);
+    p2x::stage_consts(sc);
     const int l = threadIdx.x & 15;
     const p2x::Lane k = p2x::lane_consts(sc, l);
     const uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
@@ -431,7 +355,7 @@ constexpr uint32_t kTopCtas = 8, kTopThreads = 128, kTopGroups = kTopCtas * kTop
 __global__ void __cluster_dims__(kTopCtas, 1, 1) __launch_bounds__(kTopThreads)
     compress_top_kernel(uint64_t *layers, uint64_t H, uint32_t l_in, uint32_t depth) {
     __shared__ uint64_t sc[p2::N_PARAMS];
-    p2q::stage_consts(sc);
+    p2x::stage_consts(sc);
     const int l = threadIdx.x & 15;
     const p2x::Lane k = p2x::lane_consts(sc, l);
     const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
