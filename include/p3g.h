@@ -144,6 +144,39 @@ int p3g_coset_lde_noalloc(const uint64_t *d_in, uint64_t height, uint64_t width,
                           uint64_t *d_out, void *stream);
 uint64_t p3g_coset_lde_noalloc_max_words(void);
 
+/* ------------------------------------------------------------ verifier */
+/* verify_multi (p3-miden-lifted-stark/src/verifier/mod.rs:170-364) of a
+ * proof made by p3g_prove, with the LMCS openings, the DEEP and the FRI
+ * query checks on the device and the transcript replay on the host.
+ * `instances` give the shapes only (air, height, width, consts; trace and
+ * trace_on_device are ignored). Returns P3G_OK when the check ran, with
+ * *verdict = P3G_ACCEPT or the first failing check in verify_multi's order
+ * (VerifierError, verifier/mod.rs:75-98; PcsError, p3-miden-lifted-fri/src/
+ * verifier.rs:165; FriError, fri/verifier.rs:232; DeepError,
+ * deep/verifier.rs:220; LmcsError, p3-miden-lmcs/src/lib.rs:303).
+ * P3G_ERR_INVALID for a null pointer, an unsupported parameter or a
+ * transcript word that is not a canonical field element. */
+enum p3g_verdict {
+    P3G_ACCEPT = 0,
+    P3G_VERR_SHAPE = 1,      /* instance shapes, ConstraintDegreeTooHigh */
+    P3G_VERR_OPENING = 2,    /* an opened index outside its tree */
+    P3G_VERR_ROOT = 3,       /* an opening does not hash to its commitment */
+    P3G_VERR_POW = 4,        /* a proof-of-work witness fails its bits */
+    P3G_VERR_DEEP = 5,       /* a query point equals an out-of-domain point */
+    P3G_VERR_FRI = 6,        /* a fold does not match the next round's opening */
+    P3G_VERR_FINAL = 7,      /* the final polynomial disagrees with the last fold */
+    P3G_VERR_QUOTIENT = 8,   /* ConstraintMismatch at the out-of-domain point */
+    P3G_VERR_TRANSCRIPT = 9, /* transcript too short or not fully consumed */
+    P3G_VERR_DIGEST = 10     /* transcript digest differs */
+};
+typedef struct {
+    double host_ms;   /* transcript replay and opening layout */
+    double device_ms; /* uploads, kernels and read-back */
+    uint64_t gpu_launches;
+} p3g_verify_stats;
+int p3g_verify(p3g_ctx *ctx, const p3g_pcs_params *pcs, const p3g_instance *instances, uint64_t n,
+               const uint64_t *fields, uint64_t n_fields, const uint64_t *commits, uint64_t n_commits,
+               const uint64_t *digest12, int32_t *verdict, p3g_verify_stats *stats);
 /* ------------------------------------------- batched and served proving */
 /* No counterpart in the reference: a job queue in front of p3g_prove
  * (prove_multi, p3-miden-lifted-stark/src/prover/mod.rs:223). n_workers

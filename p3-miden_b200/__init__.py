@@ -73,6 +73,10 @@ class ProofC(C.Structure):
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
+class VerifyStatsC(C.Structure):
+    _fields_ = [("host_ms", C.c_double), ("device_ms", C.c_double), ("gpu_launches", C.c_uint64)]
+
+
 def lib():
     """Load the CUDA library; raise if it has not been built."""
     global _lib
@@ -104,6 +108,8 @@ def lib():
             "p3g_keccak_inputs": (C.c_int, [C.c_uint64, C.c_uint64, u64p]),
             "p3g_cubic_trace": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, u64p, u64p]),
             "p3g_air_num_constraints": (C.c_uint64, [C.c_int32, C.c_uint64]),
+            "p3g_verify": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, u64p, C.c_uint64,
+                                     u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -348,6 +354,66 @@ def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> St
 
 def prove_single(ctx: Context, pcs: PcsParams, witness: AirWitness) -> StarkOutput:
     return prove_multi(ctx, pcs, [witness])
+
+
+# ------------------------------------------------------------- verifier
+VERDICTS = ("accept", "shape", "opening", "root", "pow", "deep", "fri", "final", "quotient", "transcript",
+            "digest")
+
+
+@dataclass
+class AirShape:
+    """The verifier's view of one instance: AIR id, trace height and width,
+    and the AIR's constants (cubic: k[w])."""
+    air: int
+    height: int
+    width: int
+    consts: np.ndarray | None = None
+
+
+@dataclass
+class VerifyResult:
+    verdict: int  # 0 = accepted, else the first failing check (VERDICTS)
+    host_ms: float
+    device_ms: float
+    gpu_launches: int
+
+    @property
+    def ok(self) -> bool:
+        return self.verdict == 0
+
+    @property
+    def name(self) -> str:
+        return VERDICTS[self.verdict]
+
+
+def verify_multi(ctx: Context, pcs: PcsParams, shapes: list[AirShape], fields: np.ndarray,
+                 commitments: np.ndarray, digest: np.ndarray) -> VerifyResult:
+    """verify_multi (p3-miden-lifted-stark/src/verifier/mod.rs:170-364) of a
+    proof of prove_multi, with the opening, DEEP and FRI query checks on the
+    GPU. Raises on a bad argument (including a transcript word >= p); a
+    rejected proof is a verdict, not an exception."""
+    n = len(shapes)
+    arr = (InstanceC * max(1, n))()
+    keep = []
+    for i, sh in enumerate(shapes):
+        c = np.ascontiguousarray(sh.consts if sh.consts is not None else np.zeros(0), dtype=np.uint64)
+        keep.append(c)
+        arr[i] = InstanceC(sh.air, 0, sh.height, sh.width, None, c.ctypes.data_as(u64p) if c.size else None, c.size)
+    f = np.ascontiguousarray(fields, dtype=np.uint64).reshape(-1)
+    cm = np.ascontiguousarray(commitments, dtype=np.uint64).reshape(-1)
+    dg = np.ascontiguousarray(digest, dtype=np.uint64).reshape(-1)
+    assert dg.size == 12 and cm.size % 4 == 0
+    pc = pcs.as_c()
+    verdict = C.c_int32(-1)
+    st = VerifyStatsC()
+    ctx.check(lib().p3g_verify(ctx.handle, C.byref(pc), arr, n, _ptr(f), f.size, _ptr(cm), cm.size // 4, _ptr(dg),
+                               C.byref(verdict), C.byref(st)))
+    return VerifyResult(int(verdict.value), float(st.host_ms), float(st.device_ms), int(st.gpu_launches))
+
+
+def verify_output(ctx: Context, pcs: PcsParams, shapes: list[AirShape], out: StarkOutput) -> VerifyResult:
+    return verify_multi(ctx, pcs, shapes, out.proof.fields, out.proof.commitments, out.digest)
 
 
 # ------------------------------------------------------- trace builders

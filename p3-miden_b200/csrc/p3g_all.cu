@@ -3,3 +3,4 @@
 #include "capi_stage.cuh"
 #include "capi_prove.cuh"
 #include "capi_server.cuh"
+#include "capi_verify.cuh"

@@ -88,10 +88,46 @@ constexpr int KC_STEP = 0, KC_EXPORT = 24, KC_PRE = 25, KC_A = 125, KC_C = 225, 
 __constant__ uint64_t c_keccak_rc[24];
 __constant__ int c_keccak_rot[25];  // rot[x*5+y]
 
-__device__ __forceinline__ uint64_t kxor2(uint64_t a, uint64_t b) { return gl::sub(gl::add(a, b), gl::dbl(gl::mul(a, b))); }
-__device__ __forceinline__ uint64_t kxor3(uint64_t a, uint64_t b, uint64_t c) { return kxor2(a, kxor2(b, c)); }
-__device__ __forceinline__ uint64_t kandn(uint64_t a, uint64_t b) { return gl::mul(gl::sub(1, a), b); }
-__device__ __forceinline__ uint64_t kbool(uint64_t a) { return gl::mul(a, gl::sub(a, 1)); }
+// The constraint bodies are generic over the value type: base-field words
+// (the prover's LDE rows, on the device) and extension elements (the
+// verifier's out-of-domain rows, on the host). fo:: overloads resolve at
+// compile time, so the base-field instance is the plain gl:: arithmetic.
+namespace fo {
+GL_HD uint64_t add(uint64_t a, uint64_t b) { return gl::add(a, b); }
+GL_HD gl::ef add(gl::ef a, gl::ef b) { return gl::ef_add(a, b); }
+GL_HD uint64_t sub(uint64_t a, uint64_t b) { return gl::sub(a, b); }
+GL_HD gl::ef sub(gl::ef a, gl::ef b) { return gl::ef_sub(a, b); }
+GL_HD uint64_t mul(uint64_t a, uint64_t b) { return gl::mul(a, b); }
+GL_HD gl::ef mul(gl::ef a, gl::ef b) { return gl::ef_mul(a, b); }
+GL_HD uint64_t dbl(uint64_t a) { return gl::dbl(a); }
+GL_HD gl::ef dbl(gl::ef a) { return gl::ef_add(a, a); }
+GL_HD uint64_t mulc(uint64_t a, uint64_t c) { return gl::mul(a, c); }  // by a base-field constant
+GL_HD gl::ef mulc(gl::ef a, uint64_t c) { return gl::ef_mulf(a, c); }
+GL_HD void konst(uint64_t c, uint64_t &out) { out = c; }
+GL_HD void konst(uint64_t c, gl::ef &out) { out = gl::ef{c, 0}; }
+template <class T>
+GL_HD T k(uint64_t c) {
+    T v;
+    konst(c, v);
+    return v;
+}
+}  // namespace fo
+
+template <class T>
+GL_HD T kxor2(T a, T b) { return fo::sub(fo::add(a, b), fo::dbl(fo::mul(a, b))); }
+template <class T>
+GL_HD T kxor3(T a, T b, T c) { return kxor2(a, kxor2(b, c)); }
+template <class T>
+GL_HD T kandn(T a, T b) { return fo::mul(fo::sub(fo::k<T>(1), a), b); }
+template <class T>
+GL_HD T kbool(T a) { return fo::mul(a, fo::sub(a, fo::k<T>(1))); }
+
+// Keccak tables for the constraint bodies: rho offsets rot[x*5+y] and the
+// round constants, from constant memory (device) or host arrays.
+struct KTabDev {
+    __device__ static int rot(int i) { return c_keccak_rot[i]; }
+    __device__ static uint64_t rc(int r) { return c_keccak_rc[r]; }
+};
 
 // Constraint indices (emission order of the AIR's eval; 3182 in total):
 //   0..23     first-row flags      24..47  flag rotation     48..147 preimage == a
@@ -114,9 +150,11 @@ struct KFold {
     }
 };
 
-__device__ __forceinline__ uint64_t kbit_b(const uint64_t *L, int bx, int by, int z) {
+#pragma nv_exec_check_disable
+template <class T, class Tab>
+GL_HD T kbit_b(const T *L, int bx, int by, int z) {
     int ax = (bx + 3 * by) % 5;
-    int rot = c_keccak_rot[ax * 5 + bx];
+    int rot = Tab::rot(ax * 5 + bx);
     return L[KC_AP + (bx * 5 + ax) * 64 + ((z + 64 - rot) & 63)];
 }
 
@@ -124,80 +162,82 @@ __device__ __forceinline__ uint64_t kbit_b(const uint64_t *L, int bx, int by, in
 // their bits, so a 16-bit limb is split into four 4-bit tasks that each add
 // alpha^k * (their part of the limb) to the fold; part 0 also subtracts
 // alpha^k * limb. All tasks then cost about the same.
-__device__ void keccak_task(int t, const uint64_t *L, const uint64_t *N, uint64_t first, uint64_t trans, KFold &f) {
-    const uint64_t not_final = gl::sub(1, L[KC_STEP + 23]);
+#pragma nv_exec_check_disable
+template <class T, class Tab, class F>
+GL_HD void keccak_task(int t, const T *L, const T *N, T first, T trans, F &f) {
+    const T not_final = fo::sub(fo::k<T>(1), L[KC_STEP + 23]);
     if (t < 400) {  // A limbs from xor(A1, C, C2), with the bools of A1
         int o = t >> 2, part = t & 3, y = o / 20, x = (o / 4) % 5, l = o % 4;
         int base = 890 + 17 * o;
-        uint64_t acc = 0;
+        T acc = fo::k<T>(0);
         for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
-            uint64_t ap = L[KC_AP + (y * 5 + x) * 64 + z];
+            T ap = L[KC_AP + (y * 5 + x) * 64 + z];
             f.emit(base + (l * 16 + 15 - z), kbool(ap));
-            acc = gl::add(gl::dbl(acc), kxor3(ap, L[KC_C + x * 64 + z], L[KC_CP + x * 64 + z]));
+            acc = fo::add(fo::dbl(acc), kxor3(ap, L[KC_C + x * 64 + z], L[KC_CP + x * 64 + z]));
         }
-        acc = gl::mul(acc, 1ull << (4 * part));
-        f.emit(base + 16, part == 0 ? gl::sub(acc, L[KC_A + o]) : acc);
+        acc = fo::mulc(acc, 1ull << (4 * part));
+        f.emit(base + 16, part == 0 ? fo::sub(acc, L[KC_A + o]) : acc);
     } else if (t < 800) {  // A2 limbs: xor(B, andn(B[x+1], B[x+2]))
         int o = (t - 400) >> 2, part = t & 3, y = o / 20, x = (o / 4) % 5, l = o % 4;
-        uint64_t acc = 0;
+        T acc = fo::k<T>(0);
         for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
-            uint64_t b0 = kbit_b(L, x, y, z), b1 = kbit_b(L, (x + 1) % 5, y, z), b2 = kbit_b(L, (x + 2) % 5, y, z);
-            acc = gl::add(gl::dbl(acc), kxor2(b0, kandn(b1, b2)));
+            T b0 = kbit_b<T, Tab>(L, x, y, z), b1 = kbit_b<T, Tab>(L, (x + 1) % 5, y, z), b2 = kbit_b<T, Tab>(L, (x + 2) % 5, y, z);
+            acc = fo::add(fo::dbl(acc), kxor2(b0, kandn(b1, b2)));
         }
-        acc = gl::mul(acc, 1ull << (4 * part));
-        f.emit(2910 + o, part == 0 ? gl::sub(acc, L[KC_APP + o]) : acc);
+        acc = fo::mulc(acc, 1ull << (4 * part));
+        f.emit(2910 + o, part == 0 ? fo::sub(acc, L[KC_APP + o]) : acc);
     } else if (t < 816) {  // A2[0][0] bits
         int l = (t - 800) >> 2, part = t & 3, base = 3010 + 17 * l;
-        uint64_t acc = 0;
+        T acc = fo::k<T>(0);
         for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
-            uint64_t bit = L[KC_APP00 + z];
+            T bit = L[KC_APP00 + z];
             f.emit(base + (l * 16 + 15 - z), kbool(bit));
-            acc = gl::add(gl::dbl(acc), bit);
+            acc = fo::add(fo::dbl(acc), bit);
         }
-        acc = gl::mul(acc, 1ull << (4 * part));
-        f.emit(base + 16, part == 0 ? gl::sub(acc, L[KC_APP + l]) : acc);
+        acc = fo::mulc(acc, 1ull << (4 * part));
+        f.emit(base + 16, part == 0 ? fo::sub(acc, L[KC_APP + l]) : acc);
     } else if (t < 832) {  // A3[0][0] = A2[0][0] xor RC
         int l = (t - 816) >> 2, part = t & 3;
-        uint64_t acc = 0;
+        T acc = fo::k<T>(0);
         for (int z = l * 16 + 4 * part + 3; z >= l * 16 + 4 * part; z--) {
-            uint64_t rcb = 0;
+            T rcb = fo::k<T>(0);
             for (int r = 0; r < 24; r++)
-                if ((c_keccak_rc[r] >> z) & 1) rcb = gl::add(rcb, L[KC_STEP + r]);
-            acc = gl::add(gl::dbl(acc), kxor2(L[KC_APP00 + z], rcb));
+                if ((Tab::rc(r) >> z) & 1) rcb = fo::add(rcb, L[KC_STEP + r]);
+            acc = fo::add(fo::dbl(acc), kxor2(L[KC_APP00 + z], rcb));
         }
-        acc = gl::mul(acc, 1ull << (4 * part));
-        f.emit(3078 + l, part == 0 ? gl::sub(acc, L[KC_APPP00 + l]) : acc);
+        acc = fo::mulc(acc, 1ull << (4 * part));
+        f.emit(3078 + l, part == 0 ? fo::sub(acc, L[KC_APPP00 + l]) : acc);
     } else if (t < 1152) {  // (x, z): bool C, C2 xor, A1 column sum
         int i = t - 832, x = i / 64, z = i % 64;
-        uint64_t cxz = L[KC_C + i];
+        T cxz = L[KC_C + i];
         f.emit(250 + 2 * i, kbool(cxz));
-        uint64_t v = kxor3(cxz, L[KC_C + ((x + 4) % 5) * 64 + z], L[KC_C + ((x + 1) % 5) * 64 + ((z + 63) & 63)]);
-        uint64_t cp = L[KC_CP + i];
-        f.emit(251 + 2 * i, gl::sub(cp, v));
-        uint64_t sm = 0;
-        for (int y = 0; y < 5; y++) sm = gl::add(sm, L[KC_AP + (y * 5 + x) * 64 + z]);
-        uint64_t d = gl::sub(sm, cp);
-        f.emit(2590 + i, gl::mul(gl::mul(d, gl::sub(d, 2)), gl::sub(d, 4)));
+        T v = kxor3(cxz, L[KC_C + ((x + 4) % 5) * 64 + z], L[KC_C + ((x + 1) % 5) * 64 + ((z + 63) & 63)]);
+        T cp = L[KC_CP + i];
+        f.emit(251 + 2 * i, fo::sub(cp, v));
+        T sm = fo::k<T>(0);
+        for (int y = 0; y < 5; y++) sm = fo::add(sm, L[KC_AP + (y * 5 + x) * 64 + z]);
+        T d = fo::sub(sm, cp);
+        f.emit(2590 + i, fo::mul(fo::mul(d, fo::sub(d, fo::k<T>(2))), fo::sub(d, fo::k<T>(4))));
     } else if (t < 1176) {  // first-row flags
         int i = t - 1152;
-        f.emit(i, gl::mul(first, i == 0 ? gl::sub(L[KC_STEP], 1) : L[KC_STEP + i]));
+        f.emit(i, fo::mul(first, i == 0 ? fo::sub(L[KC_STEP], fo::k<T>(1)) : L[KC_STEP + i]));
     } else if (t < 1200) {  // flag rotation
         int i = t - 1176;
-        f.emit(24 + i, gl::mul(trans, gl::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
+        f.emit(24 + i, fo::mul(trans, fo::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
     } else if (t < 1300) {  // first step: preimage == a
         int o = t - 1200;
-        f.emit(48 + o, gl::mul(L[KC_STEP], gl::sub(L[KC_PRE + o], L[KC_A + o])));
+        f.emit(48 + o, fo::mul(L[KC_STEP], fo::sub(L[KC_PRE + o], L[KC_A + o])));
     } else if (t < 1302) {  // export
-        uint64_t ex = L[KC_EXPORT];
+        T ex = L[KC_EXPORT];
         if (t == 1300) f.emit(148, kbool(ex));
-        else f.emit(149, gl::mul(not_final, ex));
+        else f.emit(149, fo::mul(not_final, ex));
     } else if (t < 1402) {  // preimage continuity
         int o = t - 1302;
-        f.emit(150 + o, gl::mul(gl::mul(not_final, trans), gl::sub(L[KC_PRE + o], N[KC_PRE + o])));
+        f.emit(150 + o, fo::mul(fo::mul(not_final, trans), fo::sub(L[KC_PRE + o], N[KC_PRE + o])));
     } else {  // round output == next round input (x outer, y inner)
         int i = t - 1402, x = i / 20, y = (i / 4) % 5, l = i % 4;
-        uint64_t outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
-        f.emit(3082 + i, gl::mul(gl::mul(not_final, trans), gl::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
+        T outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
+        f.emit(3082 + i, fo::mul(fo::mul(not_final, trans), fo::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
     }
 }
 
@@ -240,7 +280,7 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
         const uint64_t *N = ring + ((m + 2) % 3) * KC_NCOLS;
         const uint64_t first = sel[2 * (j & (KEC_THREADS - 1))], trans = sel[2 * (j & (KEC_THREADS - 1)) + 1];
         KFold f(a.alpha_pows);
-        for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task(t, L, N, first, trans, f);
+        for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task<uint64_t, KTabDev>(t, L, N, first, trans, f);
         uint64_t c0 = f.c0.reduce(), c1 = f.c1.reduce();
 #pragma unroll
         for (int off = 16; off; off >>= 1) {

@@ -99,8 +99,13 @@ def test_keccak_headline_2e18_verifies(product, gpu_ctx):
     # a proof for other inputs does not verify against this statement's transcript
     bad = gpu.proof.fields.copy()
     bad[len(bad) // 2] ^= 1
-    assert O.verify(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)], bad,
-                    gpu.proof.commitments, gpu.digest) != 0
+    rc = O.verify(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)], bad,
+                  gpu.proof.commitments, gpu.digest)
+    assert rc != 0
+    # the device verifier: accepts the proof, and agrees on the perturbed one
+    shapes = [product.AirShape(product.AIR_KECCAK, t.shape[0], t.shape[1])]
+    assert product.verify_output(gpu_ctx, pcs, shapes, gpu).ok
+    assert product.verify_multi(gpu_ctx, pcs, shapes, bad, gpu.proof.commitments, gpu.digest).verdict == rc
 
 
 def test_lifted_config_full_size_verifies(product, gpu_ctx):
@@ -114,3 +119,4 @@ def test_lifted_config_full_size_verifies(product, gpu_ctx):
     pcs = product.PcsParams(3, 2, 0, 16, 0, 100, 0)
     gpu = product.prove_multi(gpu_ctx, pcs, inst)
     check_verifies(gpu, pcs, meta)
+    assert product.verify_output(gpu_ctx, pcs, [product.AirShape(*m) for m in meta], gpu).ok
