@@ -421,6 +421,64 @@ def run_named(args):
     return 0
 
 
+def run_verify(args):
+    """Verification of the headline proof (2^18 x 2633 Keccak, the example's
+    parameters) through the public call p3g_verify: transcript replay on the
+    host, openings, DEEP and FRI query checks on the GPU. The proof is made
+    once; each step verifies it from host memory (wall clock around the call,
+    host and device parts reported). The verifier restatement (oracle) times
+    the same check on one host core beside it."""
+    import torch
+    dev = 0
+    torch.cuda.set_device(dev)
+    P = load_product()
+    ctx = P.Context(dev)
+    t = P.generate_keccak_trace(P.keccak_inputs(1, N_PERMS))
+    pcs = P.PcsParams(**PCS)
+    out = P.prove_multi(ctx, pcs, [P.AirWitness(P.AIR_KECCAK, torch.from_numpy(t.view(np.int64)).to(f"cuda:{dev}"))])
+    del t
+    shapes = [P.AirShape(P.AIR_KECCAK, 1 << LOG_H, 2633)]
+    for _ in range(args.warmup):
+        assert P.verify_output(ctx, pcs, shapes, out).ok
+    wall, host, device, launches = [], [], [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = P.verify_output(ctx, pcs, shapes, out)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        assert r.ok, r.name
+        host.append(r.host_ms), device.append(r.device_ms)
+        launches += r.gpu_launches
+    value = 1e3 / statistics.median(wall)
+    line = {
+        "metric": "verifications/s", "value": value, "unit": "verifications/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.median(wall), "higher_is_better": True,
+        "dtype": "u64 (Goldilocks, exact)", "data": "synthetic (seeded Keccak-f inputs); proof from p3g_prove",
+        "config": {"workload": f"verify_multi of the {WORKLOAD} proof", "pcs": PCS,
+                   "proof_bytes": int(out.proof.fields.nbytes + out.proof.commitments.nbytes)},
+        "split_ms": {"host replay + layout (median)": statistics.median(host),
+                     "device: upload, kernels, read-back (median)": statistics.median(device)},
+        "gpu_launches": launches,
+        "e2e": {"value": value, "unit": "verifications/s",
+                "h2d_bytes_per_step": int(out.proof.fields.nbytes + out.proof.commitments.nbytes),
+                "d2h_bytes_per_step": 0},
+    }
+    if args.cpu_baseline:
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_ffi as O
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            rc = O.verify(O.default_p2(), PCS, [(O.AIR_KECCAK, 1 << LOG_H, 2633, None)], out.proof.fields,
+                          out.proof.commitments, out.digest)
+            times.append(time.perf_counter() - t0)
+            assert rc == 0
+        line["cpu_baseline"] = {"value": 1.0 / min(times), "unit": "verifications/s", "cores": 1, "kind": "port",
+                                "sample": "the verifier restatement on the same proof, one host thread"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_slab(args):
     """One full-size column slab of the headline workload through the public
     LDE and LMCS entry points (2^18 x 336 seeded words, log_blowup 1, then the
@@ -495,8 +553,8 @@ def build_jobs(P, specs, device, pinned):
     return jobs
 
 
-def run_pool(P, jobs, workers, device, budget):
-    srv = P.ProofServer(device, n_workers=workers, hbm_budget=budget)
+def run_pool(P, jobs, workers, device, budget, self_check=False):
+    srv = P.ProofServer(device, n_workers=workers, hbm_budget=budget, self_check=self_check)
     try:
         t0 = time.perf_counter()
         res = srv.run(jobs)
@@ -565,18 +623,24 @@ def run_serve(args):
     stream = [P.Job(pool[k].pcs, pool[k].instances, float(a)) for k, a in zip(picks, arrivals)]
     run_pool(P, pool, 1, dev, args.budget)  # warm-up over every distinct job
     out = {}
-    for name, workers in (("plain", 1), ("served", args.workers)):
-        res, span, wall, lat, peak = run_pool(P, stream, workers, dev, args.budget)
+    arms = [("plain", 1, False), ("served", args.workers, False)]
+    if args.self_check:  # every served proof verified on the device before it is returned
+        arms.append(("served+self-check", args.workers, True))
+    for name, workers, check in arms:
+        res, span, wall, lat, peak = run_pool(P, stream, workers, dev, args.budget, self_check=check)
         out[name] = {"proofs_per_s": len(stream) / span, "p50_ms": float(np.percentile(lat, 50)),
                      "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "peak_admitted_gb": peak / 1e9,
                      "workers": workers}
+        if check:
+            assert all(r.verdict == 0 for r in res)
+            out[name]["verify_ms_mean"] = float(np.mean([r.verify_ms for r in res]))
     line = {
         "metric": "served proofs/s and p50/p99 latency", "unit": "proofs/s", "value": out["served"]["proofs_per_s"],
         "higher_is_better": True, "n_gpus": 1, "jobs": args.jobs, "arrival_rate_per_s": args.rate,
         "dtype": "u64 (Goldilocks, exact)", "data": "synthetic seeded job pool, Poisson arrivals, pinned host traces",
         "config": {"workload": "job pool: 60% cubic AIR 2^12..2^20 x {16..512}, 40% Keccak AIR 2^12..2^16",
                    "pool": args.pool, "pcs": MIX_PCS, "hbm_budget": args.budget},
-        "plain": out["plain"], "served": out["served"],
+        **out,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -591,10 +655,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--log-h", type=int, default=18,
                     help="trace height (log2); 18 is the measured workload, smaller values are profiling cases")
-    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve", "slab"],
+    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve", "slab", "verify"],
                     help="keccak: the plain prover at scale (headline); small: 42-permutation Keccak proof; "
                          "lifted: three cubic traces lifted to 2^20; batch: 64-proof uneven mix; serve: Poisson stream; "
-                         "slab: one 2^18 x 336 column slab through the LDE and the tree (kernel profiling)")
+                         "slab: one 2^18 x 336 column slab through the LDE and the tree (kernel profiling); "
+                         "verify: the device-side verifier on the headline proof")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3, help="batch: alternating passes per arm (median kept)")
@@ -602,6 +667,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--budget", type=float, default=150e9, help="HBM admission budget in bytes")
     ap.add_argument("--seed", type=int, default=2025)
+    ap.add_argument("--self-check", action="store_true", help="serve: add an arm that verifies every proof on the device")
     ap.add_argument("--max-log-cubic", type=int, default=18)
     ap.add_argument("--max-log-keccak", type=int, default=16)
     args = ap.parse_args()
@@ -619,6 +685,8 @@ def main():
         return run_reference(args)
     if args.workload == "slab":
         return run_slab(args)
+    if args.workload == "verify":
+        return run_verify(args)
     return run_gpu(args)
 
 

@@ -30,7 +30,8 @@ enum p3g_status {
     P3G_ERR_VALIDATION = 2, /* ProverError / AirValidationError equivalents */
     P3G_ERR_OOM = 3,        /* device allocation refused */
     P3G_ERR_TIMEOUT = 4,    /* a bounded search gave up (proof-of-work) */
-    P3G_ERR_CUDA = 5        /* other CUDA runtime error */
+    P3G_ERR_CUDA = 5,       /* other CUDA runtime error */
+    P3G_ERR_REJECTED = 6    /* a served proof failed the server's self-check (p3g_server_set_self_check) */
 };
 
 enum p3g_air {
@@ -195,13 +196,18 @@ typedef struct {
 } p3g_job;
 typedef struct {
     int32_t status;    /* the job's own status; other jobs are unaffected by it */
-    int32_t pad;
+    int32_t verdict;   /* self-check verdict (enum p3g_verdict), -1 when not checked */
     p3g_proof proof;   /* valid when status == P3G_OK; release with p3g_proof_free */
     double submit_s, start_s, end_s;
+    double verify_ms;  /* self-check wall time */
 } p3g_job_result;
 
 int p3g_server_create(int device, const uint64_t *poseidon2_params130, uint32_t n_workers,
                       uint64_t hbm_budget_bytes, p3g_server **out);
+/* No counterpart in the reference. With self-check on, each worker verifies
+ * its proof with p3g_verify's checks, on its own stream, before the job ends;
+ * a rejected proof ends the job with P3G_ERR_REJECTED and its verdict. */
+int p3g_server_set_self_check(p3g_server *srv, int32_t enabled);
 /* Waits for every submitted job, then releases the workers. */
 void p3g_server_destroy(p3g_server *srv);
 int p3g_server_submit(p3g_server *srv, const p3g_job *job, uint64_t *ticket);

@@ -29,7 +29,7 @@ KECCAK_ROWS_PER_HASH = 24
 u64p = C.POINTER(C.c_uint64)
 
 # status codes (include/p3g.h)
-OK, ERR_INVALID, ERR_VALIDATION, ERR_OOM, ERR_TIMEOUT, ERR_CUDA = range(6)
+OK, ERR_INVALID, ERR_VALIDATION, ERR_OOM, ERR_TIMEOUT, ERR_CUDA, ERR_REJECTED = range(7)
 
 
 class P3gError(RuntimeError):
@@ -466,8 +466,8 @@ class JobC(C.Structure):
 
 
 class JobResultC(C.Structure):
-    _fields_ = [("status", C.c_int32), ("pad", C.c_int32), ("proof", ProofC),
-                ("submit_s", C.c_double), ("start_s", C.c_double), ("end_s", C.c_double)]
+    _fields_ = [("status", C.c_int32), ("verdict", C.c_int32), ("proof", ProofC),
+                ("submit_s", C.c_double), ("start_s", C.c_double), ("end_s", C.c_double), ("verify_ms", C.c_double)]
 
 
 @dataclass
@@ -484,6 +484,8 @@ class JobResult:
     submit_s: float
     start_s: float
     end_s: float
+    verdict: int = -1  # self-check verdict (VERDICTS index), -1 when not checked
+    verify_ms: float = 0.0
 
     @property
     def latency_s(self) -> float:
@@ -519,7 +521,7 @@ def _result_from_c(r: JobResultC) -> JobResult:
                           list(p.stage_ms[:len(STAGES)]), int(p.gpu_launches), int(p.h2d_bytes),
                           int(p.d2h_bytes), float(p.stage_ms[11]))
         lib().p3g_proof_free(C.byref(r.proof))
-    return JobResult(int(r.status), out, r.submit_s, r.start_s, r.end_s)
+    return JobResult(int(r.status), out, r.submit_s, r.start_s, r.end_s, int(r.verdict), float(r.verify_ms))
 
 
 class ProofServer:
@@ -527,7 +529,7 @@ class ProofServer:
     device, admitted by estimated HBM footprint against hbm_budget bytes."""
 
     def __init__(self, device: int = 0, n_workers: int = 4, hbm_budget: int = 150 * 10**9,
-                 poseidon2_params: np.ndarray | None = None):
+                 poseidon2_params: np.ndarray | None = None, self_check: bool = False):
         L = lib()
         vp = C.c_void_p
         for name, res, args in [
@@ -537,6 +539,7 @@ class ProofServer:
             ("p3g_server_wait", C.c_int, [vp, C.c_uint64, C.POINTER(JobResultC)]),
             ("p3g_server_run", C.c_int, [vp, C.POINTER(JobC), C.c_uint64, C.POINTER(JobResultC)]),
             ("p3g_server_peak_admitted_bytes", C.c_uint64, [vp]),
+            ("p3g_server_set_self_check", C.c_int, [vp, C.c_int32]),
             ("p3g_job_footprint_bytes", C.c_uint64, [C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64]),
         ]:
             fn = getattr(L, name)
@@ -546,6 +549,8 @@ class ProofServer:
         _check(L.p3g_server_create(device, _ptr(params), n_workers, int(hbm_budget), C.byref(self._h)))
         self.n_workers = n_workers
         self._pending = {}
+        if self_check:
+            _check(L.p3g_server_set_self_check(self._h, 1))
 
     def run(self, jobs: list[Job]) -> list[JobResult]:
         """Submit every job at its arrival time (seconds from now) and wait for all."""

@@ -14,9 +14,10 @@ struct p3g_job_c {
 };
 struct p3g_job_result_c {
     int32_t status;
-    int32_t pad;
+    int32_t verdict;  // self-check verdict, -1 when not checked
     p3g_proof_c proof;
     double submit_s, start_s, end_s;
+    double verify_ms;
 };
 
 struct p3g_server {
@@ -56,6 +57,8 @@ inline std::unique_ptr<ServerJob> make_job(const p3g_job_c &j) {
 inline void fill_result(const ServerJob &job, p3g_job_result_c *r) {
     memset(r, 0, sizeof(*r));
     r->status = job.status;
+    r->verdict = job.verdict;
+    r->verify_ms = job.verify_ms;
     r->submit_s = job.submit_s;
     r->start_s = job.start_s;
     r->end_s = job.end_s;
@@ -94,6 +97,12 @@ P3G_API void p3g_server_destroy(p3g_server *srv) {
 
 // Enqueue a job now (its arrival_s is ignored); traces stay borrowed until
 // p3g_server_wait returns for the ticket.
+P3G_API int p3g_server_set_self_check(p3g_server *srv, int32_t enabled) {
+    if (!srv) return p3g::ERR_INVALID;
+    srv->s->set_self_check(enabled != 0);
+    return p3g::OK;
+}
+
 P3G_API int p3g_server_submit(p3g_server *srv, const p3g_job_c *job, uint64_t *ticket) {
     if (!srv || !job || !ticket) return p3g::ERR_INVALID;
     int v = p3g::validate(&job->pcs, job->instances, job->n_instances);

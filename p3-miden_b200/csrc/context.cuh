@@ -27,6 +27,7 @@ enum Status : int {
     ERR_OOM = 3,         // device allocation refused
     ERR_TIMEOUT = 4,     // a bounded device-side search gave up
     ERR_CUDA = 5,        // other CUDA runtime error
+    ERR_REJECTED = 6,    // the server's self-check rejected the proof
 };
 
 struct CudaError {

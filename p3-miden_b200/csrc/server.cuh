@@ -21,6 +21,7 @@
 #include <thread>
 
 #include "prover.cuh"
+#include "verifier.cuh"
 
 namespace p3g {
 
@@ -65,6 +66,8 @@ struct ServerJob {
     // results
     int status = -1;
     ProofOut out;
+    int verdict = -1;      // self-check verdict (vfy::Verdict), -1 when not checked
+    double verify_ms = 0;  // self-check wall time
     double submit_s = 0, start_s = 0, end_s = 0;
     std::string error;
 };
@@ -117,6 +120,10 @@ class Server {
         done_cv_.wait(lk, [&] { return pending_ == 0; });
     }
     uint64_t peak_bytes() const { return peak_; }
+    // Verify each proof on the device before returning it (vfy::verify, on
+    // the worker's own stream); a rejected proof ends its job with
+    // ERR_REJECTED.
+    void set_self_check(bool on) { self_check_ = on; }
 
    private:
     void worker(uint32_t w) {
@@ -161,6 +168,19 @@ class Server {
             int st = OK;
             try {
                 prove(ctx, job->pcs, job->inst.data(), job->inst.size(), job->out);
+                if (self_check_) {
+                    const auto v0 = std::chrono::steady_clock::now();
+                    const ProofOut &o = job->out;
+                    job->verdict = vfy::verify(ctx, job->pcs, job->inst.data(), job->inst.size(), o.fields.data(),
+                                               o.fields.size(), o.commits.data(), o.commits.size() / 4, o.digest,
+                                               nullptr);
+                    job->verify_ms =
+                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - v0).count();
+                    if (job->verdict != vfy::ACCEPT) {
+                        st = ERR_REJECTED;
+                        job->error = "self-check rejected the proof (verdict " + std::to_string(job->verdict) + ")";
+                    }
+                }
             } catch (const CudaError &e) {
                 st = e.status;
                 job->error = e.what;
@@ -194,6 +214,7 @@ class Server {
     bool heavy_running_ = false;
     uint64_t pending_ = 0;
     bool stop_ = false;
+    std::atomic<bool> self_check_{false};
     std::chrono::steady_clock::time_point t0_;
 };
 

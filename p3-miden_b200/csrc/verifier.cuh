@@ -228,6 +228,11 @@ __global__ void __launch_bounds__(256) fri_kernel(const __grid_constant__ FriArg
     }
 }
 
+// the digests at the given pool slots, side by side
+__global__ void gather_roots_kernel(const uint64_t *pool, const uint32_t *slots, uint32_t n, uint64_t *out) {
+    for (uint32_t i = threadIdx.x; i < 4 * n; i += blockDim.x) out[i] = pool[4 * (uint64_t)slots[i / 4] + i % 4];
+}
+
 // -------------------------------------------------------------- host side
 
 struct KTabHost {
@@ -534,9 +539,9 @@ inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         memcpy(dg, c.state, sizeof(dg));
     }
 
-    // quotient identity at z (host, one extension-field evaluation)
-    bool quotient_ok;
-    {
+    // quotient identity at z: one extension-field evaluation on the host,
+    // run while the device kernels are in flight
+    auto quotient_identity = [&]() -> bool {
         gl::ef accumulated = gl::ef_zero();
         uint64_t off = 0;
         for (size_t i = 0; i < n_inst; i++) {
@@ -567,125 +572,147 @@ inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         }
         const gl::ef qz = gl::ef_mul(num, gl::ef_inv(den));
         const gl::ef vanish = gl::ef_sub(gl::ef_exp2k(z, log_max_h), gl::ef_one());
-        quotient_ok = gl::ef_eq(accumulated, gl::ef_mul(qz, vanish));
-    }
+        return gl::ef_eq(accumulated, gl::ef_mul(qz, vanish));
+    };
 
-    // device: leaf sponges, tree levels, DEEP values, FRI rounds
+    // device: one upload of every input, then the leaf sponges, the tree
+    // levels, the DEEP values, the FRI rounds and one read-back of the roots
+    // and flags
     const uint32_t n_nodes = P.n_nodes;
     auto slot = [&](uint32_t s) { return (s & kHint) ? n_nodes + (s & ~kHint) : s; };
-    for (auto &lv : P.levels)
-        for (auto &j : lv) j.left = slot(j.left), j.right = slot(j.right);
+    std::vector<CJob> cj;
+    std::vector<size_t> lv_off{0};
+    for (auto &lv : P.levels) {
+        for (const CJob &jb : lv) cj.push_back(CJob{slot(jb.left), slot(jb.right), jb.out});
+        lv_off.push_back(cj.size());
+    }
+    bool trace_ok = true, fri_shape_ok = true;
+    for (int g = 0; g < 3; g++) trace_ok = trace_ok && !P.batches[g].bad_index;
+    for (uint64_t rr = 0; rr < rounds; rr++) fri_shape_ok = fri_shape_ok && !P.batches[3 + rr].bad_index;
+    const bool run_deep = trace_ok && nq, run_fri = run_deep && fri_shape_ok;
+    std::vector<uint64_t> apow, xq;
+    if (run_deep) {
+        apow.resize(2 * total_aligned);
+        gl::ef pw = gl::ef_one();
+        for (uint64_t i = total_aligned; i-- > 0;) apow[2 * i] = pw.c0, apow[2 * i + 1] = pw.c1, pw = gl::ef_mul(pw, ac);
+        xq.resize(nq);
+        const uint64_t gen = gl::root(log_lde);
+        for (uint64_t q = 0; q < nq; q++) xq[q] = gl::mul(gl::GEN, gl::pow(gen, gl::bitrev(idx[q], log_lde)));
+    }
+    std::vector<uint32_t> root_slot;
+    for (const Batch &B : P.batches) root_slot.push_back(B.bad_index || B.no_root ? 0 : B.root);
+    struct Seg {
+        const void *src;
+        size_t bytes, off;
+    };
+    std::vector<Seg> segs;
+    size_t words = 0;
+    auto seg = [&](const void *src, size_t bytes) {
+        segs.push_back(Seg{src, bytes, words});
+        words += (bytes + 7) / 8 + 1;  // one spare word keeps every segment non-empty
+        return segs.back().off;
+    };
+    const size_t o_rows = seg(P.rows.data(), P.rows.size() * 8);
+    const size_t o_widths = seg(P.widths.data(), P.widths.size() * 4);
+    const size_t o_leaves = seg(P.leaves.data(), P.leaves.size() * sizeof(LeafJob));
+    const size_t o_cj = seg(cj.data(), cj.size() * sizeof(CJob));
+    const size_t o_apow = seg(apow.data(), apow.size() * 8);
+    const size_t o_xq = seg(xq.data(), xq.size() * 8);
+    const size_t o_rounds = seg(fr.data(), fr.size() * sizeof(FriRound));
+    const size_t o_ek = seg(ent_k.data(), ent_k.size() * 4);
+    const size_t o_ep = seg(ent_pos.data(), ent_pos.size() * 4);
+    const size_t o_sinv = seg(s_inv.data(), s_inv.size() * 8);
+    const size_t o_fx = seg(final_x.data(), final_x.size() * 8);
+    const size_t o_fp = seg(final_poly.data(), final_poly.size() * 8);
+    const size_t o_rs = seg(root_slot.data(), root_slot.size() * 4);
+    const size_t staged = words;
+    const size_t o_hints = seg(P.hints.data(), P.hints.size() * 8);  // copied into the pool
+    const size_t pool_words = 4 * (uint64_t)n_nodes + P.hints.size() + 4;
+    const uint64_t n_flags = 2 + rounds;
+    const size_t back_words = 4 * P.batches.size() + (n_flags + 1) / 2;  // roots, then flags
     const uint64_t launches0 = ctx.launches;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     const auto t1 = std::chrono::steady_clock::now();
+    DBuf d = ctx.alloc(staged + pool_words + 3 * (2 * nq + 2) + back_words);
+    uint64_t *pool = d.p + staged, *de = pool + pool_words, *cur = de + 2 * nq + 2, *nxt = cur + 2 * nq + 2;
+    uint64_t *back = nxt + 2 * nq + 2;
+    uint64_t *st = ctx.stage(std::max(words, back_words));
+    for (const Seg &sg : segs)
+        if (sg.bytes) memcpy(st + sg.off, sg.src, sg.bytes);
     CK(cudaEventRecord(e0, ctx.stream));
-    DBuf d_rows = ctx.upload(P.rows.empty() ? std::vector<uint64_t>{0} : P.rows);
-    DBuf d_widths = ctx.upload(pack(P.widths.empty() ? std::vector<uint32_t>{0} : P.widths));
-    DBuf d_pool = ctx.alloc(4 * (uint64_t)n_nodes + P.hints.size() + 4);
-    if (!P.hints.empty()) {
-        DBuf h = ctx.upload(P.hints);
-        CK(cudaMemcpyAsync(d_pool.p + 4 * (uint64_t)n_nodes, h.p, P.hints.size() * 8, cudaMemcpyDeviceToDevice,
-                           ctx.stream));
-        ctx.sync();
-    }
+    ctx.h2d(d.p, st, staged);
+    ctx.h2d(pool + 4 * (uint64_t)n_nodes, st + o_hints, P.hints.size());
+    CK(cudaMemsetAsync(back, 0, back_words * 8, ctx.stream));
+    int32_t *d_flags = (int32_t *)(back + 4 * P.batches.size());
     if (!P.leaves.empty()) {
-        DBuf d_leaves = ctx.upload(pack(P.leaves));
         const uint32_t n = (uint32_t)P.leaves.size();
-        leaf_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)d_leaves.p, n, d_rows.p,
-                                                                  (const uint32_t *)d_widths.p, d_pool.p);
+        leaf_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)(d.p + o_leaves), n, d.p + o_rows,
+                                                                  (const uint32_t *)(d.p + o_widths), pool);
         CK(cudaGetLastError());
         ctx.launches++;
-        ctx.sync();
     }
-    for (auto &lv : P.levels) {
-        if (lv.empty()) continue;
-        DBuf d_jobs = ctx.upload(pack(lv));
-        const uint32_t n = (uint32_t)lv.size();
-        compress_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const CJob *)d_jobs.p, n, d_pool.p);
+    for (size_t l = 0; l + 1 < lv_off.size(); l++) {
+        const uint32_t n = (uint32_t)(lv_off[l + 1] - lv_off[l]);
+        if (!n) continue;
+        compress_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const CJob *)(d.p + o_cj) + lv_off[l], n,
+                                                                      pool);
         CK(cudaGetLastError());
         ctx.launches++;
-        ctx.sync();
     }
-    const uint64_t n_flags = 2 + rounds;
-    DBuf d_flags = ctx.alloc((n_flags + 1) / 2);
-    CK(cudaMemsetAsync(d_flags.p, 0, ((n_flags + 1) / 2) * 8, ctx.stream));
-    DBuf d_de = ctx.alloc(2 * nq + 2);
-    bool deep_bad = false, final_bad = false;
-    std::vector<int32_t> flags(n_flags, 0);
-    const bool trace_ok = !P.batches[0].bad_index && !P.batches[1].bad_index && !P.batches[2].bad_index;
-    if (trace_ok && nq) {
-        std::vector<uint64_t> apow(2 * total_aligned);
-        gl::ef pw = gl::ef_one();
-        for (uint64_t i = total_aligned; i-- > 0;) apow[2 * i] = pw.c0, apow[2 * i + 1] = pw.c1, pw = gl::ef_mul(pw, ac);
-        std::vector<uint64_t> xq(nq);
-        const uint64_t gen = gl::root(log_lde);
-        for (uint64_t q = 0; q < nq; q++) xq[q] = gl::mul(gl::GEN, gl::pow(gen, gl::bitrev(idx[q], log_lde)));
-        DBuf d_apow = ctx.upload(apow), d_xq = ctx.upload(xq);
+    if (run_deep) {
         DeepArgs da{};
-        da.rows = d_rows.p;
+        da.rows = d.p + o_rows;
         for (int g = 0; g < 3; g++) da.goff[g] = P.batches[g].row_off, da.gtw[g] = P.batches[g].tw;
-        da.apow = d_apow.p;
-        da.xq = d_xq.p;
+        da.apow = d.p + o_apow;
+        da.xq = d.p + o_xq;
         da.nq = (uint32_t)nq;
         da.red_open[0] = red_open[0], da.red_open[1] = red_open[1];
         da.zs[0] = zs[0], da.zs[1] = zs[1];
         da.bp = bp;
-        da.de = d_de.p;
-        da.flags = (int32_t *)d_flags.p;
+        da.de = de;
+        da.flags = d_flags;
         deep_kernel<<<(unsigned)((nq * 32 + 127) / 128), 128, 0, ctx.stream>>>(da);
         CK(cudaGetLastError());
         ctx.launches++;
-        bool fri_shape_ok = true;
-        for (uint64_t rr = 0; rr < rounds; rr++) fri_shape_ok = fri_shape_ok && !P.batches[3 + rr].bad_index;
-        if (fri_shape_ok) {
-            DBuf d_rounds = ctx.upload(pack(fr.empty() ? std::vector<FriRound>(1) : fr));
-            DBuf d_ek = ctx.upload(pack(ent_k.empty() ? std::vector<uint32_t>{0} : ent_k));
-            DBuf d_ep = ctx.upload(pack(ent_pos.empty() ? std::vector<uint32_t>{0} : ent_pos));
-            DBuf d_sinv = ctx.upload(s_inv.empty() ? std::vector<uint64_t>{0} : s_inv);
-            DBuf d_fx = ctx.upload(final_x.empty() ? std::vector<uint64_t>{0} : final_x);
-            DBuf d_fp = ctx.upload(final_poly.empty() ? std::vector<uint64_t>{0} : final_poly);
-            DBuf d_cur = ctx.alloc(2 * nq + 2), d_nxt = ctx.alloc(2 * nq + 2);
-            FriArgs fa{};
-            fa.rows = d_rows.p;
-            fa.rounds = (const FriRound *)d_rounds.p;
-            fa.n_rounds = (uint32_t)rounds;
-            fa.log_a = log_a;
-            fa.ent_k = (const uint32_t *)d_ek.p;
-            fa.ent_pos = (const uint32_t *)d_ep.p;
-            fa.s_inv = d_sinv.p;
-            {
-                const uint64_t wi = gl::inv(gl::root(log_a));
-                uint64_t x = 1;
-                for (uint64_t t = 0; t < 8; t++) fa.winv_a[t] = x, x = gl::mul(x, wi);
-            }
-            fa.inv_a = gl::inv(arity);
-            fa.de = d_de.p;
-            fa.cur = d_cur.p, fa.nxt = d_nxt.p;
-            fa.n_final = (uint32_t)final_x.size();
-            fa.final_x = d_fx.p;
-            fa.final_poly = d_fp.p;
-            fa.final_deg = (uint32_t)final_deg;
-            fa.flags = (int32_t *)d_flags.p;
-            fri_kernel<<<1, 256, 0, ctx.stream>>>(fa);
-            CK(cudaGetLastError());
-            ctx.launches++;
-            ctx.sync();
-        }
     }
-    // roots and flags back
-    std::vector<uint64_t> roots(4 * P.batches.size() + 4);
-    for (size_t b = 0; b < P.batches.size(); b++)
-        if (!P.batches[b].bad_index && !P.batches[b].no_root)
-            ctx.d2h(roots.data() + 4 * b, d_pool.p + 4 * (uint64_t)P.batches[b].root, 4);
-    std::vector<uint64_t> fw((n_flags + 1) / 2);
-    ctx.d2h(fw.data(), d_flags.p, fw.size());
+    if (run_fri) {
+        FriArgs fa{};
+        fa.rows = d.p + o_rows;
+        fa.rounds = (const FriRound *)(d.p + o_rounds);
+        fa.n_rounds = (uint32_t)rounds;
+        fa.log_a = log_a;
+        fa.ent_k = (const uint32_t *)(d.p + o_ek);
+        fa.ent_pos = (const uint32_t *)(d.p + o_ep);
+        fa.s_inv = d.p + o_sinv;
+        const uint64_t wi = gl::inv(gl::root(log_a));
+        uint64_t x = 1;
+        for (uint64_t t = 0; t < 8; t++) fa.winv_a[t] = x, x = gl::mul(x, wi);
+        fa.inv_a = gl::inv(arity);
+        fa.de = de;
+        fa.cur = cur, fa.nxt = nxt;
+        fa.n_final = (uint32_t)final_x.size();
+        fa.final_x = d.p + o_fx;
+        fa.final_poly = d.p + o_fp;
+        fa.final_deg = (uint32_t)final_deg;
+        fa.flags = d_flags;
+        fri_kernel<<<1, 256, 0, ctx.stream>>>(fa);
+        CK(cudaGetLastError());
+        ctx.launches++;
+    }
+    gather_roots_kernel<<<1, 128, 0, ctx.stream>>>(pool, (const uint32_t *)(d.p + o_rs),
+                                                   (uint32_t)P.batches.size(), back);
+    CK(cudaGetLastError());
+    ctx.launches++;
+    ctx.d2h(st, back, back_words);
     CK(cudaEventRecord(e1, ctx.stream));
+    const bool quotient_ok = quotient_identity();
     ctx.sync();
-    memcpy(flags.data(), fw.data(), n_flags * 4);
-    deep_bad = flags[0] != 0;
-    final_bad = flags[1] != 0;
+    std::vector<uint64_t> roots(st, st + 4 * P.batches.size());
+    std::vector<int32_t> flags(n_flags);
+    memcpy(flags.data(), st + 4 * P.batches.size(), n_flags * 4);
+    const bool deep_bad = flags[0] != 0, final_bad = flags[1] != 0;
     float dev_ms = 0;
     CK(cudaEventElapsedTime(&dev_ms, e0, e1));
     cudaEventDestroy(e0);

@@ -97,3 +97,24 @@ def test_submit_wait_from_python(product, gpu_ctx):
     for j, r in zip(jobs, res):
         alone = product.prove_multi(gpu_ctx, j.pcs, j.instances)
         assert r.status == product.OK and np.array_equal(alone.digest, r.output.digest)
+
+
+def test_self_check(product, gpu_ctx):
+    """With self-check on, every served proof is verified on the device
+    before its job ends; the proofs are the same as without it."""
+    jobs = mix(product, n=6, seed=11)
+    srv = product.ProofServer(0, n_workers=3, self_check=True)
+    try:
+        res = srv.run(jobs)
+    finally:
+        srv.close()
+    for j, r in zip(jobs, res):
+        assert r.status == product.OK and r.verdict == 0 and r.verify_ms > 0
+        alone = product.prove_multi(gpu_ctx, j.pcs, j.instances)
+        assert np.array_equal(alone.digest, r.output.digest)
+    srv = product.ProofServer(0, n_workers=2)
+    try:
+        plain = srv.run(jobs[:2])
+    finally:
+        srv.close()
+    assert all(r.verdict == -1 for r in plain)
