@@ -388,6 +388,17 @@ struct Tree {
     uint64_t layer_off(uint32_t l) const { return 2 * H - 2 * (H >> l); }
 };
 
+// Leaf sponge of one height class of n leaves: one thread per leaf, or one
+// 16-lane group per leaf when the class is small (latency-bound).
+inline void launch_leaf_class(Ctx &ctx, const merkle::ClassArgs &a, uint64_t n) {
+    if (n <= merkle::kCoopLeaves)
+        merkle::leaf_class_coop_kernel<<<(unsigned)((n * 16 + 127) / 128), 128, 0, ctx.stream>>>(a);
+    else
+        merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
+    CK(cudaGetLastError());
+    ctx.launches++;
+}
+
 // Compress layer 0 (already filled) up to the root (kernels only; the root
 // stays on the device); finish_tree also fetches the root. Levels with at
 // least kWideParents parents run one thread per parent, up to four levels
@@ -503,10 +514,7 @@ inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t
         uint64_t *out_states = (li % 2 == 0) ? st_a.p : st_b.p;
         a.states_out = last ? nullptr : out_states;
         a.digests_out = last ? t.layers.p : nullptr;
-        uint64_t n = launches[li].h;
-        merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
-        CK(cudaGetLastError());
-        ctx.launches++;
+        launch_leaf_class(ctx, a, launches[li].h);
         prev = out_states;
         prev_log = a.log_h;
     }

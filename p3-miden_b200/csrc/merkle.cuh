@@ -267,6 +267,40 @@ __global__ void __launch_bounds__(128) leaf_class_kernel(const __grid_constant__
     }
 }
 
+// The same leaf sponge with one 16-lane group per leaf (p2x), for classes
+// with few leaves, where one thread per leaf leaves the GPU nearly empty and
+// each of a row's chained permutations costs the full single-thread latency.
+// States are weakly reduced like leaf_class_kernel's (congruent mod p, not
+// always the same words), so classes may mix the two kernels.
+constexpr uint64_t kCoopLeaves = 4096;
+__global__ void __launch_bounds__(128) leaf_class_coop_kernel(const __grid_constant__ ClassArgs a) {
+    __shared__ uint64_t sc[p2::N_PARAMS];
+    p2x::stage_consts(sc);
+    const int l = threadIdx.x & 15;
+    const p2x::Lane k = p2x::lane_consts(sc, l);
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (((t & ~31ull) >> 4) >> a.log_h) return;  // warp-uniform: the warp's first leaf is past the class
+    const uint64_t j = t >> 4;
+    const bool ok = (j >> a.log_h) == 0;
+    uint64_t x = 0;
+    if (ok && a.prev && l < 12) x = a.prev[(j >> (a.log_h - a.prev_log_h)) * 12 + l];
+    for (int m = 0; m < a.n_mats; m++) {
+        const uint64_t w = a.width[m];
+        const uint64_t *row = a.data[m] + (ok ? j : 0) * a.ld[m];
+#pragma unroll 1
+        for (uint64_t i = 0; i < w; i += 8) {
+            if (l < 8) x = ok && i + l < w ? __ldg(row + i + l) : 0;
+            x = p2x::permute(x, l, sc, k);
+        }
+    }
+    if (!ok) return;
+    if (a.digests_out) {
+        if (l < 4) a.digests_out[j * 4 + l] = p2w::canon(x);
+    } else if (l < 12) {
+        a.states_out[j * 12 + l] = x;
+    }
+}
+
 __device__ __forceinline__ void compress2(const uint64_t *l, const uint64_t *r, uint64_t *out) {
     uint64_t s[12];
 #pragma unroll

@@ -228,10 +228,7 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
         uint64_t *out_states = st[s & 1].p;
         a.states_out = last ? nullptr : out_states;
         a.digests_out = last ? t.layers.p : nullptr;
-        const uint64_t n = h << lb;
-        merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
-        CK(cudaGetLastError());
-        ctx.launches++;
+        launch_leaf_class(ctx, a, h << lb);
         prev = out_states;
         prev_log = a.log_h;
     }
