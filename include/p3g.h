@@ -109,6 +109,15 @@ int p3g_coset_lde(p3g_ctx *ctx, const uint64_t *d_in, uint64_t height, uint64_t 
  * alignment 1 = build_tree, 8 = build_aligned_tree (the sponge rate). */
 int p3g_lmcs_build(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
                    uint64_t n, uint32_t alignment, p3g_tree **out);
+/* HidingLmcsConfig::build_tree / build_aligned_tree (p3-miden-lmcs/src/
+ * hiding_lmcs.rs:112-145): as p3g_lmcs_build, and after the matrices every
+ * leaf absorbs its row of d_salt (tree height x salt_width, row-major, on the
+ * device; the config draws it from its RNG, here the caller supplies it and
+ * it stays borrowed). p3g_lmcs_prove_batch then hints each index's salt,
+ * unpadded, after its rows (lifted_tree.rs:189-192). */
+int p3g_lmcs_build_hiding(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights,
+                          const uint64_t *widths, uint64_t n, uint32_t alignment, const uint64_t *d_salt,
+                          uint64_t salt_width, p3g_tree **out);
 /* LmcsTree::root (lib.rs:264) */
 int p3g_lmcs_root(const p3g_tree *tree, uint64_t *out4);
 /* digest layer `level` (0 = leaves) copied to host: (height >> level) x 4 words */

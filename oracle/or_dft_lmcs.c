@@ -78,8 +78,11 @@ void or_coset_lde_bitrev(const uint64_t *in, size_t h, size_t w, unsigned log_bl
  * when the height grows, each state is duplicated into a contiguous block
  * (nearest-neighbour upsampling, :385-437); squeeze; then compress pairs
  * layer by layer (:494-539). The alignment only affects hints. */
-void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment) {
+static void tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment,
+                       const uint64_t *salt, size_t salt_width) {
     memset(t, 0, sizeof(*t));
+    t->salt = salt;
+    t->salt_width = salt ? salt_width : 0;
     t->n_mats = n;
     for (size_t i = 0; i < n; i++) t->mats[i] = mats[i];
     t->alignment = alignment ? alignment : 1;
@@ -101,6 +104,12 @@ void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, si
         for (size_t r = 0; r < h; r++) or_sponge_absorb(pp, states + r * 12, d + r * w, w);
         active = h;
     }
+    /* hiding: the salt row, one more absorb call per leaf
+     * (p3-miden-lmcs/src/lifted_tree.rs:271-279) */
+    if (t->salt_width) {
+#pragma omp parallel for schedule(static)
+        for (size_t r = 0; r < H; r++) or_sponge_absorb(pp, states + r * 12, salt + r * salt_width, salt_width);
+    }
     size_t total = 2 * H - 1;
     t->layers = (uint64_t *)malloc(total * 32);
     for (size_t i = 0; i < H; i++) memcpy(t->layers + 4 * i, states + 12 * i, 32);
@@ -117,6 +126,15 @@ void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, si
         off = noff;
         len = nlen;
     }
+}
+void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment) {
+    tree_build(pp, t, mats, n, alignment, NULL, 0);
+}
+/* HidingLmcsConfig::build_tree / build_aligned_tree (hiding_lmcs.rs:112-145)
+ * with the caller's salt matrix in place of the config's RNG draw */
+void or_tree_build_hiding(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment,
+                          const uint64_t *salt, size_t salt_width) {
+    tree_build(pp, t, mats, n, alignment, salt, salt_width);
 }
 void or_tree_root(const or_tree *t, uint64_t out[4]) { memcpy(out, t->layers + 4 * t->layer_off[t->depth], 32); }
 void or_tree_free(or_tree *t) {
@@ -139,6 +157,8 @@ void or_tree_prove_batch(const or_tree *t, const size_t *idx, size_t n_idx, or_t
             size_t w = M->width, aw = (w + t->alignment - 1) / t->alignment * t->alignment;
             for (size_t c = 0; c < aw; c++) or_tr_hint_field(tr, c < w ? M->data[row * w + c] : 0);
         }
+        /* hiding: the leaf's salt, unpadded (lifted_tree.rs:189-192) */
+        for (size_t c = 0; c < t->salt_width; c++) or_tr_hint_field(tr, t->salt[idx[q] * t->salt_width + c]);
     }
     (void)H;
     size_t *known = (size_t *)malloc((n_idx + 1) * sizeof(size_t));

@@ -90,8 +90,13 @@ typedef struct {
     unsigned depth;       /* log2 of the tree height */
     uint64_t *layers;     /* all digest layers, leaves first, 4 words each */
     size_t layer_off[40]; /* offset (in digests) of layer l */
+    const uint64_t *salt; /* hiding LMCS: height x salt_width, or NULL */
+    size_t salt_width;
 } or_tree;
 void or_tree_build(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment);
+/* HidingLmcsConfig: each leaf absorbs its salt row after the matrices */
+void or_tree_build_hiding(const or_p2_params *pp, or_tree *t, const or_matrix *mats, size_t n, size_t alignment,
+                          const uint64_t *salt, size_t salt_width);
 void or_tree_root(const or_tree *t, uint64_t out[4]);
 void or_tree_free(or_tree *t);
 void or_tree_prove_batch(const or_tree *t, const size_t *sorted_unique_idx, size_t n_idx, or_transcript *tr);

@@ -93,6 +93,8 @@ def lib():
             "p3g_poseidon2_params_from_seed": (None, [C.c_uint64, u64p, u64p]),
             "p3g_coset_lde": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_void_p]),
             "p3g_lmcs_build": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32, C.POINTER(vp)]),
+            "p3g_lmcs_build_hiding": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32,
+                                                C.c_void_p, C.c_uint64, C.POINTER(vp)]),
             "p3g_lmcs_root": (C.c_int, [vp, u64p]),
             "p3g_lmcs_layer": (C.c_int, [vp, vp, C.c_uint32, u64p]),
             "p3g_lmcs_free": (None, [vp]),
@@ -204,9 +206,12 @@ def coset_lde(ctx: Context, trace_dev, log_blowup: int, shift: int):
 
 
 class LmcsTree:
-    """LmcsTree over device matrices (ascending heights)."""
+    """LmcsTree over device matrices (ascending heights). With `salt_dev`
+    (tree height x SALT, on the device) the hiding LMCS
+    (p3-miden-lmcs/src/hiding_lmcs.rs): each leaf absorbs its salt row last,
+    and openings carry the salt after the rows."""
 
-    def __init__(self, ctx: Context, mats_dev, alignment: int):
+    def __init__(self, ctx: Context, mats_dev, alignment: int, salt_dev=None):
         import torch
         torch.cuda.synchronize(ctx.device)
         self.ctx = ctx
@@ -216,7 +221,15 @@ class LmcsTree:
         hs = np.array([m.shape[0] for m in mats_dev], dtype=np.uint64)
         ws = np.array([m.shape[1] for m in mats_dev], dtype=np.uint64)
         self._h = C.c_void_p()
-        ctx.check(lib().p3g_lmcs_build(ctx.handle, ptrs, _ptr(hs), _ptr(ws), n, alignment, C.byref(self._h)))
+        self.salt_width = 0
+        if salt_dev is None:
+            ctx.check(lib().p3g_lmcs_build(ctx.handle, ptrs, _ptr(hs), _ptr(ws), n, alignment, C.byref(self._h)))
+        else:
+            assert salt_dev.shape[0] == int(hs[-1])
+            self._salt = salt_dev
+            self.salt_width = int(salt_dev.shape[1])
+            ctx.check(lib().p3g_lmcs_build_hiding(ctx.handle, ptrs, _ptr(hs), _ptr(ws), n, alignment,
+                                                  salt_dev.data_ptr(), self.salt_width, C.byref(self._h)))
         self.height = int(hs[-1])
         self.depth = self.height.bit_length() - 1
 
@@ -233,7 +246,7 @@ class LmcsTree:
 
     def prove_batch(self, indices):
         idx = np.array(sorted(set(int(i) for i in indices)), dtype=np.uint64)
-        cap_f = len(idx) * sum(((m.shape[1] + 7) // 8) * 8 for m in self._keep) + 16
+        cap_f = len(idx) * (sum(((m.shape[1] + 7) // 8) * 8 for m in self._keep) + self.salt_width) + 16
         cap_c = len(idx) * (self.depth + 1) + 4
         fields = np.zeros(cap_f, dtype=np.uint64)
         commits = np.zeros((cap_c, 4), dtype=np.uint64)

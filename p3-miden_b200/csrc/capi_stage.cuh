@@ -93,6 +93,37 @@ P3G_API int p3g_lmcs_build(p3g_ctx *x, const uint64_t *const *d_mats, const uint
     return p3g::OK;
 }
 
+// HidingLmcsConfig::build_tree / build_aligned_tree
+// (p3-miden-lmcs/src/hiding_lmcs.rs:112-145) with the caller's salt matrix
+// (tree height x salt_width, row-major, on the device; borrowed like the
+// matrices).
+P3G_API int p3g_lmcs_build_hiding(p3g_ctx *x, const uint64_t *const *d_mats, const uint64_t *heights,
+                                  const uint64_t *widths, uint64_t n, uint32_t alignment, const uint64_t *d_salt,
+                                  uint64_t salt_width, p3g_tree **out) {
+    if (!x || !d_mats || !heights || !widths || !out || !d_salt || n == 0 || n > 64) return p3g::ERR_INVALID;
+    if (salt_width == 0 || salt_width > 4096) return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++) {
+        if (heights[i] == 0 || (heights[i] & (heights[i] - 1))) return p3g::ERR_INVALID;
+        if (i && heights[i] < heights[i - 1]) return p3g::ERR_VALIDATION;
+    }
+    *out = nullptr;
+    p3g_tree *t = new p3g_tree();
+    try {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<p3g::Mat> mats;
+        for (uint64_t i = 0; i < n; i++) mats.push_back({d_mats[i], heights[i], widths[i]});
+        const p3g::Mat salt{d_salt, heights[n - 1], salt_width};
+        p3g::build_tree(x->c, t->t, mats, alignment, &salt);
+        x->c.sync();
+    } catch (const p3g::CudaError &e) {
+        x->c.last_error = e.what;
+        delete t;
+        return e.status;
+    }
+    *out = t;
+    return p3g::OK;
+}
+
 P3G_API int p3g_lmcs_root(const p3g_tree *t, uint64_t *out4) {
     if (!t || !out4) return p3g::ERR_INVALID;
     memcpy(out4, t->t.root, 32);

@@ -384,6 +384,7 @@ struct Tree {
     uint64_t H = 0;
     uint32_t alignment = 1;
     std::vector<Mat> mats;
+    Mat salt{nullptr, 0, 0};  // hiding LMCS: H x SALT per-leaf salt, absorbed last (borrowed)
     uint64_t root[4] = {0, 0, 0, 0};
     uint64_t layer_off(uint32_t l) const { return 2 * H - 2 * (H >> l); }
 };
@@ -473,12 +474,21 @@ inline void build_zero_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uin
     memcpy(t.root, &c[4 * t.depth], 32);
 }
 
-inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats, uint32_t alignment) {
-    t.mats = mats;
+// With `salt` (hiding LMCS, p3-miden-lmcs/src/hiding_lmcs.rs:59-189 and
+// lifted_tree.rs:265-283): after every matrix, each leaf absorbs its salt row
+// (one more overwrite-mode absorb call), then squeezes.
+inline void build_tree(Ctx &ctx, Tree &t, const std::vector<Mat> &mats_in, uint32_t alignment,
+                       const Mat *salt = nullptr) {
+    t.mats = mats_in;
     t.alignment = alignment ? alignment : 1;
-    t.H = mats.back().h;
+    t.H = mats_in.back().h;
     t.depth = log2u(t.H);
     t.layers = ctx.alloc((2 * t.H - 1) * 4);
+    std::vector<Mat> mats = mats_in;  // absorption order: the matrices, then the salt
+    if (salt) {
+        t.salt = *salt;
+        mats.push_back(*salt);
+    }
     // height classes in order; at most MAX_MATS matrices per launch
     struct Launch {
         std::vector<size_t> idx;

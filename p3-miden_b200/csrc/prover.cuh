@@ -74,13 +74,15 @@ struct OpeningPlan {
     std::vector<const uint64_t *> sibs;
 };
 inline void plan_openings(const Tree &t, const std::vector<uint64_t> &idx, OpeningPlan &p) {
-    for (uint64_t i : idx)
+    for (uint64_t i : idx) {
         for (const Mat &m : t.mats) {
             uint32_t lift = t.depth - log2u(m.h);
             uint64_t r = i >> lift;
             uint64_t pad = (m.w + t.alignment - 1) / t.alignment * t.alignment;
             p.rows.push_back({m.d + r * m.w, m.w, pad});
         }
+        if (t.salt.d) p.rows.push_back({t.salt.d + i * t.salt.w, t.salt.w, t.salt.w});  // salt: unpadded
+    }
     std::vector<uint64_t> known = idx;
     for (uint32_t l = 0; l < t.depth; l++) {
         std::vector<uint64_t> parents;
@@ -730,20 +732,28 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         for (auto &r : p.rows) segs.push_back({r.src, r.len, total}), total += r.len;
         for (auto *s : p.sibs) segs.push_back({s, 4, total}), total += 4;
     }
-    std::vector<uint64_t> gathered(total);
+    const uint64_t *gathered = nullptr;  // pinned staging (the gathered hints)
     if (!segs.empty()) {
-        DBuf d_segs = ctx.alloc(segs.size() * 3);
         DBuf d_out = ctx.alloc(total);
         std::vector<uint64_t> raw(segs.size() * 3);
         memcpy(raw.data(), segs.data(), segs.size() * sizeof(Seg));
         DBuf up = ctx.upload(raw);
         L(gather_kernel, (unsigned)std::min<size_t>(segs.size(), 65535), 128, 0, (const Seg *)up.p, (uint64_t)segs.size(),
           d_out.p);
-        ctx.d2h(gathered.data(), d_out.p, total);
+        uint64_t *st = ctx.stage(total);
+        ctx.d2h(st, d_out.p, total);
         ctx.sync();
+        gathered = st;
         po.d2h += 8 * total;
     }
     {
+        uint64_t n_hint_fields = 0, n_hint_commits = 0;
+        for (auto &p : plans) {
+            for (auto &r : p.rows) n_hint_fields += r.padded;
+            n_hint_commits += 4 * p.sibs.size();
+        }
+        tr.fields.reserve(tr.fields.size() + n_hint_fields);
+        tr.commits.reserve(tr.commits.size() + n_hint_commits);
         uint64_t off = 0;
         for (auto &p : plans) {
             for (auto &r : p.rows) {

@@ -55,7 +55,8 @@ class Matrix(C.Structure):
 
 class Tree(C.Structure):
     _fields_ = [("n_mats", C.c_size_t), ("mats", Matrix * 8), ("alignment", C.c_size_t),
-                ("depth", C.c_uint), ("layers", u64p), ("layer_off", C.c_size_t * 40)]
+                ("depth", C.c_uint), ("layers", u64p), ("layer_off", C.c_size_t * 40),
+                ("salt", u64p), ("salt_width", C.c_size_t)]
 
 
 class Challenger(C.Structure):
@@ -106,6 +107,8 @@ def lib():
             ("or_coset_lde_bitrev", None, [u64p, C.c_size_t, C.c_size_t, C.c_uint, C.c_uint64, u64p]),
             ("or_tree_build", None, [C.POINTER(P2Params), C.POINTER(Tree), C.POINTER(Matrix), C.c_size_t, C.c_size_t]),
             ("or_tree_root", None, [C.POINTER(Tree), u64p]),
+            ("or_tree_build_hiding", None, [C.POINTER(P2Params), C.POINTER(Tree), C.POINTER(Matrix), C.c_size_t,
+                                            C.c_size_t, u64p, C.c_size_t]),
             ("or_tree_free", None, [C.POINTER(Tree)]),
             ("or_tree_prove_batch", None, [C.POINTER(Tree), C.POINTER(C.c_size_t), C.c_size_t, C.POINTER(Transcript)]),
             ("or_tr_init", None, [C.POINTER(Transcript), C.POINTER(P2Params)]),
@@ -167,16 +170,22 @@ def coset_lde_bitrev(trace: np.ndarray, log_blowup: int, shift: int) -> np.ndarr
 
 
 class OracleTree:
-    """LMCS tree over row-major matrices (ascending heights)."""
+    """LMCS tree over row-major matrices (ascending heights); with `salt`
+    (tree height x SALT) the hiding LMCS."""
 
-    def __init__(self, pp: P2Params, mats, alignment: int):
+    def __init__(self, pp: P2Params, mats, alignment: int, salt=None):
         self._keep = [np.ascontiguousarray(m, dtype=np.uint64) for m in mats]
         arr = (Matrix * len(mats))()
         for i, m in enumerate(self._keep):
             arr[i] = Matrix(ptr(m), m.shape[0], m.shape[1])
         self.t = Tree()
         self.pp = pp
-        lib().or_tree_build(C.byref(pp), C.byref(self.t), arr, len(mats), alignment)
+        if salt is None:
+            lib().or_tree_build(C.byref(pp), C.byref(self.t), arr, len(mats), alignment)
+        else:
+            s = np.ascontiguousarray(salt, dtype=np.uint64)
+            self._keep.append(s)
+            lib().or_tree_build_hiding(C.byref(pp), C.byref(self.t), arr, len(mats), alignment, ptr(s), s.shape[1])
 
     def root(self) -> np.ndarray:
         r = np.zeros(4, dtype=np.uint64)

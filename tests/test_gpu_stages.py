@@ -80,3 +80,27 @@ def test_keccak_trace_device_matches_host(product, gpu_ctx, n_perms, log_h):
                                                                                   device="cuda:0")
     dev = product.generate_keccak_trace_device(gpu_ctx, d_in, log_h)
     assert np.array_equal(product.to_host(dev), host)
+
+
+@pytest.mark.parametrize("scenario", [0, 2, 3, 6, 9])
+@pytest.mark.parametrize("alignment", [1, 8])
+@pytest.mark.parametrize("salt_w", [0, 1, 4, 9])
+def test_lmcs_prove_batch_and_hiding_match_oracle(product, gpu_ctx, scenario, alignment, salt_w):
+    """LmcsTree::prove_batch hints (rows padded to the alignment, then the
+    siblings) and the hiding LMCS (a per-leaf salt absorbed last, hinted
+    unpadded after the rows) equal the oracle's."""
+    rng = np.random.default_rng(100 + scenario)
+    mats = [rand_mat(rng, h, w) for h, w in SCENARIOS[scenario]]
+    H = mats[-1].shape[0]
+    salt = rand_mat(rng, H, salt_w) if salt_w else None
+    pp = O.default_p2()
+    ot = O.OracleTree(pp, mats, alignment, salt)
+    gt = product.LmcsTree(gpu_ctx, [product.to_device(m) for m in mats], alignment,
+                          product.to_device(salt) if salt_w else None)
+    assert np.array_equal(gt.root(), ot.root())
+    for l in range(gt.depth + 1):
+        assert np.array_equal(gt.layer(l), ot.layer(l))
+    idx = sorted(set(rng.integers(0, H, size=min(H, 13)).tolist()))
+    fg, cg = gt.prove_batch(idx)
+    fo, co = ot.prove_batch(idx)
+    assert np.array_equal(fg, fo) and np.array_equal(cg, co)

@@ -224,3 +224,20 @@ def test_verifier_rejects_tampering():
     k2 = k.copy()
     k2[0] = (int(k2[0]) + 1) % (2**64 - 2**32 + 1)
     assert O.verify(pp, pcs, [(O.AIR_CUBIC, t.shape[0], t.shape[1], k2)], f, c, d) == 8  # quotient identity
+
+
+def test_hiding_tree_is_one_more_absorb():
+    """Hiding LMCS (p3-miden-lmcs/src/lifted_tree.rs:271-279): the salt row is
+    one more absorb call per leaf, so the root equals the plain tree's over
+    the matrices plus the salt as a last full-height matrix; the salt is
+    hinted unpadded after each index's rows."""
+    rng = np.random.default_rng(4)
+    pp = O.default_p2()
+    mats = [rng.integers(0, O.P, size=(h, w), dtype=np.uint64) for h, w in [(4, 7), (8, 8), (16, 11)]]
+    salt = rng.integers(0, O.P, size=(16, 5), dtype=np.uint64)
+    hid = O.OracleTree(pp, mats, 8, salt)
+    assert np.array_equal(hid.root(), O.OracleTree(pp, mats + [salt], 1).root())
+    assert not np.array_equal(hid.root(), O.OracleTree(pp, mats, 8).root())
+    f, c = hid.prove_batch([3, 9])
+    assert f.size == 2 * (8 + 8 + 16 + 5)
+    assert np.array_equal(f[8 + 8 + 16:8 + 8 + 16 + 5], salt[3])
