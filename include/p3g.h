@@ -187,6 +187,23 @@ typedef struct {
 int p3g_verify(p3g_ctx *ctx, const p3g_pcs_params *pcs, const p3g_instance *instances, uint64_t n,
                const uint64_t *fields, uint64_t n_fields, const uint64_t *commits, uint64_t n_commits,
                const uint64_t *digest12, int32_t *verdict, p3g_verify_stats *stats);
+/* No counterpart in the reference: verify_multi of n proofs in one call. The
+ * transcript replays run on up to host_threads host threads (0: one per
+ * hardware thread); then one device pass hashes every proof's openings
+ * (one launch for all leaves, one per tree level) and runs the DEEP and FRI
+ * checks. verdicts[i] belongs to jobs[i]; stats cover the whole call. */
+typedef struct {
+    p3g_pcs_params pcs;
+    const p3g_instance *instances;
+    uint64_t n_instances;
+    const uint64_t *fields;
+    uint64_t n_fields;
+    const uint64_t *commits;
+    uint64_t n_commits;
+    const uint64_t *digest12;
+} p3g_verify_job;
+int p3g_verify_batch(p3g_ctx *ctx, const p3g_verify_job *jobs, uint64_t n, uint32_t host_threads, int32_t *verdicts,
+                     p3g_verify_stats *stats);
 /* ------------------------------------------- batched and served proving */
 /* No counterpart in the reference: a job queue in front of p3g_prove
  * (prove_multi, p3-miden-lifted-stark/src/prover/mod.rs:223). n_workers

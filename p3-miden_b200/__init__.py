@@ -77,6 +77,12 @@ class VerifyStatsC(C.Structure):
     _fields_ = [("host_ms", C.c_double), ("device_ms", C.c_double), ("gpu_launches", C.c_uint64)]
 
 
+class VerifyJobC(C.Structure):
+    _fields_ = [("pcs", PcsParamsC), ("instances", C.POINTER(InstanceC)), ("n_instances", C.c_uint64),
+                ("fields", u64p), ("n_fields", C.c_uint64), ("commits", u64p), ("n_commits", C.c_uint64),
+                ("digest12", u64p)]
+
+
 def lib():
     """Load the CUDA library; raise if it has not been built."""
     global _lib
@@ -112,6 +118,8 @@ def lib():
             "p3g_air_num_constraints": (C.c_uint64, [C.c_int32, C.c_uint64]),
             "p3g_verify": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, u64p, C.c_uint64,
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
+            "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
+                                           C.POINTER(VerifyStatsC)]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -427,6 +435,33 @@ def verify_multi(ctx: Context, pcs: PcsParams, shapes: list[AirShape], fields: n
 
 def verify_output(ctx: Context, pcs: PcsParams, shapes: list[AirShape], out: StarkOutput) -> VerifyResult:
     return verify_multi(ctx, pcs, shapes, out.proof.fields, out.proof.commitments, out.digest)
+
+
+def verify_batch(ctx: Context, items, host_threads: int = 0) -> tuple[list[int], VerifyResult]:
+    """verify_multi of several proofs in one call: items are
+    (pcs, shapes, fields, commitments, digest); the host replays run on
+    host_threads threads (0: all), then one device pass checks every proof.
+    Returns the verdicts (0 = accepted) and the call's timing."""
+    n = len(items)
+    jobs = (VerifyJobC * max(1, n))()
+    keep = []
+    for i, (pcs, shapes, fields, commits, digest) in enumerate(items):
+        arr = (InstanceC * max(1, len(shapes)))()
+        for k, sh in enumerate(shapes):
+            c = np.ascontiguousarray(sh.consts if sh.consts is not None else np.zeros(0), dtype=np.uint64)
+            keep.append(c)
+            arr[k] = InstanceC(sh.air, 0, sh.height, sh.width, None, c.ctypes.data_as(u64p) if c.size else None,
+                               c.size)
+        f = np.ascontiguousarray(fields, dtype=np.uint64).reshape(-1)
+        cm = np.ascontiguousarray(commits, dtype=np.uint64).reshape(-1)
+        dg = np.ascontiguousarray(digest, dtype=np.uint64).reshape(-1)
+        keep += [arr, f, cm, dg]
+        jobs[i] = VerifyJobC(pcs.as_c(), arr, len(shapes), _ptr(f), f.size, _ptr(cm), cm.size // 4, _ptr(dg))
+    verdicts = (C.c_int32 * max(1, n))()
+    st = VerifyStatsC()
+    ctx.check(lib().p3g_verify_batch(ctx.handle, jobs, n, host_threads, verdicts, C.byref(st)))
+    return [int(verdicts[i]) for i in range(n)], VerifyResult(0, float(st.host_ms), float(st.device_ms),
+                                                             int(st.gpu_launches))
 
 
 # ------------------------------------------------------- trace builders

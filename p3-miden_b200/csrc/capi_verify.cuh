@@ -10,40 +10,119 @@ typedef struct {
     uint64_t gpu_launches;
 } p3g_verify_stats_c;
 
+namespace p3g {
+// Arguments of one verification: pointers, PCS parameters, AIR shapes, and
+// transcript words that are canonical field elements.
+inline bool words_canonical(const uint64_t *w, uint64_t n) {
+    uint64_t bad = 0;
+    for (uint64_t i = 0; i < n; i++) bad |= w[i] >= gl::P;
+    return !bad;
+}
+inline int verify_args_ok(const p3g_pcs_params_c *pcs, const p3g_instance_c *inst, uint64_t n, const uint64_t *fields,
+                          uint64_t n_fields, const uint64_t *commits, uint64_t n_commits, const uint64_t *digest12,
+                          bool scan_words = true) {
+    if (!pcs || !inst || !digest12 || n == 0 || n > 8) return ERR_INVALID;
+    if ((!fields && n_fields) || (!commits && n_commits)) return ERR_INVALID;
+    if (pcs->log_folding_arity < 1 || pcs->log_folding_arity > 3 || pcs->log_blowup == 0 || pcs->log_blowup > 8 ||
+        pcs->num_queries == 0 || pcs->folding_pow_bits > 30 || pcs->deep_pow_bits > 30 || pcs->query_pow_bits > 30)
+        return ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++) {
+        const p3g_instance_c &I = inst[i];
+        if (I.height > (1ull << 30)) return ERR_INVALID;
+        if (I.air == AIR_KECCAK) {
+            if (I.width != (uint64_t)keccak::NCOLS) return ERR_VALIDATION;
+        } else if (I.air == AIR_CUBIC) {
+            if (I.width == 0 || !I.consts || I.n_consts != I.width) return ERR_VALIDATION;
+        } else {
+            return ERR_VALIDATION;
+        }
+    }
+    if (scan_words && !(words_canonical(fields, n_fields) && words_canonical(commits, 4 * n_commits) &&
+                        words_canonical(digest12, 12)))
+        return ERR_INVALID;
+    return OK;
+}
+inline std::vector<Instance> shapes_of(const p3g_instance_c *inst, uint64_t n) {
+    std::vector<Instance> ins(n);
+    for (uint64_t i = 0; i < n; i++)
+        ins[i] = {inst[i].air, 0, inst[i].height, inst[i].width, nullptr, inst[i].consts, inst[i].n_consts};
+    return ins;
+}
+inline PcsParams pcs_of(const p3g_pcs_params_c *pcs) {
+    return PcsParams{pcs->log_blowup,    pcs->log_folding_arity, pcs->log_final_degree, pcs->folding_pow_bits,
+                     pcs->deep_pow_bits, pcs->num_queries,       pcs->query_pow_bits};
+}
+}  // namespace p3g
+
 P3G_API int p3g_verify(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instance_c *inst, uint64_t n,
                        const uint64_t *fields, uint64_t n_fields, const uint64_t *commits, uint64_t n_commits,
                        const uint64_t *digest12, int32_t *verdict, p3g_verify_stats_c *stats) {
-    if (!x || !pcs || !inst || !digest12 || !verdict || n == 0 || n > 8) return p3g::ERR_INVALID;
-    if ((!fields && n_fields) || (!commits && n_commits)) return p3g::ERR_INVALID;
-    if (pcs->log_folding_arity < 1 || pcs->log_folding_arity > 3 || pcs->log_blowup == 0 || pcs->log_blowup > 8 ||
-        pcs->num_queries == 0 || pcs->folding_pow_bits > 30 || pcs->deep_pow_bits > 30 || pcs->query_pow_bits > 30)
-        return p3g::ERR_INVALID;
-    for (uint64_t i = 0; i < n; i++) {
-        const p3g_instance_c &I = inst[i];
-        if (I.height > (1ull << 30)) return p3g::ERR_INVALID;
-        if (I.air == p3g::AIR_KECCAK) {
-            if (I.width != (uint64_t)p3g::keccak::NCOLS) return p3g::ERR_VALIDATION;
-        } else if (I.air == p3g::AIR_CUBIC) {
-            if (I.width == 0 || !I.consts || I.n_consts != I.width) return p3g::ERR_VALIDATION;
-        } else {
-            return p3g::ERR_VALIDATION;
-        }
-    }
-    // transcript words are field elements: canonical, below p
-    for (uint64_t i = 0; i < n_fields; i++)
-        if (fields[i] >= gl::P) return p3g::ERR_INVALID;
-    for (uint64_t i = 0; i < 4 * n_commits; i++)
-        if (commits[i] >= gl::P) return p3g::ERR_INVALID;
+    if (!x || !verdict) return p3g::ERR_INVALID;
+    if (int e = p3g::verify_args_ok(pcs, inst, n, fields, n_fields, commits, n_commits, digest12)) return e;
     P3G_TRY(x, {
         CK(cudaSetDevice(x->c.device));
-        p3g::ensure_keccak_tables(x->c.device);
-        std::vector<p3g::Instance> ins(n);
-        for (uint64_t i = 0; i < n; i++)
-            ins[i] = {inst[i].air, 0, inst[i].height, inst[i].width, nullptr, inst[i].consts, inst[i].n_consts};
-        p3g::PcsParams pp{pcs->log_blowup,    pcs->log_folding_arity, pcs->log_final_degree, pcs->folding_pow_bits,
-                          pcs->deep_pow_bits, pcs->num_queries,       pcs->query_pow_bits};
+        const std::vector<p3g::Instance> ins = p3g::shapes_of(inst, n);
         p3g::vfy::Timing tm;
-        *verdict = p3g::vfy::verify(x->c, pp, ins.data(), n, fields, n_fields, commits, n_commits, digest12, &tm);
+        *verdict = p3g::vfy::verify(x->c, p3g::pcs_of(pcs), ins.data(), n, fields, n_fields, commits, n_commits,
+                                    digest12, &tm);
+        if (stats) *stats = p3g_verify_stats_c{tm.host_ms, tm.device_ms, tm.launches};
+    })
+}
+
+typedef struct {
+    p3g_pcs_params_c pcs;
+    const p3g_instance_c *instances;
+    uint64_t n_instances;
+    const uint64_t *fields;
+    uint64_t n_fields;
+    const uint64_t *commits;
+    uint64_t n_commits;
+    const uint64_t *digest12;
+} p3g_verify_job_c;
+
+// Several proofs in one call: the host replays on up to host_threads threads
+// (0: one per hardware thread), then one device pass for all of them.
+P3G_API int p3g_verify_batch(p3g_ctx *x, const p3g_verify_job_c *jobs, uint64_t n, uint32_t host_threads,
+                             int32_t *verdicts, p3g_verify_stats_c *stats) {
+    if (!x || (n && (!jobs || !verdicts))) return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++) {
+        const p3g_verify_job_c &J = jobs[i];
+        if (int e = p3g::verify_args_ok(&J.pcs, J.instances, J.n_instances, J.fields, J.n_fields, J.commits,
+                                        J.n_commits, J.digest12, false))
+            return e;
+    }
+    const unsigned th = host_threads ? host_threads : std::max(1u, std::thread::hardware_concurrency());
+    {  // the canonical-word scan, one proof per task on the host threads
+        std::atomic<uint64_t> next{0};
+        std::atomic<bool> ok{true};
+        auto scan = [&]() {
+            for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+                const p3g_verify_job_c &J = jobs[i];
+                if (!(p3g::words_canonical(J.fields, J.n_fields) && p3g::words_canonical(J.commits, 4 * J.n_commits) &&
+                      p3g::words_canonical(J.digest12, 12)))
+                    ok = false;
+            }
+        };
+        std::vector<std::thread> ts;
+        for (unsigned t = 1; t < std::min<uint64_t>(th, n); t++) ts.emplace_back(scan);
+        scan();
+        for (auto &t : ts) t.join();
+        if (!ok) return p3g::ERR_INVALID;
+    }
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<std::vector<p3g::Instance>> ins(n);
+        std::vector<p3g::vfy::ProofRef> ps(n);
+        for (uint64_t i = 0; i < n; i++) {
+            const p3g_verify_job_c &J = jobs[i];
+            ins[i] = p3g::shapes_of(J.instances, J.n_instances);
+            ps[i] = p3g::vfy::ProofRef{p3g::pcs_of(&J.pcs), ins[i].data(), ins[i].size(), J.fields, J.n_fields,
+                                       J.commits, J.n_commits, J.digest12};
+        }
+        std::vector<int> v(n);
+        p3g::vfy::Timing tm;
+        if (n) p3g::vfy::verify_batch(x->c, ps, th, v.data(), &tm);
+        for (uint64_t i = 0; i < n; i++) verdicts[i] = v[i];
         if (stats) *stats = p3g_verify_stats_c{tm.host_ms, tm.device_ms, tm.launches};
     })
 }

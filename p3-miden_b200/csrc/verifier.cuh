@@ -33,8 +33,10 @@
 #pragma once
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "context.cuh"
@@ -97,6 +99,28 @@ __global__ void __launch_bounds__(128) leaf_kernel(const LeafJob *jobs, uint32_t
     }
     if (threadIdx.x % 32 < 4) pool[4 * (uint64_t)job.out + l] = p2w::canon(x);
 }
+
+// The same sponge with one thread per leaf, for large batches: with many
+// leaves in flight throughput decides, and the single-thread permutation
+// costs about a fifth of the cooperative one's issue slots.
+__global__ void __launch_bounds__(128) leaf_thread_kernel(const LeafJob *jobs, uint32_t n, const uint64_t *rows,
+                                                          const uint32_t *widths, uint64_t *pool) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const LeafJob job = jobs[j];
+    const uint64_t *row = rows + job.row_off;
+    uint64_t s[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = 0;
+    for (uint32_t m = 0; m < job.n_w; m++) {
+        const uint32_t w = widths[job.w_off + m];
+        merkle::absorb_row(s, row, w);
+        row += w;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) pool[4 * (uint64_t)job.out + i] = p2w::canon(s[i]);
+}
+constexpr uint32_t kThreadLeaves = 2048;  // from this many leaves on, one thread per leaf
 
 // One warp per compression of one tree level.
 __global__ void __launch_bounds__(128) compress_kernel(const CJob *jobs, uint32_t n, uint64_t *pool) {
@@ -261,6 +285,18 @@ struct Reader {
         }
         return f[pf++];
     }
+    // `n` hinted words read in place: returns their offset in the field
+    // stream. Offsets keep advancing past the end of a short stream (vpos),
+    // where the device reads zeros, as the reads of hint() would give.
+    uint64_t vpos = 0;
+    uint64_t skip(uint64_t n) {
+        if (vpos < pf) vpos = pf;  // in step with the stream until it runs out
+        const uint64_t off = vpos;
+        vpos += n;
+        if (vpos > nf) short_read = true;
+        pf = std::min(vpos, nf);
+        return off;
+    }
     uint64_t field() {
         if (pf >= nf) {
             short_read = true;
@@ -301,10 +337,12 @@ struct Batch {  // one LMCS open_batch
     uint64_t commit[4];
     uint32_t root = 0;     // node slot of the computed root
     bool bad_index = false, no_root = false;
-    uint64_t row_off = 0, tw = 0;
+    uint64_t row_off = 0, tw = 0;  // first opened row: its offset in the proof's field stream; row width
 };
+// Opened rows are read in place from the proof's field stream: query q's row
+// of a batch starts at row_off + q * tw (rows are hinted back to back).
 struct Plan {
-    std::vector<uint64_t> rows, hints;
+    std::vector<uint64_t> hints;
     std::vector<uint32_t> widths;
     std::vector<LeafJob> leaves;
     std::vector<std::vector<CJob>> levels;
@@ -320,7 +358,7 @@ struct Plan {
         memcpy(b.commit, commit, 32);
         const uint32_t w_off = (uint32_t)widths.size();
         for (uint32_t x : w) widths.push_back(x), b.tw += x;
-        b.row_off = rows.size();
+        b.row_off = std::max(r.vpos, r.pf);  // where the first skip() of the batch starts
         std::vector<uint64_t> pos;
         std::vector<uint32_t> id;
         for (uint64_t q : idx) {
@@ -329,8 +367,7 @@ struct Plan {
                 batches.push_back(b);
                 return;
             }
-            const uint64_t off = rows.size();
-            for (uint64_t c = 0; c < b.tw; c++) rows.push_back(r.hint());
+            const uint64_t off = r.skip(b.tw);
             leaves.push_back(LeafJob{off, w_off, (uint32_t)w.size(), n_nodes, 0});
             pos.push_back(q);
             id.push_back(n_nodes++);
@@ -404,203 +441,222 @@ inline gl::ef folded_constraints(const Instance &I, const gl::ef *L, const gl::e
     return folded;
 }
 
-// Returns the verdict. Throws CudaError on device failures.
-inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, const uint64_t *fields,
-                  uint64_t n_fields, const uint64_t *commits, uint64_t n_commits, const uint64_t digest[12],
-                  Timing *tm) {
-    const auto t0 = std::chrono::steady_clock::now();
-    if (n_inst == 0 || n_inst > 8) return V_SHAPE;
+// One proof after the host replay: the challenges, the opening layout and
+// the tables of the query checks; the device pass fills roots and flags.
+struct Prepared {
+    int early = -1;  // a verdict known before the device pass (shape), else -1
+    std::vector<Instance> inst;
+    const uint64_t *fields = nullptr;  // the proof's field stream (borrowed; opened rows are read from it)
+    uint64_t n_fields = 0;
+    uint64_t row_end = 0;  // end of the furthest opened row (past n_fields only for a short stream)
+    bool pow_ok = true, consumed = true, short_read = false, digest_ok = true;
+    bool quotient_ok = false, quotient_done = false;
+    uint64_t dg[12];
+    gl::ef alpha, beta, z, ac, bp, red_open[2], zs[2];
+    std::vector<gl::ef> evals;
+    std::vector<uint64_t> aw;
+    uint64_t total_aligned = 0, D = 1, rounds = 0, final_deg = 1, arity = 2, nq = 0;
+    uint32_t log_max_h = 0, log_qd = 0, log_lde = 0, log_a = 1;
+    std::vector<uint64_t> idx, final_poly, final_x, s_inv, apow, xq;
+    Plan P;
+    std::vector<FriRound> fr;
+    std::vector<uint32_t> ent_k, ent_pos;
+    // device results
+    std::vector<uint64_t> roots;
+    std::vector<int32_t> flags;
+};
+
+// The quotient identity at z: one extension-field evaluation.
+inline bool quotient_identity(const Prepared &v) {
+    const size_t n_inst = v.inst.size();
+    gl::ef accumulated = gl::ef_zero();
+    uint64_t off = 0;
+    for (size_t i = 0; i < n_inst; i++) {
+        const uint32_t log_h = log2u(v.inst[i].height), lift = v.log_max_h - log_h;
+        const gl::ef zl = gl::ef_exp2k(v.z, lift);
+        const gl::ef van = gl::ef_sub(gl::ef_exp2k(zl, log_h), gl::ef_one());
+        const uint64_t oinv = gl::inv(gl::root(log_h));
+        const gl::ef first = gl::ef_mul(van, gl::ef_inv(gl::ef_sub(zl, gl::ef_one())));
+        const gl::ef trans = gl::ef_sub(zl, gl::ef{oinv, 0});
+        const gl::ef folded =
+            folded_constraints(v.inst[i], &v.evals[off], &v.evals[v.total_aligned + off], first, trans, v.alpha);
+        accumulated = gl::ef_add(gl::ef_mul(accumulated, v.beta), folded);
+        off += v.aw[i];
+    }
+    uint64_t qoff = 0;
+    for (size_t m = 0; m < 2 * n_inst; m++) qoff += v.aw[m];
+    const gl::ef X{0, 1};
+    const gl::ef u = gl::ef_exp2k(gl::ef_mulf(v.z, gl::inv(gl::GEN)), v.log_max_h);
+    const uint64_t ws = gl::root(v.log_qd);
+    uint64_t wt = 1;
+    gl::ef num = gl::ef_zero(), den = gl::ef_zero();
+    for (uint64_t t = 0; t < v.D; t++) {
+        const gl::ef qt = gl::ef_add(v.evals[qoff + 2 * t], gl::ef_mul(X, v.evals[qoff + 2 * t + 1]));
+        const gl::ef wgt = gl::ef_mulf(gl::ef_inv(gl::ef_sub(u, gl::ef{wt, 0})), wt);
+        num = gl::ef_add(num, gl::ef_mul(wgt, qt));
+        den = gl::ef_add(den, wgt);
+        wt = gl::mul(wt, ws);
+    }
+    const gl::ef qz = gl::ef_mul(num, gl::ef_inv(den));
+    const gl::ef vanish = gl::ef_sub(gl::ef_exp2k(v.z, v.log_max_h), gl::ef_one());
+    return gl::ef_eq(accumulated, gl::ef_mul(qz, vanish));
+}
+
+// Host replay of one proof (no device work; safe to run on several threads
+// with distinct outputs). With `quotient` the quotient identity is checked
+// here too, else by the device pass while its kernels run.
+inline void prepare(const uint64_t *p2, const PcsParams &pcs, const Instance *inst, size_t n_inst,
+                    const uint64_t *fields, uint64_t n_fields, const uint64_t *commits, uint64_t n_commits,
+                    const uint64_t digest[12], bool quotient, Prepared &v) {
+    v.inst.assign(inst, inst + n_inst);
+    v.fields = fields, v.n_fields = n_fields;
+    if (n_inst == 0 || n_inst > 8) {
+        v.early = V_SHAPE;
+        return;
+    }
     for (size_t i = 0; i < n_inst; i++)
-        if (inst[i].height == 0 || (inst[i].height & (inst[i].height - 1)) || (i && inst[i].height < inst[i - 1].height))
-            return V_SHAPE;
+        if (inst[i].height == 0 || (inst[i].height & (inst[i].height - 1)) || (i && inst[i].height < inst[i - 1].height)) {
+            v.early = V_SHAPE;
+            return;
+        }
     Reader r{};
-    r.ch.p2 = ctx.p2;
+    r.ch.p2 = p2;
     r.f = fields, r.nf = n_fields, r.c = commits, r.nc = n_commits;
     const uint32_t lb = pcs.log_blowup;
-    const uint32_t log_max_h = log2u(inst[n_inst - 1].height);
-    uint32_t log_qd = 0;
-    for (size_t i = 0; i < n_inst; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
-    if (log_qd > lb) return V_SHAPE;
-    const uint64_t D = 1ull << log_qd;
-    const uint32_t log_lde = log_max_h + lb;
+    v.log_max_h = log2u(inst[n_inst - 1].height);
+    for (size_t i = 0; i < n_inst; i++) v.log_qd = std::max(v.log_qd, air_log_quotient_degree(inst[i].air));
+    if (v.log_qd > lb) {
+        v.early = V_SHAPE;
+        return;
+    }
+    v.D = 1ull << v.log_qd;
+    v.log_lde = v.log_max_h + lb;
+    const uint32_t log_lde = v.log_lde;
 
     // commitments and challenges in prover order
     uint64_t main_c[4], aux_c[4], quot_c[4];
     r.commit(main_c, true);
     (void)r.ch.sample_ef();  // aux randomness
     r.commit(aux_c, true);
-    const gl::ef alpha = r.ch.sample_ef();
-    const gl::ef beta = r.ch.sample_ef();
+    v.alpha = r.ch.sample_ef();
+    v.beta = r.ch.sample_ef();
     r.commit(quot_c, true);
     // out-of-domain point outside H and gK (coset.rs:329-342)
-    gl::ef z;
     for (;;) {
-        z = r.ch.sample_ef();
-        const bool in_h = gl::ef_eq(gl::ef_exp2k(z, log_max_h), gl::ef_one());
-        const bool in_gk = gl::ef_eq(gl::ef_exp2k(gl::ef_mulf(z, gl::inv(gl::GEN)), log_lde), gl::ef_one());
+        v.z = r.ch.sample_ef();
+        const bool in_h = gl::ef_eq(gl::ef_exp2k(v.z, v.log_max_h), gl::ef_one());
+        const bool in_gk = gl::ef_eq(gl::ef_exp2k(gl::ef_mulf(v.z, gl::inv(gl::GEN)), log_lde), gl::ef_one());
         if (!in_h && !in_gk) break;
     }
-    const gl::ef zs[2] = {z, gl::ef_mulf(z, gl::root(log_max_h))};
+    v.zs[0] = v.z;
+    v.zs[1] = gl::ef_mulf(v.z, gl::root(v.log_max_h));
 
     // matrices: main (one per instance), aux (2 columns each), quotient (2D)
-    std::vector<uint64_t> ow, aw;
+    std::vector<uint64_t> ow;
     for (size_t i = 0; i < n_inst; i++) ow.push_back(inst[i].width);
     for (size_t i = 0; i < n_inst; i++) ow.push_back(2);
-    ow.push_back(2 * D);
-    uint64_t total_aligned = 0;
-    for (uint64_t w : ow) aw.push_back((w + 7) / 8 * 8), total_aligned += aw.back();
+    ow.push_back(2 * v.D);
+    for (uint64_t w : ow) v.aw.push_back((w + 7) / 8 * 8), v.total_aligned += v.aw.back();
+    const uint64_t T = v.total_aligned;
 
     // DEEP oracle: aligned out-of-domain evaluations per point, grind, challenges
-    std::vector<gl::ef> evals(2 * total_aligned);
-    for (auto &e : evals) e = r.ef();
-    bool pow_ok = r.grind(pcs.deep_pow_bits);
-    const gl::ef ac = r.ch.sample_ef();
-    const gl::ef bp = r.ch.sample_ef();
-    gl::ef red_open[2];
+    v.evals.resize(2 * T);
+    for (auto &e : v.evals) e = r.ef();
+    v.pow_ok = r.grind(pcs.deep_pow_bits);
+    v.ac = r.ch.sample_ef();
+    v.bp = r.ch.sample_ef();
     for (int p = 0; p < 2; p++) {
         gl::ef acc = gl::ef_zero();
-        for (uint64_t c = 0; c < total_aligned; c++) acc = gl::ef_add(gl::ef_mul(acc, ac), evals[p * total_aligned + c]);
-        red_open[p] = acc;
+        for (uint64_t c = 0; c < T; c++) acc = gl::ef_add(gl::ef_mul(acc, v.ac), v.evals[p * T + c]);
+        v.red_open[p] = acc;
     }
     // FRI oracle: round commitments, grinds, betas, final polynomial
-    const uint32_t log_a = pcs.log_folding_arity;
-    const uint64_t arity = 1ull << log_a;
+    v.log_a = pcs.log_folding_arity;
+    v.arity = 1ull << v.log_a;
     const uint32_t log_max_final = pcs.log_final_degree + lb;
-    const uint64_t rounds = log_lde > log_max_final ? (log_lde - log_max_final + log_a - 1) / log_a : 0;
-    const uint32_t log_final_size = log_lde - (uint32_t)rounds * log_a;
-    const uint64_t final_deg = 1ull << (log_final_size > lb ? log_final_size - lb : 0);
-    std::vector<std::array<uint64_t, 4>> fri_c(rounds);
-    std::vector<gl::ef> fri_beta(rounds);
-    for (uint64_t rr = 0; rr < rounds; rr++) {
+    v.rounds = log_lde > log_max_final ? (log_lde - log_max_final + v.log_a - 1) / v.log_a : 0;
+    const uint32_t log_final_size = log_lde - (uint32_t)v.rounds * v.log_a;
+    v.final_deg = 1ull << (log_final_size > lb ? log_final_size - lb : 0);
+    std::vector<std::array<uint64_t, 4>> fri_c(v.rounds);
+    std::vector<gl::ef> fri_beta(v.rounds);
+    for (uint64_t rr = 0; rr < v.rounds; rr++) {
         r.commit(fri_c[rr].data(), true);
-        pow_ok = r.grind(pcs.folding_pow_bits) && pow_ok;
+        v.pow_ok = r.grind(pcs.folding_pow_bits) && v.pow_ok;
         fri_beta[rr] = r.ch.sample_ef();
     }
-    std::vector<uint64_t> final_poly(2 * final_deg);
-    for (uint64_t i = 0; i < final_deg; i++) {
+    v.final_poly.resize(2 * v.final_deg);
+    for (uint64_t i = 0; i < v.final_deg; i++) {
         const gl::ef e = r.ef();
-        final_poly[2 * i] = e.c0, final_poly[2 * i + 1] = e.c1;
+        v.final_poly[2 * i] = e.c0, v.final_poly[2 * i + 1] = e.c1;
     }
-    pow_ok = r.grind(pcs.query_pow_bits) && pow_ok;
-    std::vector<uint64_t> idx(pcs.num_queries);
-    for (auto &q : idx) q = gl::bitrev(r.ch.sample_bits(log_lde), log_lde);
-    idx = sort_unique(idx);
-    const uint64_t nq = idx.size();
+    v.pow_ok = r.grind(pcs.query_pow_bits) && v.pow_ok;
+    v.idx.resize(pcs.num_queries);
+    for (auto &q : v.idx) q = gl::bitrev(r.ch.sample_bits(log_lde), log_lde);
+    v.idx = sort_unique(v.idx);
+    v.nq = v.idx.size();
 
     // openings: the three trace trees, then the FRI rounds
-    Plan P;
     const uint64_t *gcommit[3] = {main_c, aux_c, quot_c};
     const size_t gfirst[4] = {0, n_inst, 2 * n_inst, 2 * n_inst + 1};
     for (int g = 0; g < 3; g++) {
         std::vector<uint32_t> w;
-        for (size_t m = gfirst[g]; m < gfirst[g + 1]; m++) w.push_back((uint32_t)aw[m]);
-        P.open_batch(r, gcommit[g], w, log_lde, idx);
+        for (size_t m = gfirst[g]; m < gfirst[g + 1]; m++) w.push_back((uint32_t)v.aw[m]);
+        v.P.open_batch(r, gcommit[g], w, log_lde, v.idx);
     }
-    std::vector<FriRound> fr;
-    std::vector<uint32_t> ent_k, ent_pos;
-    std::vector<uint64_t> s_inv;
-    std::vector<uint64_t> cur_idx = idx;
+    std::vector<uint64_t> cur_idx = v.idx;
     uint32_t log_dom = log_lde;
     uint64_t g_inv = gl::inv(gl::root(log_lde));
-    for (uint64_t rr = 0; rr < rounds; rr++) {
-        const uint32_t log_folded = log_dom - log_a;
+    for (uint64_t rr = 0; rr < v.rounds; rr++) {
+        const uint32_t log_folded = log_dom - v.log_a;
         std::vector<uint64_t> ridx;
-        for (uint64_t q : cur_idx) ridx.push_back(q >> log_a);
+        for (uint64_t q : cur_idx) ridx.push_back(q >> v.log_a);
         ridx = sort_unique(ridx);
         FriRound R{};
         R.ncur = (uint32_t)cur_idx.size();
         R.nr = (uint32_t)ridx.size();
-        R.ent_off = (uint32_t)ent_k.size();
-        R.row_off = (uint32_t)s_inv.size();
+        R.ent_off = (uint32_t)v.ent_k.size();
+        R.row_off = (uint32_t)v.s_inv.size();
         R.beta = fri_beta[rr];
-        R.row_base = P.rows.size();
-        P.open_batch(r, fri_c[rr].data(), {(uint32_t)(2 * arity)}, log_folded, ridx);
+        R.row_base = std::max(r.vpos, r.pf);
+        v.P.open_batch(r, fri_c[rr].data(), {(uint32_t)(2 * v.arity)}, log_folded, ridx);
         for (uint64_t q : cur_idx) {
-            ent_k.push_back((uint32_t)(std::lower_bound(ridx.begin(), ridx.end(), q >> log_a) - ridx.begin()));
-            ent_pos.push_back((uint32_t)(q & (arity - 1)));
+            v.ent_k.push_back((uint32_t)(std::lower_bound(ridx.begin(), ridx.end(), q >> v.log_a) - ridx.begin()));
+            v.ent_pos.push_back((uint32_t)(q & (v.arity - 1)));
         }
-        for (uint64_t k : ridx) s_inv.push_back(gl::pow(g_inv, gl::bitrev(k, log_folded)));
-        fr.push_back(R);
+        for (uint64_t k : ridx) v.s_inv.push_back(gl::pow(g_inv, gl::bitrev(k, log_folded)));
+        v.fr.push_back(R);
         cur_idx = ridx;
         log_dom = log_folded;
-        g_inv = gl::exp2k(g_inv, log_a);
+        g_inv = gl::exp2k(g_inv, v.log_a);
     }
-    std::vector<uint64_t> final_x;
     {
         const uint64_t gen = gl::root(log_dom);
-        for (uint64_t q : cur_idx) final_x.push_back(gl::pow(gen, gl::bitrev(q, log_dom)));
+        for (uint64_t q : cur_idx) v.final_x.push_back(gl::pow(gen, gl::bitrev(q, log_dom)));
     }
-    const bool consumed = r.pf == r.nf && r.pc == r.nc;
-    const bool short_read = r.short_read;
-    uint64_t dg[12];
+    v.consumed = r.pf == r.nf && r.pc == r.nc;
+    v.row_end = std::max(r.vpos, r.pf);
+    v.short_read = r.short_read;
     {
         Challenger c = r.ch;
         c.duplex();
-        memcpy(dg, c.state, sizeof(dg));
+        memcpy(v.dg, c.state, sizeof(v.dg));
+        v.digest_ok = memcmp(v.dg, digest, 96) == 0;
     }
+    // tables of the DEEP check
+    v.apow.resize(2 * T);
+    gl::ef pw = gl::ef_one();
+    for (uint64_t i = T; i-- > 0;) v.apow[2 * i] = pw.c0, v.apow[2 * i + 1] = pw.c1, pw = gl::ef_mul(pw, v.ac);
+    v.xq.resize(v.nq);
+    const uint64_t gen = gl::root(log_lde);
+    for (uint64_t q = 0; q < v.nq; q++) v.xq[q] = gl::mul(gl::GEN, gl::pow(gen, gl::bitrev(v.idx[q], log_lde)));
+    if (quotient) v.quotient_ok = quotient_identity(v), v.quotient_done = true;
+}
 
-    // quotient identity at z: one extension-field evaluation on the host,
-    // run while the device kernels are in flight
-    auto quotient_identity = [&]() -> bool {
-        gl::ef accumulated = gl::ef_zero();
-        uint64_t off = 0;
-        for (size_t i = 0; i < n_inst; i++) {
-            const uint32_t log_h = log2u(inst[i].height), lift = log_max_h - log_h;
-            const gl::ef zl = gl::ef_exp2k(z, lift);
-            const gl::ef van = gl::ef_sub(gl::ef_exp2k(zl, log_h), gl::ef_one());
-            const uint64_t oinv = gl::inv(gl::root(log_h));
-            const gl::ef first = gl::ef_mul(van, gl::ef_inv(gl::ef_sub(zl, gl::ef_one())));
-            const gl::ef trans = gl::ef_sub(zl, gl::ef{oinv, 0});
-            const gl::ef folded =
-                folded_constraints(inst[i], &evals[off], &evals[total_aligned + off], first, trans, alpha);
-            accumulated = gl::ef_add(gl::ef_mul(accumulated, beta), folded);
-            off += aw[i];
-        }
-        uint64_t qoff = 0;
-        for (size_t m = 0; m < 2 * n_inst; m++) qoff += aw[m];
-        const gl::ef X{0, 1};
-        const gl::ef u = gl::ef_exp2k(gl::ef_mulf(z, gl::inv(gl::GEN)), log_max_h);
-        const uint64_t ws = gl::root(log_qd);
-        uint64_t wt = 1;
-        gl::ef num = gl::ef_zero(), den = gl::ef_zero();
-        for (uint64_t t = 0; t < D; t++) {
-            const gl::ef qt = gl::ef_add(evals[qoff + 2 * t], gl::ef_mul(X, evals[qoff + 2 * t + 1]));
-            const gl::ef wgt = gl::ef_mulf(gl::ef_inv(gl::ef_sub(u, gl::ef{wt, 0})), wt);
-            num = gl::ef_add(num, gl::ef_mul(wgt, qt));
-            den = gl::ef_add(den, wgt);
-            wt = gl::mul(wt, ws);
-        }
-        const gl::ef qz = gl::ef_mul(num, gl::ef_inv(den));
-        const gl::ef vanish = gl::ef_sub(gl::ef_exp2k(z, log_max_h), gl::ef_one());
-        return gl::ef_eq(accumulated, gl::ef_mul(qz, vanish));
-    };
-
-    // device: one upload of every input, then the leaf sponges, the tree
-    // levels, the DEEP values, the FRI rounds and one read-back of the roots
-    // and flags
-    const uint32_t n_nodes = P.n_nodes;
-    auto slot = [&](uint32_t s) { return (s & kHint) ? n_nodes + (s & ~kHint) : s; };
-    std::vector<CJob> cj;
-    std::vector<size_t> lv_off{0};
-    for (auto &lv : P.levels) {
-        for (const CJob &jb : lv) cj.push_back(CJob{slot(jb.left), slot(jb.right), jb.out});
-        lv_off.push_back(cj.size());
-    }
-    bool trace_ok = true, fri_shape_ok = true;
-    for (int g = 0; g < 3; g++) trace_ok = trace_ok && !P.batches[g].bad_index;
-    for (uint64_t rr = 0; rr < rounds; rr++) fri_shape_ok = fri_shape_ok && !P.batches[3 + rr].bad_index;
-    const bool run_deep = trace_ok && nq, run_fri = run_deep && fri_shape_ok;
-    std::vector<uint64_t> apow, xq;
-    if (run_deep) {
-        apow.resize(2 * total_aligned);
-        gl::ef pw = gl::ef_one();
-        for (uint64_t i = total_aligned; i-- > 0;) apow[2 * i] = pw.c0, apow[2 * i + 1] = pw.c1, pw = gl::ef_mul(pw, ac);
-        xq.resize(nq);
-        const uint64_t gen = gl::root(log_lde);
-        for (uint64_t q = 0; q < nq; q++) xq[q] = gl::mul(gl::GEN, gl::pow(gen, gl::bitrev(idx[q], log_lde)));
-    }
-    std::vector<uint32_t> root_slot;
-    for (const Batch &B : P.batches) root_slot.push_back(B.bad_index || B.no_root ? 0 : B.root);
+// The device pass over several prepared proofs: one staged upload, the leaf
+// sponges of every proof in one launch, every tree level of every proof in
+// one launch per level, then per proof the DEEP and FRI kernels, and one
+// read-back of all roots and flags. Proofs decided early are skipped.
+inline void device_pass(Ctx &ctx, const std::vector<Prepared *> &vs, Timing *tm, unsigned threads = 1) {
     struct Seg {
         const void *src;
         size_t bytes, off;
@@ -612,44 +668,115 @@ inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         words += (bytes + 7) / 8 + 1;  // one spare word keeps every segment non-empty
         return segs.back().off;
     };
-    const size_t o_rows = seg(P.rows.data(), P.rows.size() * 8);
-    const size_t o_widths = seg(P.widths.data(), P.widths.size() * 4);
-    const size_t o_leaves = seg(P.leaves.data(), P.leaves.size() * sizeof(LeafJob));
+    std::vector<Prepared *> act;
+    for (Prepared *v : vs)
+        if (v->early < 0) act.push_back(v);
+    const size_t nj = act.size();
+    // per proof: offsets into the shared rows / widths / nodes / hints
+    std::vector<uint64_t> row_base(nj), node_base(nj), hint_base(nj), flag_base(nj), root_base(nj);
+    uint64_t n_rows = 0, n_nodes = 0, n_hints = 0, n_flags = 0, n_roots = 0;
+    uint32_t n_widths = 0;
+    for (size_t j = 0; j < nj; j++) {
+        const Plan &P = act[j]->P;
+        row_base[j] = n_rows, node_base[j] = n_nodes, hint_base[j] = n_hints / 4;
+        flag_base[j] = n_flags, root_base[j] = n_roots;
+        n_rows += std::max(act[j]->row_end, act[j]->n_fields) + 1;  // the field stream, then zeros
+        n_nodes += P.n_nodes, n_hints += P.hints.size(), n_widths += P.widths.size();
+        n_flags += 2 + act[j]->rounds;
+        n_roots += P.batches.size();
+    }
+    std::vector<uint32_t> widths, root_slot;
+    std::vector<uint64_t> hints;
+    std::vector<LeafJob> leaves;
+    std::vector<std::vector<CJob>> levels;
+    widths.reserve(n_widths), hints.reserve(n_hints);
+    for (size_t j = 0; j < nj; j++) {
+        const Plan &P = act[j]->P;
+        const uint32_t w0 = (uint32_t)widths.size();
+        widths.insert(widths.end(), P.widths.begin(), P.widths.end());
+        hints.insert(hints.end(), P.hints.begin(), P.hints.end());
+        auto slot = [&](uint32_t s) {
+            return (s & kHint) ? (uint32_t)(n_nodes + hint_base[j] + (s & ~kHint)) : (uint32_t)(node_base[j] + s);
+        };
+        for (const LeafJob &L : P.leaves)
+            leaves.push_back(LeafJob{row_base[j] + L.row_off, w0 + L.w_off, L.n_w, (uint32_t)(node_base[j] + L.out), 0});
+        if (levels.size() < P.levels.size()) levels.resize(P.levels.size());
+        for (size_t l = 0; l < P.levels.size(); l++)
+            for (const CJob &c : P.levels[l]) levels[l].push_back(CJob{slot(c.left), slot(c.right), slot(c.out)});
+        for (const Batch &B : P.batches) root_slot.push_back(B.bad_index || B.no_root ? 0 : slot(B.root));
+    }
+    std::vector<CJob> cj;
+    std::vector<size_t> lv_off{0};
+    for (auto &lv : levels) {
+        cj.insert(cj.end(), lv.begin(), lv.end());
+        lv_off.push_back(cj.size());
+    }
+    const size_t o_rows = seg(nullptr, n_rows * 8);  // filled from each proof's field stream below
+    const size_t o_widths = seg(widths.data(), widths.size() * 4);
+    const size_t o_leaves = seg(leaves.data(), leaves.size() * sizeof(LeafJob));
     const size_t o_cj = seg(cj.data(), cj.size() * sizeof(CJob));
-    const size_t o_apow = seg(apow.data(), apow.size() * 8);
-    const size_t o_xq = seg(xq.data(), xq.size() * 8);
-    const size_t o_rounds = seg(fr.data(), fr.size() * sizeof(FriRound));
-    const size_t o_ek = seg(ent_k.data(), ent_k.size() * 4);
-    const size_t o_ep = seg(ent_pos.data(), ent_pos.size() * 4);
-    const size_t o_sinv = seg(s_inv.data(), s_inv.size() * 8);
-    const size_t o_fx = seg(final_x.data(), final_x.size() * 8);
-    const size_t o_fp = seg(final_poly.data(), final_poly.size() * 8);
     const size_t o_rs = seg(root_slot.data(), root_slot.size() * 4);
+    std::vector<size_t> o_apow(nj), o_xq(nj), o_rounds(nj), o_ek(nj), o_ep(nj), o_sinv(nj), o_fx(nj), o_fp(nj);
+    std::vector<std::vector<FriRound>> frs(nj);  // rounds with row offsets into the shared rows
+    for (size_t j = 0; j < nj; j++) {
+        const Prepared &v = *act[j];
+        o_apow[j] = seg(v.apow.data(), v.apow.size() * 8);
+        o_xq[j] = seg(v.xq.data(), v.xq.size() * 8);
+        frs[j] = v.fr;
+        for (FriRound &R : frs[j]) R.row_base += row_base[j];
+        o_rounds[j] = seg(frs[j].data(), frs[j].size() * sizeof(FriRound));
+        o_ek[j] = seg(v.ent_k.data(), v.ent_k.size() * 4);
+        o_ep[j] = seg(v.ent_pos.data(), v.ent_pos.size() * 4);
+        o_sinv[j] = seg(v.s_inv.data(), v.s_inv.size() * 8);
+        o_fx[j] = seg(v.final_x.data(), v.final_x.size() * 8);
+        o_fp[j] = seg(v.final_poly.data(), v.final_poly.size() * 8);
+    }
     const size_t staged = words;
-    const size_t o_hints = seg(P.hints.data(), P.hints.size() * 8);  // copied into the pool
-    const size_t pool_words = 4 * (uint64_t)n_nodes + P.hints.size() + 4;
-    const uint64_t n_flags = 2 + rounds;
-    const size_t back_words = 4 * P.batches.size() + (n_flags + 1) / 2;  // roots, then flags
+    const size_t o_hints = seg(hints.data(), hints.size() * 8);  // copied into the pool
+    const size_t pool_words = 4 * n_nodes + hints.size() + 4;
+    uint64_t max_nq = 0;
+    for (Prepared *v : act) max_nq = std::max(max_nq, v->nq);
+    const size_t q_words = 2 * max_nq + 2;
+    const size_t back_words = 4 * n_roots + (n_flags + 1) / 2;  // roots, then flags
     const uint64_t launches0 = ctx.launches;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    const auto t1 = std::chrono::steady_clock::now();
-    DBuf d = ctx.alloc(staged + pool_words + 3 * (2 * nq + 2) + back_words);
-    uint64_t *pool = d.p + staged, *de = pool + pool_words, *cur = de + 2 * nq + 2, *nxt = cur + 2 * nq + 2;
-    uint64_t *back = nxt + 2 * nq + 2;
+    DBuf d = ctx.alloc(staged + pool_words + 3 * q_words * std::max<size_t>(nj, 1) + back_words);
+    uint64_t *pool = d.p + staged, *qbuf = pool + pool_words, *back = qbuf + 3 * q_words * std::max<size_t>(nj, 1);
     uint64_t *st = ctx.stage(std::max(words, back_words));
     for (const Seg &sg : segs)
-        if (sg.bytes) memcpy(st + sg.off, sg.src, sg.bytes);
+        if (sg.bytes && sg.src) memcpy(st + sg.off, sg.src, sg.bytes);
+    {  // each proof's field stream into its region, on up to `threads` host threads
+        std::atomic<size_t> next{0};
+        auto copy = [&]() {
+            for (size_t j; (j = next.fetch_add(1)) < nj;) {
+                uint64_t *dst = st + o_rows + row_base[j];
+                const uint64_t nf = act[j]->n_fields;
+                if (nf) memcpy(dst, act[j]->fields, nf * 8);
+                memset(dst + nf, 0, (std::max(act[j]->row_end, nf) + 1 - nf) * 8);
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < std::min<size_t>(threads, nj); t++) th.emplace_back(copy);
+        copy();
+        for (auto &t : th) t.join();
+    }
     CK(cudaEventRecord(e0, ctx.stream));
     ctx.h2d(d.p, st, staged);
-    ctx.h2d(pool + 4 * (uint64_t)n_nodes, st + o_hints, P.hints.size());
+    ctx.h2d(pool + 4 * n_nodes, st + o_hints, hints.size());
     CK(cudaMemsetAsync(back, 0, back_words * 8, ctx.stream));
-    int32_t *d_flags = (int32_t *)(back + 4 * P.batches.size());
-    if (!P.leaves.empty()) {
-        const uint32_t n = (uint32_t)P.leaves.size();
-        leaf_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)(d.p + o_leaves), n, d.p + o_rows,
-                                                                  (const uint32_t *)(d.p + o_widths), pool);
+    int32_t *d_flags = (int32_t *)(back + 4 * n_roots);
+    if (!leaves.empty()) {
+        const uint32_t n = (uint32_t)leaves.size();
+        if (n >= kThreadLeaves)
+            leaf_thread_kernel<<<(n + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)(d.p + o_leaves), n,
+                                                                        d.p + o_rows, (const uint32_t *)(d.p + o_widths),
+                                                                        pool);
+        else
+            leaf_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)(d.p + o_leaves), n,
+                                                                      d.p + o_rows, (const uint32_t *)(d.p + o_widths),
+                                                                      pool);
         CK(cudaGetLastError());
         ctx.launches++;
     }
@@ -661,88 +788,149 @@ inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         CK(cudaGetLastError());
         ctx.launches++;
     }
-    if (run_deep) {
+    for (size_t j = 0; j < nj; j++) {
+        const Prepared &v = *act[j];
+        const Plan &P = v.P;
+        bool trace_ok = true, fri_shape_ok = true;
+        for (int g = 0; g < 3; g++) trace_ok = trace_ok && !P.batches[g].bad_index;
+        for (uint64_t rr = 0; rr < v.rounds; rr++) fri_shape_ok = fri_shape_ok && !P.batches[3 + rr].bad_index;
+        if (!trace_ok || !v.nq) continue;
+        uint64_t *de = qbuf + 3 * q_words * j, *cur = de + q_words, *nxt = cur + q_words;
+        int32_t *fl = d_flags + flag_base[j];
         DeepArgs da{};
         da.rows = d.p + o_rows;
-        for (int g = 0; g < 3; g++) da.goff[g] = P.batches[g].row_off, da.gtw[g] = P.batches[g].tw;
-        da.apow = d.p + o_apow;
-        da.xq = d.p + o_xq;
-        da.nq = (uint32_t)nq;
-        da.red_open[0] = red_open[0], da.red_open[1] = red_open[1];
-        da.zs[0] = zs[0], da.zs[1] = zs[1];
-        da.bp = bp;
+        for (int g = 0; g < 3; g++) da.goff[g] = row_base[j] + P.batches[g].row_off, da.gtw[g] = P.batches[g].tw;
+        da.apow = d.p + o_apow[j];
+        da.xq = d.p + o_xq[j];
+        da.nq = (uint32_t)v.nq;
+        da.red_open[0] = v.red_open[0], da.red_open[1] = v.red_open[1];
+        da.zs[0] = v.zs[0], da.zs[1] = v.zs[1];
+        da.bp = v.bp;
         da.de = de;
-        da.flags = d_flags;
-        deep_kernel<<<(unsigned)((nq * 32 + 127) / 128), 128, 0, ctx.stream>>>(da);
+        da.flags = fl;
+        deep_kernel<<<(unsigned)((v.nq * 32 + 127) / 128), 128, 0, ctx.stream>>>(da);
         CK(cudaGetLastError());
         ctx.launches++;
-    }
-    if (run_fri) {
+        if (!fri_shape_ok) continue;
         FriArgs fa{};
         fa.rows = d.p + o_rows;
-        fa.rounds = (const FriRound *)(d.p + o_rounds);
-        fa.n_rounds = (uint32_t)rounds;
-        fa.log_a = log_a;
-        fa.ent_k = (const uint32_t *)(d.p + o_ek);
-        fa.ent_pos = (const uint32_t *)(d.p + o_ep);
-        fa.s_inv = d.p + o_sinv;
-        const uint64_t wi = gl::inv(gl::root(log_a));
+        fa.rounds = (const FriRound *)(d.p + o_rounds[j]);
+        fa.n_rounds = (uint32_t)v.rounds;
+        fa.log_a = v.log_a;
+        fa.ent_k = (const uint32_t *)(d.p + o_ek[j]);
+        fa.ent_pos = (const uint32_t *)(d.p + o_ep[j]);
+        fa.s_inv = d.p + o_sinv[j];
+        const uint64_t wi = gl::inv(gl::root(v.log_a));
         uint64_t x = 1;
         for (uint64_t t = 0; t < 8; t++) fa.winv_a[t] = x, x = gl::mul(x, wi);
-        fa.inv_a = gl::inv(arity);
+        fa.inv_a = gl::inv(v.arity);
         fa.de = de;
         fa.cur = cur, fa.nxt = nxt;
-        fa.n_final = (uint32_t)final_x.size();
-        fa.final_x = d.p + o_fx;
-        fa.final_poly = d.p + o_fp;
-        fa.final_deg = (uint32_t)final_deg;
-        fa.flags = d_flags;
+        fa.n_final = (uint32_t)v.final_x.size();
+        fa.final_x = d.p + o_fx[j];
+        fa.final_poly = d.p + o_fp[j];
+        fa.final_deg = (uint32_t)v.final_deg;
+        fa.flags = fl;
         fri_kernel<<<1, 256, 0, ctx.stream>>>(fa);
         CK(cudaGetLastError());
         ctx.launches++;
     }
-    gather_roots_kernel<<<1, 128, 0, ctx.stream>>>(pool, (const uint32_t *)(d.p + o_rs),
-                                                   (uint32_t)P.batches.size(), back);
-    CK(cudaGetLastError());
-    ctx.launches++;
+    if (n_roots) {
+        gather_roots_kernel<<<1, 128, 0, ctx.stream>>>(pool, (const uint32_t *)(d.p + o_rs), (uint32_t)n_roots, back);
+        CK(cudaGetLastError());
+        ctx.launches++;
+    }
     ctx.d2h(st, back, back_words);
     CK(cudaEventRecord(e1, ctx.stream));
-    const bool quotient_ok = quotient_identity();
+    for (Prepared *v : act)
+        if (!v->quotient_done) v->quotient_ok = quotient_identity(*v), v->quotient_done = true;
     ctx.sync();
-    std::vector<uint64_t> roots(st, st + 4 * P.batches.size());
-    std::vector<int32_t> flags(n_flags);
-    memcpy(flags.data(), st + 4 * P.batches.size(), n_flags * 4);
-    const bool deep_bad = flags[0] != 0, final_bad = flags[1] != 0;
+    for (size_t j = 0; j < nj; j++) {
+        Prepared &v = *act[j];
+        v.roots.assign(st + 4 * root_base[j], st + 4 * (root_base[j] + v.P.batches.size()));
+        v.flags.resize(2 + v.rounds);
+        memcpy(v.flags.data(), (const int32_t *)(st + 4 * n_roots) + flag_base[j], v.flags.size() * 4);
+    }
     float dev_ms = 0;
     CK(cudaEventElapsedTime(&dev_ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (tm) {
-        tm->device_ms = dev_ms;
-        tm->host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        tm->launches = ctx.launches - launches0;
-    }
+    if (tm) tm->device_ms = dev_ms, tm->launches = ctx.launches - launches0;
+}
+
+// The first failing check, in verify_multi's order.
+inline int verdict(const Prepared &v) {
+    if (v.early >= 0) return v.early;
+    const Plan &P = v.P;
     auto batch_err = [&](size_t b) -> int {
         const Batch &B = P.batches[b];
         if (B.bad_index) return V_OPENING;
-        if (B.no_root || memcmp(roots.data() + 4 * b, B.commit, 32) != 0) return V_ROOT;
+        if (B.no_root || memcmp(v.roots.data() + 4 * b, B.commit, 32) != 0) return V_ROOT;
         return ACCEPT;
     };
-
-    // the first failing check, in verify_multi's order
-    if (!pow_ok) return V_POW;
+    if (!v.pow_ok) return V_POW;
     for (size_t g = 0; g < 3; g++)
         if (int e = batch_err(g)) return e;
-    if (deep_bad) return V_DEEP;
-    for (uint64_t rr = 0; rr < rounds; rr++) {
+    if (v.flags[0]) return V_DEEP;
+    for (uint64_t rr = 0; rr < v.rounds; rr++) {
         if (int e = batch_err(3 + rr)) return e;
-        if (flags[2 + rr]) return V_FRI;
+        if (v.flags[2 + rr]) return V_FRI;
     }
-    if (final_bad) return V_FINAL;
-    if (!quotient_ok) return V_QUOTIENT;
-    if (short_read || !consumed) return V_TRANSCRIPT;
-    if (memcmp(dg, digest, 96) != 0) return V_DIGEST;
+    if (v.flags[1]) return V_FINAL;
+    if (!v.quotient_ok) return V_QUOTIENT;
+    if (v.short_read || !v.consumed) return V_TRANSCRIPT;
+    if (!v.digest_ok) return V_DIGEST;
     return ACCEPT;
+}
+
+// One proof. Throws CudaError on device failures.
+inline int verify(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, const uint64_t *fields,
+                  uint64_t n_fields, const uint64_t *commits, uint64_t n_commits, const uint64_t digest[12],
+                  Timing *tm) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Prepared v;
+    prepare(ctx.p2, pcs, inst, n_inst, fields, n_fields, commits, n_commits, digest, false, v);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (tm) tm->host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (v.early >= 0) return v.early;
+    device_pass(ctx, {&v}, tm);
+    return verdict(v);
+}
+
+struct ProofRef {  // one proof of a batch
+    PcsParams pcs;
+    const Instance *inst;
+    size_t n_inst;
+    const uint64_t *fields;
+    uint64_t n_fields;
+    const uint64_t *commits;
+    uint64_t n_commits;
+    const uint64_t *digest;
+};
+// Several proofs: the host replays run on up to `threads` host threads
+// (each with its quotient identity), then one device pass serves them all.
+inline void verify_batch(Ctx &ctx, const std::vector<ProofRef> &ps, unsigned threads, int *verdicts, Timing *tm) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<Prepared> vs(ps.size());
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < ps.size();) {
+            const ProofRef &p = ps[i];
+            prepare(ctx.p2, p.pcs, p.inst, p.n_inst, p.fields, p.n_fields, p.commits, p.n_commits, p.digest, true,
+                    vs[i]);
+        }
+    };
+    threads = std::max(1u, std::min<unsigned>(threads, (unsigned)ps.size()));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < threads; t++) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (tm) tm->host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    std::vector<Prepared *> ptrs;
+    for (auto &v : vs) ptrs.push_back(&v);
+    device_pass(ctx, ptrs, tm, threads);
+    for (size_t i = 0; i < vs.size(); i++) verdicts[i] = verdict(vs[i]);
 }
 
 }  // namespace vfy

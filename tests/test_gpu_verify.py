@@ -121,3 +121,31 @@ def test_noncanonical_word_is_an_error(product, gpu_ctx, case):
     with pytest.raises(Exception):
         product.verify_multi(gpu_ctx, pcs, [product.AirShape(a, h, w, k) for a, h, w, k in oinst], f,
                              out.proof.commitments, out.digest)
+
+
+def test_batch_matches_single(product, gpu_ctx):
+    """p3g_verify_batch: one device pass for proofs of different shapes,
+    valid and perturbed, gives each proof its single-call verdict."""
+    items, want = [], []
+    for i, make in enumerate(CASES.values()):
+        pcs, inst, oinst = make(product)
+        out = product.prove_multi(gpu_ctx, pcs, inst)
+        shapes = [product.AirShape(a, h, w, k) for a, h, w, k in oinst]
+        f, c, d = out.proof.fields, out.proof.commitments, out.digest
+        variants = [(f, c, d)]
+        bad = f.copy()
+        k = (len(bad) * (i + 1)) // 5
+        bad[k] = (int(bad[k]) + 1) % P
+        variants.append((bad, c, d))
+        d2 = d.copy()
+        d2[0] = (int(d2[0]) + 1) % P
+        variants.append((f, c, d2))
+        variants.append((f[:-3], c, d))
+        for ff, cc, dd in variants:
+            items.append((pcs, shapes, ff, cc, dd))
+            want.append(product.verify_multi(gpu_ctx, pcs, shapes, ff, cc, dd).verdict)
+    for threads in (1, 0):
+        got, stats = product.verify_batch(gpu_ctx, items, threads)
+        assert got == want
+        assert stats.gpu_launches > 0
+    assert want.count(0) == len(CASES)
