@@ -96,6 +96,17 @@ void p3g_poseidon2_params_from_seed(uint64_t seed, const uint64_t *diag12, uint6
 int p3g_prove(p3g_ctx *ctx, const p3g_pcs_params *pcs, const p3g_instance *instances, uint64_t n,
               p3g_proof *out);
 void p3g_proof_free(p3g_proof *proof);
+/* Wire format of a proof (digest + TranscriptData, p3-miden-transcript/src/
+ * data.rs:11-49), little-endian: "P3GPROOF", u32 version 1, u32 0,
+ * u64 n_fields, u64 n_commits, the 12 digest words (128-byte header), then the
+ * field words, then the commitment words (the payload TranscriptData::
+ * size_in_bytes counts). p3g_proof_serialize sets *len to the size and fails
+ * with P3G_ERR_INVALID when cap is smaller; p3g_proof_deserialize checks the
+ * header, the length and that every word is canonical, and fills malloc'ed
+ * buffers (release with p3g_proof_free; timing fields are zero). */
+uint64_t p3g_proof_wire_size(const p3g_proof *proof);
+int p3g_proof_serialize(const p3g_proof *proof, uint8_t *buf, uint64_t cap, uint64_t *len);
+int p3g_proof_deserialize(const uint8_t *buf, uint64_t len, p3g_proof *out);
 
 /* ------------------------------------------------------- stage seams */
 /* TwoAdicSubgroupDft::coset_lde_batch(trace, log_blowup, shift) followed by

@@ -111,6 +111,9 @@ def lib():
             "p3g_grind": (C.c_int, [vp, u64p, u64p, C.c_uint32, C.c_uint32, u64p]),
             "p3g_prove": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, C.POINTER(ProofC)]),
             "p3g_proof_free": (None, [C.POINTER(ProofC)]),
+            "p3g_proof_wire_size": (C.c_uint64, [C.POINTER(ProofC)]),
+            "p3g_proof_serialize": (C.c_int, [C.POINTER(ProofC), C.c_char_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+            "p3g_proof_deserialize": (C.c_int, [C.c_char_p, C.c_uint64, C.POINTER(ProofC)]),
             "p3g_keccak_trace": (C.c_int, [u64p, C.c_uint64, C.c_uint32, u64p]),
             "p3g_keccak_trace_device": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
             "p3g_keccak_inputs": (C.c_int, [C.c_uint64, C.c_uint64, u64p]),
@@ -313,6 +316,35 @@ class TranscriptData:
     def to_bytes(self) -> bytes:
         """Raw payload: field words then commitment words, little-endian u64."""
         return self.fields.astype("<u8").tobytes() + self.commitments.astype("<u8").tobytes()
+
+
+def proof_to_wire(digest: np.ndarray, proof: TranscriptData) -> bytes:
+    """p3g_proof_serialize: the library's wire format of a proof."""
+    f = np.ascontiguousarray(proof.fields, dtype=np.uint64)
+    c = np.ascontiguousarray(proof.commitments, dtype=np.uint64).reshape(-1)
+    p = ProofC()
+    p.fields, p.n_fields = f.ctypes.data_as(u64p), f.size
+    p.commits, p.n_commits = c.ctypes.data_as(u64p), c.size // 4
+    for i in range(12):
+        p.digest[i] = int(digest[i])
+    n = int(lib().p3g_proof_wire_size(C.byref(p)))
+    buf = C.create_string_buffer(n)
+    ln = C.c_uint64()
+    _check(lib().p3g_proof_serialize(C.byref(p), buf, n, C.byref(ln)))
+    return buf.raw[: ln.value]
+
+
+def proof_from_wire(data: bytes) -> tuple[np.ndarray, TranscriptData]:
+    """p3g_proof_deserialize: (digest, TranscriptData); raises on a malformed buffer."""
+    p = ProofC()
+    _check(lib().p3g_proof_deserialize(data, len(data), C.byref(p)))
+    try:
+        fields = np.ctypeslib.as_array(p.fields, shape=(p.n_fields,)).copy() if p.n_fields else np.zeros(0, np.uint64)
+        commits = (np.ctypeslib.as_array(p.commits, shape=(p.n_commits * 4,)).reshape(-1, 4).copy()
+                   if p.n_commits else np.zeros((0, 4), np.uint64))
+        return np.array(p.digest[:], dtype=np.uint64), TranscriptData(fields, commits)
+    finally:
+        lib().p3g_proof_free(C.byref(p))
 
 
 @dataclass

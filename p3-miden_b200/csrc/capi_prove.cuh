@@ -129,6 +129,68 @@ P3G_API int p3g_prove(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instanc
     return p3g::OK;
 }
 
+// Wire format of a proof (StarkOutput: digest + TranscriptData,
+// p3-miden-lifted-stark/src/proof.rs:39-44, p3-miden-transcript/src/data.rs:11-14),
+// little-endian: "P3GPROOF", u32 version 1, u32 0, u64 n_fields, u64 n_commits,
+// 12 digest words (a 128-byte header), then the field words, then the
+// commitment words. The payload is TranscriptData's size_in_bytes
+// (data.rs:46-48): 8 bytes per field element, 32 per commitment.
+namespace p3g {
+constexpr uint64_t kWireHeader = 128;
+constexpr char kWireMagic[8] = {'P', '3', 'G', 'P', 'R', 'O', 'O', 'F'};
+}  // namespace p3g
+P3G_API uint64_t p3g_proof_wire_size(const p3g_proof_c *p) {
+    return p ? p3g::kWireHeader + 8 * p->n_fields + 32 * p->n_commits : 0;
+}
+P3G_API int p3g_proof_serialize(const p3g_proof_c *p, uint8_t *buf, uint64_t cap, uint64_t *len) {
+    if (!p || !len || (p->n_fields && !p->fields) || (p->n_commits && !p->commits)) return p3g::ERR_INVALID;
+    const uint64_t n = p3g_proof_wire_size(p);
+    *len = n;
+    if (!buf || cap < n) return p3g::ERR_INVALID;
+    const uint32_t ver[2] = {1, 0};
+    const uint64_t counts[2] = {p->n_fields, p->n_commits};
+    memcpy(buf, p3g::kWireMagic, 8);
+    memcpy(buf + 8, ver, 8);
+    memcpy(buf + 16, counts, 16);
+    memcpy(buf + 32, p->digest, 96);
+    if (p->n_fields) memcpy(buf + p3g::kWireHeader, p->fields, 8 * p->n_fields);
+    if (p->n_commits) memcpy(buf + p3g::kWireHeader + 8 * p->n_fields, p->commits, 32 * p->n_commits);
+    return p3g::OK;
+}
+// Parses a serialized proof into malloc'ed buffers (release with
+// p3g_proof_free). P3G_ERR_INVALID for a wrong magic or version, a length
+// that does not match the counts, or a word that is not a canonical field
+// element.
+P3G_API int p3g_proof_deserialize(const uint8_t *buf, uint64_t len, p3g_proof_c *out) {
+    if (!buf || !out || len < p3g::kWireHeader) return p3g::ERR_INVALID;
+    memset(out, 0, sizeof(*out));
+    uint32_t ver[2];
+    uint64_t counts[2];
+    memcpy(ver, buf + 8, 8);
+    memcpy(counts, buf + 16, 16);
+    if (memcmp(buf, p3g::kWireMagic, 8) != 0 || ver[0] != 1 || ver[1] != 0) return p3g::ERR_INVALID;
+    if (counts[0] > (len / 8) || counts[1] > (len / 32)) return p3g::ERR_INVALID;
+    if (p3g::kWireHeader + 8 * counts[0] + 32 * counts[1] != len) return p3g::ERR_INVALID;
+    const uint8_t *body = buf + p3g::kWireHeader;
+    for (uint64_t i = 0; i < 12 + counts[0] + 4 * counts[1]; i++) {
+        uint64_t w;
+        memcpy(&w, i < 12 ? buf + 32 + 8 * i : body + 8 * (i - 12), 8);
+        if (w >= gl::P) return p3g::ERR_INVALID;
+    }
+    out->fields = (uint64_t *)malloc(std::max<uint64_t>(1, counts[0]) * 8);
+    out->commits = (uint64_t *)malloc(std::max<uint64_t>(1, counts[1]) * 32);
+    if (!out->fields || !out->commits) {
+        free(out->fields), free(out->commits);
+        out->fields = out->commits = nullptr;
+        return p3g::ERR_OOM;
+    }
+    out->n_fields = counts[0], out->n_commits = counts[1];
+    memcpy(out->digest, buf + 32, 96);
+    if (counts[0]) memcpy(out->fields, body, 8 * counts[0]);
+    if (counts[1]) memcpy(out->commits, body + 8 * counts[0], 32 * counts[1]);
+    return p3g::OK;
+}
+
 P3G_API void p3g_proof_free(p3g_proof_c *p) {
     if (!p) return;
     free(p->fields);

@@ -68,3 +68,32 @@ def test_invalid_arguments_are_rejected_without_a_device(product):
     assert lib.p3g_keccak_trace(inp.ctypes.data_as(product.u64p), 2, 5, out.ctypes.data_as(product.u64p)) \
         == product.ERR_INVALID
     assert lib.p3g_coset_lde(None, None, 4, 1, 1, 7, None) == product.ERR_INVALID
+
+
+def test_proof_wire_format_roundtrip(product):
+    """p3g_proof_serialize / p3g_proof_deserialize: a 128-byte header, then
+    8 bytes per field element and 32 per commitment (TranscriptData's
+    size_in_bytes); malformed buffers are rejected."""
+    rng = np.random.default_rng(5)
+    P = O.P
+    for n_f, n_c in [(0, 0), (1, 0), (0, 3), (1000, 37)]:
+        digest = rng.integers(0, P, size=12, dtype=np.uint64)
+        proof = product.TranscriptData(rng.integers(0, P, size=n_f, dtype=np.uint64),
+                                       rng.integers(0, P, size=(n_c, 4), dtype=np.uint64))
+        wire = product.proof_to_wire(digest, proof)
+        assert len(wire) == 128 + 8 * n_f + 32 * n_c
+        assert wire[:8] == b"P3GPROOF"
+        assert wire[128:] == proof.to_bytes()
+        d2, p2 = product.proof_from_wire(wire)
+        assert np.array_equal(d2, digest)
+        assert np.array_equal(p2.fields, proof.fields) and np.array_equal(p2.commitments, proof.commitments)
+    bad = [b"", wire[:127], b"X" + wire[1:], wire[:-1], wire + b"\0" * 8]
+    nc = bytearray(wire)
+    nc[128:136] = (P).to_bytes(8, "little")  # a field word equal to p
+    bad.append(bytes(nc))
+    for b in bad:
+        try:
+            product.proof_from_wire(b)
+        except product.P3gError:
+            continue
+        raise AssertionError(f"accepted a malformed buffer of {len(b)} bytes")

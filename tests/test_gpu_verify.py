@@ -149,3 +149,11 @@ def test_batch_matches_single(product, gpu_ctx):
         assert got == want
         assert stats.gpu_launches > 0
     assert want.count(0) == len(CASES)
+
+
+def test_wire_roundtrip_verifies(product, gpu_ctx, case):
+    """A proof sent through the wire format verifies like the original."""
+    name, pcs, oinst, out = case
+    digest, proof = product.proof_from_wire(product.proof_to_wire(out.digest, out.proof))
+    shapes = [product.AirShape(a, h, w, k) for a, h, w, k in oinst]
+    assert product.verify_multi(gpu_ctx, pcs, shapes, proof.fields, proof.commitments, digest).ok, name
