@@ -129,6 +129,17 @@ int p3g_lmcs_build(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *
 int p3g_lmcs_build_hiding(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights,
                           const uint64_t *widths, uint64_t n, uint32_t alignment, const uint64_t *d_salt,
                           uint64_t salt_width, p3g_tree **out);
+/* Lmcs::open_batch (p3-miden-lmcs/src/lmcs.rs:167-290), hashed on the
+ * device: checks the hints of p3g_lmcs_prove_batch (fields: each index's
+ * rows padded to the alignment, then salt_width salt words for a hiding
+ * tree; commits: the streamed siblings) against commit4 for strictly
+ * ascending indices. *verdict: P3G_ACCEPT, P3G_VERR_OPENING (an index outside
+ * the tree), P3G_VERR_ROOT or P3G_VERR_TRANSCRIPT (hints too short or left
+ * over). */
+int p3g_lmcs_open_batch(p3g_ctx *ctx, const uint64_t *commit4, const uint64_t *widths, uint64_t n_mats,
+                        uint32_t alignment, uint64_t salt_width, uint32_t log_height, const uint64_t *indices,
+                        uint64_t n_idx, const uint64_t *fields, uint64_t n_fields, const uint64_t *commits,
+                        uint64_t n_commits, int32_t *verdict);
 /* LmcsTree::root (lib.rs:264) */
 int p3g_lmcs_root(const p3g_tree *tree, uint64_t *out4);
 /* digest layer `level` (0 = leaves) copied to host: (height >> level) x 4 words */

@@ -101,6 +101,8 @@ def lib():
             "p3g_lmcs_build": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32, C.POINTER(vp)]),
             "p3g_lmcs_build_hiding": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32,
                                                 C.c_void_p, C.c_uint64, C.POINTER(vp)]),
+            "p3g_lmcs_open_batch": (C.c_int, [vp, u64p, u64p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, u64p,
+                                              C.c_uint64, u64p, C.c_uint64, u64p, C.c_uint64, C.POINTER(C.c_int32)]),
             "p3g_lmcs_root": (C.c_int, [vp, u64p]),
             "p3g_lmcs_layer": (C.c_int, [vp, vp, C.c_uint32, u64p]),
             "p3g_lmcs_free": (None, [vp]),
@@ -233,6 +235,8 @@ class LmcsTree:
         ws = np.array([m.shape[1] for m in mats_dev], dtype=np.uint64)
         self._h = C.c_void_p()
         self.salt_width = 0
+        self.alignment = alignment
+        self.widths = [int(w) for w in ws]
         if salt_dev is None:
             ctx.check(lib().p3g_lmcs_build(ctx.handle, ptrs, _ptr(hs), _ptr(ws), n, alignment, C.byref(self._h)))
         else:
@@ -266,6 +270,22 @@ class LmcsTree:
         self.ctx.check(lib().p3g_lmcs_prove_batch(self.ctx.handle, self._h, _ptr(idx), len(idx),
                                                   _ptr(fields), _ptr(nf), _ptr(commits.reshape(-1)), _ptr(nc)))
         return fields[: int(nf[0])], commits[: int(nc[0])]
+
+    def open_batch(self, indices, fields, commits, commitment=None) -> int:
+        """Lmcs::open_batch of hints from prove_batch against this tree's root
+        (or `commitment`), hashed on the device; returns the verdict
+        (0 = accepted, else VERDICTS: opening, root or transcript)."""
+        idx = np.array(sorted(set(int(i) for i in indices)), dtype=np.uint64)
+        root = np.ascontiguousarray(self.root() if commitment is None else commitment, dtype=np.uint64)
+        w = np.array(self.widths, dtype=np.uint64)
+        f = np.ascontiguousarray(fields, dtype=np.uint64).reshape(-1)
+        c = np.ascontiguousarray(commits, dtype=np.uint64).reshape(-1)
+        v = C.c_int32(-1)
+        self.ctx.check(lib().p3g_lmcs_open_batch(self.ctx.handle, _ptr(root), _ptr(w), w.size, self.alignment,
+                                                 self.salt_width, self.depth, _ptr(idx) if idx.size else None,
+                                                 idx.size, _ptr(f) if f.size else None, f.size,
+                                                 _ptr(c) if c.size else None, c.size // 4, C.byref(v)))
+        return int(v.value)
 
     def __del__(self):
         try:

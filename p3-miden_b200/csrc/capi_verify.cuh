@@ -126,3 +126,33 @@ P3G_API int p3g_verify_batch(p3g_ctx *x, const p3g_verify_job_c *jobs, uint64_t 
         if (stats) *stats = p3g_verify_stats_c{tm.host_ms, tm.device_ms, tm.launches};
     })
 }
+
+// Lmcs::open_batch (p3-miden-lmcs/src/lmcs.rs:167-290) for a tree of height
+// 2^log_height over matrices of the given widths, opened at strictly
+// ascending indices: fields are the hinted rows (each matrix's row padded to
+// the alignment, then salt_width salt words for a hiding tree), commits the
+// streamed sibling digests. *verdict: P3G_ACCEPT, P3G_VERR_OPENING,
+// P3G_VERR_ROOT or P3G_VERR_TRANSCRIPT.
+P3G_API int p3g_lmcs_open_batch(p3g_ctx *x, const uint64_t *commit4, const uint64_t *widths, uint64_t n_mats,
+                                uint32_t alignment, uint64_t salt_width, uint32_t log_height, const uint64_t *indices,
+                                uint64_t n_idx, const uint64_t *fields, uint64_t n_fields, const uint64_t *commits,
+                                uint64_t n_commits, int32_t *verdict) {
+    if (!x || !commit4 || !verdict || (n_mats && !widths) || (n_idx && !indices) || (!fields && n_fields) ||
+        (!commits && n_commits) || log_height > 40 || n_mats > 64 || salt_width > 4096)
+        return p3g::ERR_INVALID;
+    for (uint64_t i = 1; i < n_idx; i++)
+        if (indices[i] <= indices[i - 1]) return p3g::ERR_INVALID;
+    const uint64_t a = alignment ? alignment : 1;
+    std::vector<uint32_t> w;
+    for (uint64_t m = 0; m < n_mats; m++) {
+        if (widths[m] > (1u << 24)) return p3g::ERR_INVALID;
+        w.push_back((uint32_t)((widths[m] + a - 1) / a * a));
+    }
+    if (salt_width) w.push_back((uint32_t)salt_width);
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        *verdict = p3g::vfy::lmcs_open_batch(x->c, commit4, w, log_height,
+                                             std::vector<uint64_t>(indices, indices + n_idx), fields, n_fields,
+                                             commits, n_commits);
+    })
+}

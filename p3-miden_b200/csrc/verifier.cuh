@@ -858,6 +858,71 @@ inline void device_pass(Ctx &ctx, const std::vector<Prepared *> &vs, Timing *tm,
     if (tm) tm->device_ms = dev_ms, tm->launches = ctx.launches - launches0;
 }
 
+// Lmcs::open_batch (p3-miden-lmcs/src/lmcs.rs:167-290) on the device: the
+// hinted rows of each sorted unique index (absorbed widths, the salt last for
+// a hiding tree), then the streamed siblings, hashed to a root and compared
+// with the commitment. Returns ACCEPT, V_OPENING (an index outside the tree),
+// V_ROOT, or V_TRANSCRIPT (hints too short or not all used).
+inline int lmcs_open_batch(Ctx &ctx, const uint64_t commit[4], const std::vector<uint32_t> &widths, uint32_t log_h,
+                           const std::vector<uint64_t> &idx, const uint64_t *fields, uint64_t n_fields,
+                           const uint64_t *commits, uint64_t n_commits) {
+    Reader r{};
+    r.ch.p2 = ctx.p2;
+    r.f = fields, r.nf = n_fields, r.c = commits, r.nc = n_commits;
+    Plan P;
+    P.open_batch(r, commit, widths, log_h, idx);
+    const Batch &B = P.batches[0];
+    if (B.bad_index) return V_OPENING;
+    const uint64_t row_end = std::max(r.vpos, r.pf);
+    const uint32_t n_nodes = P.n_nodes;
+    auto slot = [&](uint32_t s) { return (s & kHint) ? n_nodes + (s & ~kHint) : s; };
+    std::vector<CJob> cj;
+    std::vector<size_t> lv_off{0};
+    for (auto &lv : P.levels) {
+        for (const CJob &c : lv) cj.push_back(CJob{slot(c.left), slot(c.right), c.out});
+        lv_off.push_back(cj.size());
+    }
+    const uint64_t rows_w = std::max(row_end, n_fields) + 1;
+    const uint64_t o_widths = rows_w, o_leaves = o_widths + (P.widths.size() + 1) / 2 + 1;
+    const uint64_t o_cj = o_leaves + P.leaves.size() * sizeof(LeafJob) / 8 + 1;
+    const uint64_t o_pool = o_cj + (cj.size() * sizeof(CJob) + 7) / 8 + 1;
+    const uint64_t total = o_pool + 4 * (uint64_t)n_nodes + P.hints.size() + 4;
+    DBuf d = ctx.alloc(total);
+    uint64_t *st = ctx.stage(total);
+    memset(st, 0, o_pool * 8);
+    if (n_fields) memcpy(st, fields, n_fields * 8);
+    memcpy(st + o_widths, P.widths.data(), P.widths.size() * 4);
+    memcpy(st + o_leaves, P.leaves.data(), P.leaves.size() * sizeof(LeafJob));
+    memcpy(st + o_cj, cj.data(), cj.size() * sizeof(CJob));
+    memcpy(st + o_pool + 4 * (uint64_t)n_nodes, P.hints.data(), P.hints.size() * 8);
+    ctx.h2d(d.p, st, total);
+    uint64_t *pool = d.p + o_pool;
+    if (!P.leaves.empty()) {
+        const uint32_t n = (uint32_t)P.leaves.size();
+        leaf_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const LeafJob *)(d.p + o_leaves), n, d.p,
+                                                                  (const uint32_t *)(d.p + o_widths), pool);
+        CK(cudaGetLastError());
+        ctx.launches++;
+    }
+    for (size_t l = 0; l + 1 < lv_off.size(); l++) {
+        const uint32_t n = (uint32_t)(lv_off[l + 1] - lv_off[l]);
+        if (!n) continue;
+        compress_kernel<<<(n * 32 + 127) / 128, 128, 0, ctx.stream>>>((const CJob *)(d.p + o_cj) + lv_off[l], n,
+                                                                      pool);
+        CK(cudaGetLastError());
+        ctx.launches++;
+    }
+    uint64_t root[4] = {0, 0, 0, 0};
+    if (!B.no_root) {
+        ctx.d2h(st, pool + 4 * (uint64_t)B.root, 4);
+        ctx.sync();
+        memcpy(root, st, 32);
+    }
+    if (B.no_root || memcmp(root, commit, 32) != 0) return V_ROOT;
+    if (r.short_read || r.pf != r.nf || r.pc != r.nc) return V_TRANSCRIPT;
+    return ACCEPT;
+}
+
 // The first failing check, in verify_multi's order.
 inline int verdict(const Prepared &v) {
     if (v.early >= 0) return v.early;

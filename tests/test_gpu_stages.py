@@ -104,3 +104,35 @@ def test_lmcs_prove_batch_and_hiding_match_oracle(product, gpu_ctx, scenario, al
     fg, cg = gt.prove_batch(idx)
     fo, co = ot.prove_batch(idx)
     assert np.array_equal(fg, fo) and np.array_equal(cg, co)
+
+
+@pytest.mark.parametrize("salt_w", [0, 4])
+@pytest.mark.parametrize("alignment", [1, 8])
+def test_lmcs_open_batch_roundtrip(product, gpu_ctx, salt_w, alignment):
+    """Lmcs::open_batch on the device (p3g_lmcs_open_batch) accepts the hints
+    of prove_batch, for plain and hiding trees (the hiding round trip of
+    p3-miden-lmcs/src/tests.rs:203-221), and rejects changed rows, salts,
+    siblings and commitments and truncated or extended hints."""
+    rng = np.random.default_rng(7 + salt_w + alignment)
+    mats = [rand_mat(rng, h, w) for h, w in [(4, 3), (8, 5), (16, 9)]]
+    salt = rand_mat(rng, 16, salt_w) if salt_w else None
+    gt = product.LmcsTree(gpu_ctx, [product.to_device(m) for m in mats], alignment,
+                          product.to_device(salt) if salt_w else None)
+    for idx in ([1, 3, 5], [0, 15], list(range(16)), [7]):
+        f, c = gt.prove_batch(idx)
+        assert gt.open_batch(idx, f, c) == 0
+        f2 = f.copy()
+        f2[-1] = (int(f2[-1]) + 1) % O.P  # the last index's salt, or its last row word
+        assert product.VERDICTS[gt.open_batch(idx, f2, c)] == "root"
+        if len(c):
+            c2 = c.copy()
+            c2[0, 0] = (int(c2[0, 0]) + 1) % O.P
+            assert product.VERDICTS[gt.open_batch(idx, f, c2)] == "root"
+        assert product.VERDICTS[gt.open_batch(idx, f, c, commitment=gt.root() ^ np.uint64(1))] == "root"
+        assert gt.open_batch(idx, f[:-1], c) != 0
+        assert product.VERDICTS[gt.open_batch(idx, np.append(f, np.uint64(0)), c)] == "transcript"
+    # different salts, different commitments (tests.rs:223-238)
+    if salt_w:
+        other = product.LmcsTree(gpu_ctx, [product.to_device(m) for m in mats], alignment,
+                                 product.to_device(rand_mat(rng, 16, salt_w)))
+        assert not np.array_equal(other.root(), gt.root())
