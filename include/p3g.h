@@ -115,6 +115,13 @@ int p3g_proof_deserialize(const uint8_t *buf, uint64_t len, p3g_proof *out);
 int p3g_coset_lde(p3g_ctx *ctx, const uint64_t *d_in, uint64_t height, uint64_t width, uint32_t log_blowup,
                   uint64_t shift, uint64_t *d_out);
 
+/* PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
+ * d_repeated holds the periodic columns repeated to the largest period
+ * (max_period x width); d_out receives their LDE on the coset of shift
+ * lde_shift^(2^log_trace_height / max_period), (max_period << log_blowup) x
+ * width in natural order, read at row i mod that height (periodic.rs:88-98). */
+int p3g_periodic_lde(p3g_ctx *ctx, const uint64_t *d_repeated, uint64_t max_period, uint64_t width,
+                     uint32_t log_blowup, uint32_t log_trace_height, uint64_t lde_shift, uint64_t *d_out);
 /* Lmcs::build_tree / build_aligned_tree (p3-miden-lmcs/src/lib.rs:191-197,
  * lmcs.rs:412-440) over device matrices sorted by ascending height;
  * alignment 1 = build_tree, 8 = build_aligned_tree (the sponge rate). */

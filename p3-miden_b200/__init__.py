@@ -104,6 +104,8 @@ def lib():
             "p3g_lmcs_open_batch": (C.c_int, [vp, u64p, u64p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, u64p,
                                               C.c_uint64, u64p, C.c_uint64, u64p, C.c_uint64, C.POINTER(C.c_int32)]),
             "p3g_lmcs_root": (C.c_int, [vp, u64p]),
+            "p3g_periodic_lde": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
+                                           C.c_uint64, C.c_void_p]),
             "p3g_lmcs_layer": (C.c_int, [vp, vp, C.c_uint32, u64p]),
             "p3g_lmcs_free": (None, [vp]),
             "p3g_poseidon2_permute_batch": (C.c_int, [vp, C.c_void_p, C.c_uint64]),
@@ -215,6 +217,20 @@ def coset_lde(ctx: Context, trace_dev, log_blowup: int, shift: int):
     torch.cuda.synchronize(ctx.device)
     out = empty_device((h << log_blowup, w), ctx.device)
     ctx.check(lib().p3g_coset_lde(ctx.handle, trace_dev.data_ptr(), h, w, log_blowup, shift, out.data_ptr()))
+    return out
+
+
+def periodic_lde(ctx: Context, repeated_dev, log_blowup: int, log_trace_height: int, lde_shift: int = 7):
+    """PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
+    periodic columns repeated to the largest period (a device matrix), extended
+    on the period's coset in natural order; row i of the trace's LDE is row
+    i mod the result's height."""
+    import torch
+    torch.cuda.synchronize(ctx.device)
+    p, w = repeated_dev.shape
+    out = empty_device((p << log_blowup, w), ctx.device)
+    ctx.check(lib().p3g_periodic_lde(ctx.handle, repeated_dev.data_ptr(), p, w, log_blowup, log_trace_height,
+                                     lde_shift, out.data_ptr()))
     return out
 
 

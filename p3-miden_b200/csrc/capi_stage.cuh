@@ -69,6 +69,41 @@ P3G_API int p3g_coset_lde(p3g_ctx *x, const uint64_t *d_in, uint64_t height, uin
     })
 }
 
+namespace p3g {
+// out[r] = in[bitrev(r)] for the rows of an n x w matrix (n = 2^L)
+__global__ void bitrev_rows_kernel(const uint64_t *in, uint64_t *out, uint32_t L, uint64_t w) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >> L >= w) return;
+    const uint64_t r = i / w, c = i % w;
+    out[r * w + c] = in[gl::bitrev(r, L) * w + c];
+}
+}  // namespace p3g
+
+// PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
+// the periodic columns repeated to the largest period (max_period x width,
+// row-major, on the device) extended on the coset of shift
+// lde_shift^(trace_height / max_period), natural order. d_out holds
+// (max_period << log_blowup) x width; the constraint evaluation reads row
+// i mod that height (periodic.rs:88-98).
+P3G_API int p3g_periodic_lde(p3g_ctx *x, const uint64_t *d_repeated, uint64_t max_period, uint64_t width,
+                             uint32_t log_blowup, uint32_t log_trace_height, uint64_t lde_shift, uint64_t *d_out) {
+    if (!x || !d_repeated || !d_out || max_period == 0 || (max_period & (max_period - 1)) || log_blowup > 8 ||
+        log_trace_height > 32 || max_period > (1ull << log_trace_height) || width == 0)
+        return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        const uint32_t log_p = p3g::log2u(max_period), L = log_p + log_blowup;
+        const uint64_t shift = gl::exp2k(lde_shift % gl::P, log_trace_height - log_p);
+        p3g::DBuf tmp = x->c.alloc(max_period * width), brev = x->c.alloc((max_period << log_blowup) * width);
+        p3g::coset_lde(x->c, d_repeated, width, max_period, width, log_blowup, shift, brev.p, tmp.p);
+        const uint64_t n = (max_period << log_blowup) * width;
+        p3g::bitrev_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, x->c.stream>>>(brev.p, d_out, L, width);
+        CK(cudaGetLastError());
+        x->c.launches++;
+        x->c.sync();
+    })
+}
+
 P3G_API int p3g_lmcs_build(p3g_ctx *x, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
                            uint64_t n, uint32_t alignment, p3g_tree **out) {
     if (!x || !d_mats || !heights || !widths || !out || n == 0 || n > 64) return p3g::ERR_INVALID;

@@ -136,3 +136,29 @@ def test_lmcs_open_batch_roundtrip(product, gpu_ctx, salt_w, alignment):
         other = product.LmcsTree(gpu_ctx, [product.to_device(m) for m in mats], alignment,
                                  product.to_device(rand_mat(rng, 16, salt_w)))
         assert not np.array_equal(other.root(), gt.root())
+
+
+def _bitrev(i, bits):
+    return int(format(i, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+@pytest.mark.parametrize("log_h,log_blowup,periods", [(6, 1, [1, 2, 4, 8]), (6, 3, [4, 2]), (3, 2, [8, 1]),
+                                                      (5, 2, [1])])
+def test_periodic_lde_matches_full_lde(product, gpu_ctx, log_h, log_blowup, periods):
+    """PeriodicLde (p3-miden-lifted-stark/src/prover/periodic.rs; its own test
+    assert_periodic_lde_matches_full): row i of the full coset LDE of the
+    columns repeated to the trace height equals row i mod the periodic LDE's
+    height, in natural order."""
+    rng = np.random.default_rng(log_h * 10 + log_blowup)
+    cols = [rng.integers(0, O.P, size=p, dtype=np.uint64) for p in periods]
+    max_p = max(periods)
+    repeated = np.array([[c[r % len(c)] for c in cols] for r in range(max_p)], dtype=np.uint64)
+    h = 1 << log_h
+    full = np.array([[c[i % len(c)] for c in cols] for i in range(h)], dtype=np.uint64)
+    per = product.to_host(product.periodic_lde(gpu_ctx, product.to_device(repeated), log_blowup, log_h, 7))
+    assert per.shape == (max_p << log_blowup, len(periods))
+    brev = product.to_host(product.coset_lde(gpu_ctx, product.to_device(full), log_blowup, 7))
+    L = log_h + log_blowup
+    nat = brev[[_bitrev(i, L) for i in range(h << log_blowup)]]
+    for i in range(h << log_blowup):
+        assert np.array_equal(nat[i], per[i % per.shape[0]]), i
