@@ -90,6 +90,28 @@ __device__ __forceinline__ uint64_t sbox(uint64_t x) {
     uint64_t x2 = mul(x, x), x4 = mul(x2, x2), x3 = mul(x2, x);
     return mul(x4, x3);
 }
+// a*b + c for a, b < 2^64 and a 96-bit c below 2^68: c enters the product's
+// carry chain whole (its top word on the third limb, where the product chain
+// starts from zero), so a sum shared by several products is never reduced on
+// its own. a*b + c <= (2^64-1)^2 + 2^68 < 2^128; weakly reduced.
+__device__ __forceinline__ uint64_t mul_add_w(uint64_t a, uint64_t b, W c) {
+    uint32_t r0, r1, r2, r3;
+    asm("mad.lo.cc.u32 %0, %4, %6, %8;\n\t"
+        "madc.hi.cc.u32 %1, %4, %6, %9;\n\t"
+        "addc.u32 %2, %10, 0;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32 %2, %4, %7, %2;\n\t"
+        "addc.u32 %3, 0, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "addc.u32 %3, %3, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, %3;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)),
+          "r"((uint32_t)c.lo), "r"((uint32_t)(c.lo >> 32)), "r"(c.hi));
+    return gl::reduce4_dev(r0, r1, r2, r3);
+}
 // circ(2*M4, M4, M4), M4 = circ(2,3,1,1): 96-bit accumulation, one reduction per
 // output. With rc_off >= 0 the next round's constants c_p2[rc_off + i] join the
 // 96-bit sums before the reduction (the same value mod p as adding them after it,
@@ -141,10 +163,9 @@ __device__ __forceinline__ void p2_permute_dev(uint64_t *s) {
             s[0] = p2w::sbox(p2w::add_c(s[0], c_p2[p2::OFF_INT + r - 4]));
             p2w::W acc = p2w::wide(s[0]);
 #pragma unroll
-            for (int i = 1; i < 12; i++) acc = p2w::wadd1(acc, s[i]);
-            const uint64_t sum = p2w::wreduce(acc);
+            for (int i = 1; i < 12; i++) acc = p2w::wadd1(acc, s[i]);  // below 12 * 2^64
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl::mul_add_weak(s[i], c_p2[p2::OFF_DIAG + i], sum);
+            for (int i = 0; i < 12; i++) s[i] = p2w::mul_add_w(s[i], c_p2[p2::OFF_DIAG + i], acc);
         }
     }
 }
