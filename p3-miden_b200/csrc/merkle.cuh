@@ -238,10 +238,8 @@ __device__ __forceinline__ uint64_t permute(uint64_t x, int l, const uint64_t *s
         W P = wide(rest ? x : 0);
 #pragma unroll
         for (int m = 1; m < 16; m <<= 1) P = wadd(P, shflW_xor(P, m));
-        const uint64_t R = wreduce(P);
-        const uint64_t sum = wreduce(wadd1(P, zs));
-        z = gl::mul_add_weak(zs, k.mu0p1, R);
-        x = rest ? gl::mul_add_weak(x, k.mu, sum) : 0;
+        z = mul_add_w(zs, k.mu0p1, P);                       // P < 11 * 2^64
+        x = rest ? mul_add_w(x, k.mu, wadd1(P, zs)) : 0;     // sum < 12 * 2^64
     }
     if (l == 0) x = z;
     return ext_rounds(x, l, sc + p2::OFF_TERM);
