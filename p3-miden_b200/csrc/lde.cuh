@@ -68,6 +68,23 @@ __device__ __forceinline__ uint64_t shl(uint64_t x) {
         h1 = x1 >> 16;
     }
     uint32_t r0, r1;
+    if (S == 24) {  // h1 = 0: the generic form's first five instructions do nothing
+        asm("{\n\t.reg .u32 m, u0, u1, t0, t1;\n\t.reg .pred q;\n\t"
+            "sub.cc.u32 u0, 0, %4;\n\t"    // h0*eps
+            "subc.u32 u1, %4, 0;\n\t"
+            "add.cc.u32 %0, %2, u0;\n\t"
+            "addc.cc.u32 %1, %3, u1;\n\t"
+            "addc.u32 m, 0, 0;\n\t"
+            "add.cc.u32 t0, %0, 0xFFFFFFFF;\n\t"  // r + eps: r - p, or the value of a wrapped sum
+            "addc.cc.u32 t1, %1, 0;\n\t"
+            "addc.u32 m, m, 0;\n\t"
+            "setp.ne.u32 q, m, 0;\n\t"
+            "selp.b32 %0, t0, %0, q;\n\t"
+            "selp.b32 %1, t1, %1, q;\n\t}"
+            : "=&r"(r0), "=&r"(r1)
+            : "r"(l0), "r"(l1), "r"(h0));
+        return ((uint64_t)r1 << 32) | r0;
+    }
     asm("{\n\t.reg .u32 m, u0, u1, t0, t1;\n\t.reg .pred q;\n\t"
         "sub.cc.u32 %0, %2, %5;\n\t"   // (l1:l0) - h1
         "subc.cc.u32 %1, %3, 0;\n\t"
