@@ -150,26 +150,6 @@ __device__ __forceinline__ uint64_t mul_weak(uint64_t a, uint64_t b) {
     mul128_dev(a, b, r0, r1, r2, r3);
     return reduce4_dev(r0, r1, r2, r3);
 }
-// a*b + c for a, b, c < 2^64 (below 2^128), weakly reduced. The addend
-// enters the first partial product's carry chain (a*b + c <= 2^128 - 2^64).
-__device__ __forceinline__ uint64_t mul_add_weak(uint64_t a, uint64_t b, uint64_t c) {
-    uint32_t r0, r1, r2, r3;
-    asm("mad.lo.cc.u32 %0, %4, %6, %8;\n\t"
-        "madc.hi.cc.u32 %1, %4, %6, %9;\n\t"
-        "addc.u32 %2, 0, 0;\n\t"
-        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
-        "madc.hi.cc.u32 %2, %4, %7, %2;\n\t"
-        "addc.u32 %3, 0, 0;\n\t"
-        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
-        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
-        "addc.u32 %3, %3, 0;\n\t"
-        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
-        "madc.hi.u32 %3, %5, %7, %3;"
-        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
-        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)),
-          "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
-    return reduce4_dev(r0, r1, r2, r3);
-}
 #endif
 #if defined(__CUDACC__)
 // Lazy sum of products: sum a_i * b_i held in 160 bits (r4 counts the
