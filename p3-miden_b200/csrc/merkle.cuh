@@ -209,7 +209,9 @@ __device__ __forceinline__ Lane lane_consts(const uint64_t *sc, int l) {
 }
 // circ(2*M4, M4, M4) for word l: M4 row (l mod 4) of its block, plus the sum
 // over the three blocks of that row; lanes 12..15 return 0
-__device__ __forceinline__ uint64_t ext_linear(uint64_t x, int l) {
+// rc: the lane's constant of the next round (0 for none), added to the
+// 96-bit sum before the reduction
+__device__ __forceinline__ uint64_t ext_linear(uint64_t x, int l, uint64_t rc = 0) {
     using namespace p2w;
     const int base = l & ~3, j = l & 3;
     const uint64_t x0 = shfl64(x, base), x1 = shfl64(x, base + 1), x2 = shfl64(x, base + 2), x3 = shfl64(x, base + 3);
@@ -219,17 +221,20 @@ __device__ __forceinline__ uint64_t ext_linear(uint64_t x, int l) {
     const W f = j == 0 ? t01 : j == 1 ? wdbl(x2) : j == 2 ? t23 : wdbl(x0);
     const W y = wadd(wadd1(t0123, e), f);
     const W t = wadd(wadd(shflW(y, j), shflW(y, j + 4)), shflW(y, j + 8));
-    return l < 12 ? wreduce(wadd(y, t)) : 0;
+    return l < 12 ? wreduce(wadd1(wadd(y, t), rc)) : 0;
 }
+// four external rounds whose first constant is already in x; each linear
+// layer takes in the next round's constant
 __device__ __forceinline__ uint64_t ext_rounds(uint64_t x, int l, const uint64_t *rc) {
     const int li = l < 12 ? l : 11;
 #pragma unroll 1
-    for (int r = 0; r < 4; r++) x = ext_linear(p2w::sbox(p2w::add_c(x, rc[12 * r + li])), l);
+    for (int r = 0; r < 4; r++) x = ext_linear(p2w::sbox(x), l, r < 3 ? rc[12 * (r + 1) + li] : 0);
     return x;
 }
 __device__ __forceinline__ uint64_t permute(uint64_t x, int l, const uint64_t *sc, const Lane &k) {
     using namespace p2w;
-    x = ext_rounds(ext_linear(x, l), l, sc + p2::OFF_INIT);
+    const int li = l < 12 ? l : 11;
+    x = ext_rounds(ext_linear(x, l, sc[p2::OFF_INIT + li]), l, sc + p2::OFF_INIT);
     uint64_t z = shfl64(x, 0);
     const bool rest = l >= 1 && l < 12;
 #pragma unroll 1
@@ -242,7 +247,7 @@ __device__ __forceinline__ uint64_t permute(uint64_t x, int l, const uint64_t *s
         x = rest ? mul_add_w(x, k.mu, wadd1(P, zs)) : 0;     // sum < 12 * 2^64
     }
     if (l == 0) x = z;
-    return ext_rounds(x, l, sc + p2::OFF_TERM);
+    return ext_rounds(add_c(x, sc[p2::OFF_TERM + li]), l, sc + p2::OFF_TERM);
 }
 }  // namespace p2x
 

@@ -102,6 +102,16 @@ GL_HD gl::ef mul(gl::ef a, gl::ef b) { return gl::ef_mul(a, b); }
 GL_HD uint64_t dbl(uint64_t a) { return gl::dbl(a); }
 GL_HD gl::ef dbl(gl::ef a) { return gl::ef_add(a, a); }
 GL_HD uint64_t mulc(uint64_t a, uint64_t c) { return gl::mul(a, c); }  // by a base-field constant
+// a product that goes straight into the fold: the lazy accumulator takes any
+// 64-bit word, so the device form skips the final canonicalisation
+GL_HD uint64_t mulw(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return gl::mul_weak(a, b);
+#else
+    return gl::mul(a, b);
+#endif
+}
+GL_HD gl::ef mulw(gl::ef a, gl::ef b) { return gl::ef_mul(a, b); }
 GL_HD gl::ef mulc(gl::ef a, uint64_t c) { return gl::ef_mulf(a, c); }
 GL_HD void konst(uint64_t c, uint64_t &out) { out = c; }
 GL_HD void konst(uint64_t c, gl::ef &out) { out = gl::ef{c, 0}; }
@@ -120,7 +130,7 @@ GL_HD T kxor3(T a, T b, T c) { return kxor2(a, kxor2(b, c)); }
 template <class T>
 GL_HD T kandn(T a, T b) { return fo::mul(fo::sub(fo::k<T>(1), a), b); }
 template <class T>
-GL_HD T kbool(T a) { return fo::mul(a, fo::sub(a, fo::k<T>(1))); }
+GL_HD T kbool(T a) { return fo::mulw(a, fo::sub(a, fo::k<T>(1))); }  // only ever emitted
 
 // Keccak tables for the constraint bodies: rho offsets rot[x*5+y] and the
 // round constants, from constant memory (device) or host arrays.
@@ -217,27 +227,27 @@ GL_HD void keccak_task(int t, const T *L, const T *N, T first, T trans, F &f) {
         T sm = fo::k<T>(0);
         for (int y = 0; y < 5; y++) sm = fo::add(sm, L[KC_AP + (y * 5 + x) * 64 + z]);
         T d = fo::sub(sm, cp);
-        f.emit(2590 + i, fo::mul(fo::mul(d, fo::sub(d, fo::k<T>(2))), fo::sub(d, fo::k<T>(4))));
+        f.emit(2590 + i, fo::mulw(fo::mul(d, fo::sub(d, fo::k<T>(2))), fo::sub(d, fo::k<T>(4))));
     } else if (t < 1176) {  // first-row flags
         int i = t - 1152;
-        f.emit(i, fo::mul(first, i == 0 ? fo::sub(L[KC_STEP], fo::k<T>(1)) : L[KC_STEP + i]));
+        f.emit(i, fo::mulw(first, i == 0 ? fo::sub(L[KC_STEP], fo::k<T>(1)) : L[KC_STEP + i]));
     } else if (t < 1200) {  // flag rotation
         int i = t - 1176;
-        f.emit(24 + i, fo::mul(trans, fo::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
+        f.emit(24 + i, fo::mulw(trans, fo::sub(N[KC_STEP + (i + 1) % 24], L[KC_STEP + i])));
     } else if (t < 1300) {  // first step: preimage == a
         int o = t - 1200;
-        f.emit(48 + o, fo::mul(L[KC_STEP], fo::sub(L[KC_PRE + o], L[KC_A + o])));
+        f.emit(48 + o, fo::mulw(L[KC_STEP], fo::sub(L[KC_PRE + o], L[KC_A + o])));
     } else if (t < 1302) {  // export
         T ex = L[KC_EXPORT];
         if (t == 1300) f.emit(148, kbool(ex));
-        else f.emit(149, fo::mul(not_final, ex));
+        else f.emit(149, fo::mulw(not_final, ex));
     } else if (t < 1402) {  // preimage continuity
         int o = t - 1302;
-        f.emit(150 + o, fo::mul(fo::mul(not_final, trans), fo::sub(L[KC_PRE + o], N[KC_PRE + o])));
+        f.emit(150 + o, fo::mulw(fo::mul(not_final, trans), fo::sub(L[KC_PRE + o], N[KC_PRE + o])));
     } else {  // round output == next round input (x outer, y inner)
         int i = t - 1402, x = i / 20, y = (i / 4) % 5, l = i % 4;
         T outv = (x == 0 && y == 0) ? L[KC_APPP00 + l] : L[KC_APP + (y * 5 + x) * 4 + l];
-        f.emit(3082 + i, fo::mul(fo::mul(not_final, trans), fo::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
+        f.emit(3082 + i, fo::mulw(fo::mul(not_final, trans), fo::sub(outv, N[KC_A + (y * 5 + x) * 4 + l])));
     }
 }
 
