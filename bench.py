@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -35,19 +36,29 @@ N_PERMS = 10922
 LOG_H = 18  # overridden by --log-h for small profiling cases
 PCS = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bits=16,
            deep_pow_bits=0, num_queries=100, query_pow_bits=0)
-WORKLOAD = "keccak-f1600 AIR, 10922 perms -> 2^18 x 2633 Goldilocks trace, lifted STARK (Poseidon2-12 LMCS)"
 METRIC = "proofs/s"
-# DRAM bytes per algorithmic byte, from ncu captures of one full-size column
-# slab (2^18 x 336 through the LDE, 2^19 leaves through the sponge): the sum of
-# dram__bytes_read.sum + dram__bytes_write.sum over the slab's launches divided
-# by the slab's algorithmic bytes; the slabs of the 2^18 x 2633 trace are alike.
-LDE_TRAFFIC_PER_ALG_BYTE = 2.93
-HASH_TRAFFIC_PER_ALG_BYTE = 1.03
-# Binding resource of the two kernels, from the same captures (ncu
-# sm__inst_executed_pipe_alu / smsp__issue_active, % of peak).
-HASH_BINDING = ("integer ALU pipe: 19.9 k instructions per permutation; 74.9 % of the ALU pipe and 66.7 % issue "
-                "at 21.5 k instructions per permutation (ncu, full-size slab)")
-LDE_BINDING = "integer ALU pipe: 74-80 % of peak, issue 60-68 % (ncu, full-size slab)"
+# ncu summaries of the current kernels (profiles/): per-launch instruction
+# counts, pipe utilisation and DRAM traffic, each with the command that made it
+HASH_PROFILE = ROOT / "profiles" / "leaf_class_kernel_slab_2e18.json"
+LDE_PROFILE = ROOT / "profiles" / "lde_kernels_slab_2e18.json"
+
+
+def workload_name() -> str:
+    return (f"keccak-f1600 AIR, {N_PERMS} perms -> 2^{LOG_H} x 2633 Goldilocks trace, "
+            f"lifted STARK (Poseidon2-12 LMCS)")
+
+
+def base_config() -> dict:
+    """The workload description shared by both arms (the GPU prover and the
+    CPU reference arm) so that their lines name the same configuration."""
+    return {"workload": workload_name(), "pcs": PCS}
+
+
+def load_profile(path: Path):
+    try:
+        return json.loads(path.read_text())
+    except Exception:
+        return None
 
 
 def load_product():
@@ -73,11 +84,12 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_gpu{gpu}.csv"
+        fd, name = tempfile.mkstemp(prefix=f"p3g_clocks_gpu{gpu}_", suffix=".csv")
+        os.close(fd)
+        self.path = Path(name)
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu),
@@ -108,6 +120,11 @@ class ClockSampler:
             return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
         except Exception:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        finally:
+            try:
+                self.path.unlink()
+            except OSError:
+                pass
 
 
 def dist_setup(backend: str = "nccl"):
@@ -187,28 +204,102 @@ def cpu_sample_rate(log_h_sample: int, threads: int, reps: int):
 
 
 def run_reference(args):
+    """The CPU arm: the oracle (a plain-C restatement of the reference prover;
+    the Rust reference cannot be built without a Rust toolchain) on all host
+    cores. Each step is one full oracle proof of a 2^12-row sample of the
+    workload (170 permutations, same parameters, about 10 s on 16 cores), so
+    that the whole run ends within minutes; ms_per_step is that sample's time
+    and value extrapolates it linearly in rows to the 2^18 workload."""
     # CPU-only arm with no collectives: under torchrun, rank 0 alone runs and prints
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     threads = os.cpu_count() or 1
     log_s = int(os.environ.get("P3G_CPU_SAMPLE_LOG_H", "12"))
-    sample = f"full oracle proof of a 2^{log_s}-row Keccak trace ({(1 << log_s) // 24} perms), " \
-             f"same parameters, scaled x{1 << (LOG_H - log_s)} (linear in rows) to the 2^18 workload"
     _, scale = cpu_sample_rate(log_s, threads, max(1, args.warmup))
     times, scale = cpu_sample_rate(log_s, threads, args.steps)
-    per_proof = statistics.median(times) * scale
+    sample_s = statistics.median(times)
+    per_proof = sample_s * scale
     value = 1.0 / per_proof
+    sample = (f"one full oracle proof of a 2^{log_s}-row Keccak trace ({(1 << log_s) // 24} perms, same parameters) "
+              f"per step, median {sample_s:.2f} s on {threads} threads, scaled x{int(scale)} (linear in rows) "
+              f"to the 2^{LOG_H} workload")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_proof * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks, exact)",
         "data": "synthetic (seeded Keccak-f inputs)",
-        "config": {"workload": WORKLOAD, "pcs": PCS, "parallelism": "host threads"},
+        "config": base_config(),
+        "arm": {"parallelism": f"{threads} host threads (OpenMP)", "ms_per_proof_extrapolated": per_proof * 1e3,
+                "step": f"a 2^{log_s}-row sample proof"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def slab_widths(w: int):
+    """Column slabs of the main commit (prover.cuh commit_main_pipelined)."""
+    sw = ((w + 7) // 8 + 7) // 8 * 8 if w >= 256 else w
+    return [min(sw, w - c0) for c0 in range(0, w, sw)]
+
+
+def hash_roofline(n_lde: int, w: int, leaf_ms: float, n_launches: int, hbm_peak: float, peak_src: str,
+                  sm_mhz):
+    """Roofline line of the dominant kernel, merkle::leaf_class_kernel (one
+    launch per column slab). It is bound by the integer ALU pipe: achieved =
+    this run's ALU-pipe warp instructions per second (the live launch time
+    times the per-permutation ALU count of the committed ncu summary), peak =
+    the pipe's rate at this run's SM clock (from the same summary's
+    instruction count and % of peak). The HBM figures sit beside it."""
+    n_launches = max(1, n_launches)
+    launch_s = leaf_ms / 1e3 / n_launches
+    perms = n_lde * sum((x + 7) // 8 for x in slab_widths(w))
+    perms_per_launch = perms / n_launches
+    alg_bytes = 8.0 * n_lde * w / n_launches
+    hbm_gbs = alg_bytes / launch_s / 1e9
+    hbm = {"achieved": hbm_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_gbs / hbm_peak,
+           "peak_source": peak_src, "algorithmic_bytes": alg_bytes}
+    base = {"kernel": "merkle::leaf_class_kernel (LMCS leaf sponge, Poseidon2-12)", "kernel_ms": launch_s * 1e3,
+            "launches_per_proof": n_launches, "perms_per_launch": perms_per_launch,
+            "perms_per_s": perms_per_launch / launch_s, "algorithmic_bytes": alg_bytes}
+    prof = load_profile(HASH_PROFILE)
+    if not prof:
+        return {**base, "bound": "hbm", "achieved": hbm_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": hbm_gbs / hbm_peak, "traffic": None, "peak_source": peak_src}
+    alu_per_perm = prof["inst_alu"] / prof["perms_per_launch"]
+    peak_rate = prof["inst_alu"] / (prof["duration_ns"] * 1e-9) / (prof["alu_pct_of_peak"] / 100.0)
+    if sm_mhz and prof.get("sm_mhz"):
+        peak_rate *= sm_mhz / prof["sm_mhz"]
+    achieved = perms_per_launch * alu_per_perm / launch_s
+    return {**base, "bound": "int_alu", "achieved": achieved / 1e9, "peak": peak_rate / 1e9,
+            "unit": "G warp-instructions/s (ALU pipe)", "frac": achieved / peak_rate,
+            "traffic": prof["dram_bytes"] / prof["perms_per_launch"] * perms_per_launch,
+            "alu_inst_per_perm": alu_per_perm, "issue_frac_in_profile": prof["issue_pct"] / 100.0,
+            "peak_source": f"ALU-pipe rate from {HASH_PROFILE.relative_to(ROOT)}", "hbm": hbm}
+
+
+def lde_roofline(w: int, B: int, lde_ms: float, hbm_peak: float, sm_mhz):
+    """The main-trace coset LDE (3 launches per column slab): HBM fraction of
+    the algorithmic bytes 8*w*N*(1+B), and its binding resource, the integer
+    ALU pipe, scaled from the committed ncu summary by algorithmic bytes."""
+    lde_bytes = 8.0 * w * (1 << LOG_H) * (1 + B)
+    gbs = lde_bytes / (lde_ms * 1e-3) / 1e9
+    out = {"kernel": "lde::lde_pass_kernel + lde::lde_fused_kernel (coset LDE, 3 launches x 8 slabs)",
+           "bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+           "algorithmic_bytes": lde_bytes, "kernel_ms": lde_ms, "traffic": None}
+    prof = load_profile(LDE_PROFILE)
+    if prof:
+        per_byte = prof["inst_alu"] / prof["algorithmic_bytes"]
+        peak_rate = prof["inst_alu"] / (prof["duration_ns"] * 1e-9) / (prof["alu_pct_of_peak"] / 100.0)
+        if sm_mhz and prof.get("sm_mhz"):
+            peak_rate *= sm_mhz / prof["sm_mhz"]
+        achieved = per_byte * lde_bytes / (lde_ms * 1e-3)
+        out.update({"bound": "int_alu", "traffic": prof["dram_bytes"] / prof["algorithmic_bytes"] * lde_bytes,
+                    "alu_pipe": {"achieved": achieved / 1e9, "peak": peak_rate / 1e9,
+                                 "unit": "G warp-instructions/s (ALU pipe)", "frac": achieved / peak_rate,
+                                 "source": str(LDE_PROFILE.relative_to(ROOT))}})
+    return out
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -236,13 +327,15 @@ def run_gpu(args):
     ref_digest = out.digest.copy()
     barrier(pg, dev)
     torch.cuda.synchronize(dev)
-    lat, launches, stages, lde_k = [], 0, np.zeros(len(P.STAGES)), []
+    lat, launches, stages, lde_k, leaf_k = [], 0, np.zeros(len(P.STAGES)), [], []
     with ClockSampler(dev) as clocks:
         t0 = time.perf_counter()
         for _ in range(args.steps):
             out = P.prove_multi(ctx, pcs, wit_dev)
             lat.append(out.device_ms)
             lde_k.append(out.lde_kernel_ms)
+            leaf_k.append(out.leaf_kernel_ms)
+            leaf_n = out.leaf_launches
             launches += out.gpu_launches
             stages += np.array(out.stage_ms)
             assert np.array_equal(out.digest, ref_digest), "non-deterministic proof"
@@ -302,38 +395,27 @@ def run_gpu(args):
     w = P.KECCAK_NUM_COLS
     B = 1 << PCS["log_blowup"]
     n_lde = (1 << LOG_H) * B
-    # dominant kernel: the LMCS leaf sponge ("main tree" stage, which also holds
-    # the compress kernels); it reads every LDE word once
     tree_ms = float(stages_ms[1])
-    hash_bytes = 8 * w * n_lde
-    hash_gbs = hash_bytes / (tree_ms * 1e-3) / 1e9
     perms = n_lde * ((w + 7) // 8) + n_lde - 1
-    # coset LDE: 8*w*N*(1+B) algorithmic bytes over the LDE kernels' event time
-    lde_bytes = 8 * w * (1 << LOG_H) * (1 + B)
-    lde_ms = float(np.mean(lde_k))
-    lde_gbs = lde_bytes / (lde_ms * 1e-3) / 1e9
     dominant = int(np.argmax(stages_ms))
     clk = clocks.summary()
+    roofline = hash_roofline(n_lde, w, float(np.mean(leaf_k)), int(leaf_n), hbm_peak,
+                             "measured" if "hbm_gbs" in pk else "fallback", clk.get("sm_mhz"))
+    lde = lde_roofline(w, B, float(np.mean(lde_k)), hbm_peak, clk.get("sm_mhz"))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks, exact)",
         "data": "synthetic (seeded Keccak-f inputs)",
-        "config": {"workload": WORKLOAD, "pcs": PCS, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (5.5 GB trace, 11 GB LDE)", "timing": "CUDA events on the prover stream"},
+        "config": base_config(),
+        "arm": {"parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (5.5 GB trace, 11 GB LDE)",
+                "timing": "CUDA events on the prover stream"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "wall_per_step": wall / args.steps * 1e3},
         "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages_ms)},
         "dominant_stage": P.STAGES[dominant],
-        "roofline": {"kernel": "merkle::leaf_class_kernel (LMCS leaf sponge, Poseidon2-12)", "bound": "hbm",
-                     "achieved": hash_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": hash_gbs / hbm_peak,
-                     "traffic": HASH_TRAFFIC_PER_ALG_BYTE * hash_bytes, "algorithmic_bytes": hash_bytes,
-                     "kernel_ms": tree_ms, "peak_source": "measured" if "hbm_gbs" in pk else "fallback",
-                     "binding_resource": HASH_BINDING},
-        "lde": {"kernel": "lde::lde_pass_kernel + lde::lde_fused_kernel (coset LDE, 3 trips x 8 slabs)",
-                "bound": "hbm", "achieved": lde_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": lde_gbs / hbm_peak,
-                "traffic": LDE_TRAFFIC_PER_ALG_BYTE * lde_bytes, "algorithmic_bytes": lde_bytes, "kernel_ms": lde_ms,
-                "binding_resource": LDE_BINDING},
+        "roofline": roofline,
+        "lde": lde,
         "hash": {"kernel": "LMCS leaf sponge + compress (Poseidon2-12)", "perms": perms,
                  "perms_per_s": perms / (tree_ms * 1e-3)},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -346,13 +428,15 @@ def run_gpu(args):
         "proof_bytes": int(out.proof.fields.nbytes + out.proof.commitments.nbytes),
     }
     if args.cpu_baseline and world == 1:
-        log_s = int(os.environ.get("P3G_CPU_SAMPLE_LOG_H", "12"))
+        # one oracle proof of a 2^13-row sample (about 20 s on 16 host cores)
+        log_s = int(os.environ.get("P3G_CPU_SAMPLE_LOG_H", "13"))
         threads = os.cpu_count() or 1
-        times, scale = cpu_sample_rate(log_s, threads, 2)
+        times, scale = cpu_sample_rate(log_s, threads, 1)
         per_proof = min(times) * scale
         line["cpu_baseline"] = {
             "value": 1.0 / per_proof, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"oracle proof of a 2^{log_s}-row Keccak trace, x{int(scale)} linear scaling to 2^18 rows",
+            "sample": f"one oracle proof of a 2^{log_s}-row Keccak trace ({(1 << log_s) // 24} perms, same "
+                      f"parameters) in {min(times):.1f} s, x{int(scale)} linear scaling in rows to 2^{LOG_H}",
         }
     print(json.dumps(line), flush=True)
     ctx.close()
@@ -465,7 +549,7 @@ def run_verify(args):
         "metric": "verifications/s", "value": value, "unit": "verifications/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": statistics.median(wall), "higher_is_better": True,
         "dtype": "u64 (Goldilocks, exact)", "data": "synthetic (seeded Keccak-f inputs); proof from p3g_prove",
-        "config": {"workload": f"verify_multi of the {WORKLOAD} proof", "pcs": PCS, "proofs_per_call": B,
+        "config": {"workload": f"verify_multi of the {workload_name()} proof", "pcs": PCS, "proofs_per_call": B,
                    "proof_bytes": int(out.proof.fields.nbytes + out.proof.commitments.nbytes)},
         "split_ms": {"host replay + layout (median)": statistics.median(host),
                      "device: upload, kernels, read-back (median)": statistics.median(device)},

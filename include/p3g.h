@@ -13,8 +13,13 @@
  *  - Every call returns a status (P3G_OK = 0) and never aborts the process
  *    or traps the GPU; p3g_last_error() describes the last failure of a
  *    context. Calls on one context must come from one host thread at a time.
- *  - Results are bit-identical to the reference prover's on the same inputs
- *    (see the oracle under oracle/ and the parity tests).
+ *  - Results are bit-identical to the oracle's (oracle/, a CPU restatement of
+ *    the reference prover) on the same inputs and permutation table. The
+ *    pieces the reference takes from third-party crates that are not in its
+ *    source tree are restated, not pinned: the Poseidon2 internal diagonal
+ *    (a placeholder by default; the real table is a p3g_ctx_create
+ *    argument), DuplexChallenger::finalize, the grind witness choice and the
+ *    Keccak AIR's constraint order.
  */
 #ifndef P3G_H
 #define P3G_H
@@ -71,7 +76,9 @@ typedef struct {
     uint64_t *commits; /* 4 words per commitment */
     uint64_t n_commits;
     uint64_t digest[12];
-    double stage_ms[12]; /* device time per protocol stage; [11] = whole proof */
+    double stage_ms[12]; /* device time per protocol stage [0..7]; [8] main-trace LDE kernels;
+                            [9] main-tree leaf-sponge launches (span on the prover stream);
+                            [10] number of those launches; [11] = whole proof */
     uint64_t gpu_launches;
     uint64_t h2d_bytes, d2h_bytes;
 } p3g_proof;

@@ -187,3 +187,31 @@ void or_tree_prove_batch(const or_tree *t, const size_t *idx, size_t n_idx, or_t
     }
     free(known);
 }
+
+/* PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
+ * NaiveDft::coset_lde_batch of the columns repeated to the largest period p
+ * (p x w, row-major) on the coset of period_shift = lde_shift^(2^(log_h -
+ * log p)) (periodic.rs:66-71), natural order, (p << log_blowup) x w. Restated
+ * from the defining sums, O(p * pB) per column: interpolate on the subgroup
+ * of order p, then evaluate at period_shift * w_{pB}^i. */
+void or_periodic_lde(const uint64_t *repeated, size_t p, size_t w, unsigned log_blowup, unsigned log_trace_height,
+                     uint64_t lde_shift, uint64_t *out) {
+    unsigned lp = or_log2(p);
+    size_t n = p << log_blowup;
+    uint64_t ps = or_exp2(lde_shift % OR_P, log_trace_height - lp);
+    uint64_t wp_inv = or_inv(or_root(lp)), wn = or_root(lp + log_blowup), pinv = or_inv((uint64_t)p % OR_P);
+    uint64_t *coef = (uint64_t *)malloc(p * 8);
+    for (size_t c = 0; c < w; c++) {
+        for (size_t k = 0; k < p; k++) { /* a_k = (1/p) sum_j v_j w_p^{-jk} */
+            uint64_t s = 0;
+            for (size_t j = 0; j < p; j++) s = or_add(s, or_mul(repeated[j * w + c], or_pow(wp_inv, (j * k) % p)));
+            coef[k] = or_mul(s, pinv);
+        }
+        for (size_t i = 0; i < n; i++) { /* f(ps * w_n^i) by Horner */
+            uint64_t x = or_mul(ps, or_pow(wn, i)), acc = 0;
+            for (size_t k = p; k-- > 0;) acc = or_add(or_mul(acc, x), coef[k]);
+            out[i * w + c] = acc;
+        }
+    }
+    free(coef);
+}

@@ -78,6 +78,11 @@ void or_intt(uint64_t *a, size_t n); /* inverse, includes 1/n */
 void or_coset_lde_bitrev(const uint64_t *in, size_t h, size_t w, unsigned log_blowup,
                          uint64_t shift, uint64_t *out);
 
+/* PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
+ * natural-order coset LDE of the repeated periodic columns (NaiveDft). */
+void or_periodic_lde(const uint64_t *repeated, size_t p, size_t w, unsigned log_blowup, unsigned log_trace_height,
+                     uint64_t lde_shift, uint64_t *out);
+
 /* ----------------------------------------------------------------- LMCS */
 typedef struct {
     const uint64_t *data; /* row-major */

@@ -393,6 +393,8 @@ class StarkOutput:
     d2h_bytes: int
     device_ms: float  # whole proof on the device timeline (CUDA events)
     lde_kernel_ms: float = 0.0  # main-trace coset-LDE kernels (events on their stream)
+    leaf_kernel_ms: float = 0.0  # main-tree leaf-sponge launches (events on the prover stream)
+    leaf_launches: int = 0
 
 
 # Device-timeline stages of one proof. "main LDE" ends when the last column
@@ -435,7 +437,8 @@ def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> St
         commits = np.ctypeslib.as_array(out.commits, shape=(out.n_commits * 4,)).reshape(-1, 4).copy()
         res = StarkOutput(np.array(out.digest[:], dtype=np.uint64), TranscriptData(fields, commits),
                           list(out.stage_ms[:len(STAGES)]), int(out.gpu_launches), int(out.h2d_bytes),
-                          int(out.d2h_bytes), float(out.stage_ms[11]), float(out.stage_ms[8]))
+                          int(out.d2h_bytes), float(out.stage_ms[11]), float(out.stage_ms[8]),
+                          float(out.stage_ms[9]), int(out.stage_ms[10]))
     finally:
         lib().p3g_proof_free(C.byref(out))
     return res

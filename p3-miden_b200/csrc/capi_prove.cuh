@@ -98,6 +98,7 @@ P3G_API int p3g_prove(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instanc
     }
     try {
         CK(cudaSetDevice(x->c.device));
+        p3g::bind_p2(x->c);
         p3g::ensure_keccak_tables(x->c.device);
         std::vector<p3g::Instance> ins(n);
         for (uint64_t i = 0; i < n; i++)

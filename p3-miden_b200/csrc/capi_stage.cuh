@@ -14,6 +14,7 @@ struct p3g_tree {
 
 #define P3G_TRY(ctxp, ...)                                    \
     try {                                                     \
+        if (ctxp) ::p3g::bind_p2((ctxp)->c);                  \
         __VA_ARGS__;                                          \
         return p3g::OK;                                       \
     } catch (const p3g::CudaError &e) {                       \
@@ -34,7 +35,7 @@ P3G_API int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&x->c.stream, cudaStreamNonBlocking));
         memcpy(x->c.p2, poseidon2_params130, sizeof(x->c.p2));
-        CK(cudaMemcpyToSymbol(c_p2, x->c.p2, sizeof(x->c.p2)));
+        p3g::bind_p2(x->c);
         // keep freed blocks in the pool across proofs
         cudaMemPool_t pool;
         CK(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -115,6 +116,7 @@ P3G_API int p3g_lmcs_build(p3g_ctx *x, const uint64_t *const *d_mats, const uint
     p3g_tree *t = new p3g_tree();
     try {
         CK(cudaSetDevice(x->c.device));
+        p3g::bind_p2(x->c);
         std::vector<p3g::Mat> mats;
         for (uint64_t i = 0; i < n; i++) mats.push_back({d_mats[i], heights[i], widths[i]});
         p3g::build_tree(x->c, t->t, mats, alignment);
@@ -145,6 +147,7 @@ P3G_API int p3g_lmcs_build_hiding(p3g_ctx *x, const uint64_t *const *d_mats, con
     p3g_tree *t = new p3g_tree();
     try {
         CK(cudaSetDevice(x->c.device));
+        p3g::bind_p2(x->c);
         std::vector<p3g::Mat> mats;
         for (uint64_t i = 0; i < n; i++) mats.push_back({d_mats[i], heights[i], widths[i]});
         const p3g::Mat salt{d_salt, heights[n - 1], salt_width};

@@ -167,6 +167,24 @@ struct Ctx {
     }
 };
 
+// The permutation constants live in the __constant__ table c_p2, one copy
+// per device for the whole process. Each context keeps its own constants
+// (the StarkConfig's permutation) and makes them current on its device
+// before launching kernels that hash; the upload happens only when a context
+// with different constants ran last on that device. Contexts whose constants
+// differ must therefore not have hashing kernels in flight at the same time.
+inline void bind_p2(const Ctx &ctx) {
+    static std::mutex mu;
+    static std::map<int, std::vector<uint64_t>> bound;
+    std::lock_guard<std::mutex> lk(mu);
+    std::vector<uint64_t> &b = bound[ctx.device];
+    if (b.size() == p2::N_PARAMS && memcmp(b.data(), ctx.p2, sizeof(ctx.p2)) == 0) return;
+    CK(cudaSetDevice(ctx.device));
+    CK(cudaDeviceSynchronize());  // kernels of the previous constants finish first
+    CK(cudaMemcpyToSymbol(c_p2, ctx.p2, sizeof(ctx.p2)));
+    b.assign(ctx.p2, ctx.p2 + p2::N_PARAMS);
+}
+
 // Host-built two-level power table of v for exponents < 2^L.
 inline void pow_table(uint64_t v, uint32_t L, uint32_t lo_bits, std::vector<uint64_t> &out_lo,
                       std::vector<uint64_t> &out_hi) {

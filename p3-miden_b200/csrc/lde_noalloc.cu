@@ -24,12 +24,21 @@
 // Set-up: the first call on each device (with that device current) looks up
 // the array's device address with cudaGetSymbolAddress and sets the kernels'
 // shared-memory limits; make that first call before any stream capture.
+// The address is cached for the life of the process: a cudaDeviceReset (or
+// any other end of the device's primary context) invalidates it, and this
+// entry point does not support calls after one.
 // The call is asynchronous on `stream` (0 = the legacy default stream).
+//
+// Errors: P3G_ERR_INVALID for arguments outside the limits (nothing is
+// queued); P3G_ERR_CUDA when a launch fails, or when an error from earlier,
+// unrelated work is already pending on this host thread (that error is left
+// in place for its owner and nothing is queued).
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <mutex>
 
+#include "../../include/p3g.h"
 #include "gl.cuh"
 #include "ntt.cuh"
 
@@ -85,7 +94,7 @@ int setup_device(int dev, uint64_t **out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_ptr[dev]) {
         uint64_t *p = nullptr;
-        if (cudaGetSymbolAddress((void **)&p, g_lde_scratch) != cudaSuccess || !p) return 5;
+        if (cudaGetSymbolAddress((void **)&p, g_lde_scratch) != cudaSuccess || !p) return P3G_ERR_CUDA;
         set_smem_limit<2, false>();
         set_smem_limit<4, false>();
         set_smem_limit<8, false>();
@@ -104,6 +113,11 @@ unsigned log2_exact(uint64_t n) {
     return l;
 }
 
+// Column tiles sit on grid.y, whose limit is 65535: a wide matrix is
+// launched in column chunks of at most 65535 tiles (the row strides stay the
+// full width, so each chunk is the same pass over a column range).
+constexpr uint64_t MAX_TILES_Y = 65535;
+
 template <bool DIF>
 void launch(const ntt::PassArgs &a, uint64_t h, cudaStream_t s) {
     uint32_t k = a.bhi - a.blo;
@@ -115,8 +129,14 @@ void launch(const ntt::PassArgs &a, uint64_t h, cudaStream_t s) {
         dim3 g((unsigned)(h >> k), (unsigned)((a.w + 3) / 4));
         ntt::ntt_pass_kernel<4, DIF><<<g, 256, (smem_words_per_col * 4 + 512 + 16) * 8, s>>>(a);
     } else {
-        dim3 g((unsigned)(h >> k), (unsigned)((a.w + 7) / 8));
-        ntt::ntt_pass_kernel<8, DIF><<<g, 256, (smem_words_per_col * 8 + 512 + 16) * 8, s>>>(a);
+        for (uint64_t c0 = 0; c0 < a.w; c0 += 8 * MAX_TILES_Y) {
+            ntt::PassArgs b = a;
+            b.src = a.src + c0;
+            b.dst = a.dst + c0;
+            b.w = a.w - c0 < 8 * MAX_TILES_Y ? a.w - c0 : 8 * MAX_TILES_Y;
+            dim3 g((unsigned)(h >> k), (unsigned)((b.w + 7) / 8));
+            ntt::ntt_pass_kernel<8, DIF><<<g, 256, (smem_words_per_col * 8 + 512 + 16) * 8, s>>>(b);
+        }
     }
 }
 
@@ -126,14 +146,17 @@ extern "C" __attribute__((visibility("default"))) int p3g_coset_lde_noalloc(cons
                                                                          uint64_t width, uint32_t log_blowup,
                                                                          uint64_t shift, uint64_t *d_out,
                                                                          void *stream) {
-    if (!d_in || !d_out || height == 0 || (height & (height - 1)) || width == 0) return 1;
+    if (!d_in || !d_out || height == 0 || (height & (height - 1)) || width == 0) return P3G_ERR_INVALID;
     const uint32_t L = log2_exact(height);
-    if (L > NOALLOC_MAX_LOG_H || log_blowup > 8 || L + log_blowup > 32) return 1;
-    if (width > NOALLOC_MAX_WORDS || height * width > NOALLOC_MAX_WORDS) return 1;
+    if (L > NOALLOC_MAX_LOG_H || log_blowup > 8 || L + log_blowup > 32) return P3G_ERR_INVALID;
+    if (width > NOALLOC_MAX_WORDS || height * width > NOALLOC_MAX_WORDS) return P3G_ERR_INVALID;
+    // an error left by earlier work on this thread is not this call's: report
+    // it without clearing it, and queue nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return P3G_ERR_CUDA;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 5;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return P3G_ERR_CUDA;
     uint64_t *S = nullptr;
-    if (setup_device(dev, &S)) return 5;
+    if (setup_device(dev, &S)) return P3G_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
     shift %= gl::P;
 
@@ -197,7 +220,7 @@ extern "C" __attribute__((visibility("default"))) int p3g_coset_lde_noalloc(cons
         }
         sk = gl::mul(sk, wb);
     }
-    return cudaGetLastError() == cudaSuccess ? 0 : 5;
+    return cudaGetLastError() == cudaSuccess ? P3G_OK : P3G_ERR_CUDA;
 }
 
 extern "C" __attribute__((visibility("default"))) uint64_t p3g_coset_lde_noalloc_max_words(void) {

@@ -213,11 +213,15 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
     // starts after the whole LDE and each phase runs alone.
     const uint64_t *prev = nullptr;
     uint32_t prev_log = 0;
+    cudaEvent_t ev_leaf[2];
+    CK(cudaEventCreate(&ev_leaf[0]));
+    CK(cudaEventCreate(&ev_leaf[1]));
     for (size_t s = 0; s < slabs.size(); s++) {
         const Slab &sl = slabs[s];
         const Instance &I = inst[sl.trace];
         const uint64_t h = I.height, w = I.width;
         CK(cudaStreamWaitEvent(ctx.stream, any_host ? ev_lde[s] : ev_lde[slabs.size() - 1], 0));
+        if (s == 0) CK(cudaEventRecord(ev_leaf[0], ctx.stream));
         merkle::ClassArgs a{};
         a.n_mats = 1;
         a.data[0] = main_lde[sl.trace].p + sl.c0;
@@ -234,6 +238,7 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
         prev = out_states;
         prev_log = a.log_h;
     }
+    CK(cudaEventRecord(ev_leaf[1], ctx.stream));
     CK(cudaEventRecord(ev_lde_done, ctx.lde_stream));  // the last LDE slab is written
     finish_tree(ctx, t);
     t.mats = main_mats;
@@ -247,6 +252,14 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
         cudaEventDestroy(ev_t0[s]);
     }
     po.stage_ms[8] = lde_ms;
+    // leaf sponge: the span of its launches on the context stream (with a
+    // host trace the span also holds waits for slab LDEs) and their count
+    float leaf_ms = 0;
+    CK(cudaEventElapsedTime(&leaf_ms, ev_leaf[0], ev_leaf[1]));
+    po.stage_ms[9] = leaf_ms;
+    po.stage_ms[10] = (double)slabs.size();
+    cudaEventDestroy(ev_leaf[0]);
+    cudaEventDestroy(ev_leaf[1]);
 }
 
 inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, ProofOut &po) {

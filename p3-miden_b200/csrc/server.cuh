@@ -84,7 +84,7 @@ class Server {
             memcpy(c->p2, p2, sizeof(c->p2));
             ctxs_.push_back(std::move(c));
         }
-        CK(cudaMemcpyToSymbol(c_p2, p2, p2::N_PARAMS * 8));
+        bind_p2(*ctxs_[0]);
         t0_ = std::chrono::steady_clock::now();
         for (uint32_t w = 0; w < n_workers; w++) workers_.emplace_back([this, w] { worker(w); });
     }
@@ -167,6 +167,7 @@ class Server {
             job->start_s = now_s();
             int st = OK;
             try {
+                bind_p2(ctx);
                 prove(ctx, job->pcs, job->inst.data(), job->inst.size(), job->out);
                 if (self_check_) {
                     const auto v0 = std::chrono::steady_clock::now();

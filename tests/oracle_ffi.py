@@ -105,6 +105,7 @@ def lib():
             ("or_ntt", None, [u64p, C.c_size_t]),
             ("or_intt", None, [u64p, C.c_size_t]),
             ("or_coset_lde_bitrev", None, [u64p, C.c_size_t, C.c_size_t, C.c_uint, C.c_uint64, u64p]),
+            ("or_periodic_lde", None, [u64p, C.c_size_t, C.c_size_t, C.c_uint, C.c_uint, C.c_uint64, u64p]),
             ("or_tree_build", None, [C.POINTER(P2Params), C.POINTER(Tree), C.POINTER(Matrix), C.c_size_t, C.c_size_t]),
             ("or_tree_root", None, [C.POINTER(Tree), u64p]),
             ("or_tree_build_hiding", None, [C.POINTER(P2Params), C.POINTER(Tree), C.POINTER(Matrix), C.c_size_t,
@@ -153,6 +154,22 @@ def default_p2() -> P2Params:
 def p2_to_array(pp: P2Params) -> np.ndarray:
     """Flatten to the product's layout: rc_init[48], rc_term[48], rc_int[22], diag[12]."""
     return np.frombuffer(bytes(pp), dtype=np.uint64).copy()
+
+
+def p2_from_array(a) -> P2Params:
+    """The inverse of p2_to_array: 130 words -> oracle parameters."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    assert a.size == 130
+    return P2Params.from_buffer_copy(a.tobytes())
+
+
+def periodic_lde(repeated: np.ndarray, log_blowup: int, log_trace_height: int, lde_shift: int) -> np.ndarray:
+    """PeriodicLde::build: natural-order LDE of the repeated periodic columns."""
+    r = np.ascontiguousarray(repeated, dtype=np.uint64)
+    p, w = r.shape
+    out = np.zeros((p << log_blowup, w), dtype=np.uint64)
+    lib().or_periodic_lde(ptr(r), p, w, log_blowup, log_trace_height, lde_shift, ptr(out))
+    return out
 
 
 def permute(pp: P2Params, st) -> np.ndarray:

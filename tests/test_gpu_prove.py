@@ -79,6 +79,53 @@ def test_keccak_42_perms_config(product, gpu_ctx):
     check_verifies(gpu, pcs, [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)])
 
 
+def test_keccak_2e13_bit_exact(product, gpu_ctx):
+    """341 permutations (8184 rows, padded to 2^13) with the headline's
+    parameters: the smallest whole proof whose main tree runs the
+    throughput leaf kernel (2^14 leaves, above the cooperative kernel's
+    4096) over the slab-carried sponge states, the multi-level compression
+    and the two-range LDE; bit-identical to the oracle."""
+    inputs = O.keccak_inputs(3, 341)
+    t = O.keccak_trace(inputs, 13)
+    pcs = product.PcsParams(1, 1, 0, 16, 0, 100, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_KECCAK, t)])
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_KECCAK, t, None)])
+    check_same(gpu, orc)
+    check_verifies(gpu, pcs, [(O.AIR_KECCAK, t.shape[0], t.shape[1], None)])
+
+
+def test_non_default_poseidon2_table(product, gpu_ctx):
+    """The prover is parametric in the 130-word permutation table the
+    StarkConfig supplies (configs.rs:215-217): with other round constants
+    and a random internal diagonal, GPU and oracle still agree bit for bit,
+    and the proof differs from the default table's. A context with the
+    default table used afterwards is unaffected."""
+    rng = np.random.default_rng(77)
+    diag = rng.integers(0, O.P, size=12, dtype=np.uint64)
+    table = product.poseidon2_params_from_seed(99, diag)
+    pp = O.p2_from_array(table)
+    k, t = O.cubic_trace(7, 12, 4)
+    k2, t2 = O.cubic_trace(9, 5, 6)
+    pcs = product.PcsParams(2, 2, 0, 5, 1, 16, 2)
+    inst = [product.AirWitness(product.AIR_CUBIC, t, k), product.AirWitness(product.AIR_CUBIC, t2, k2)]
+    oinst = [(O.AIR_CUBIC, t, k), (O.AIR_CUBIC, t2, k2)]
+    ctx = product.Context(0, table)
+    try:
+        gpu = product.prove_multi(ctx, pcs, inst)
+        kt = O.keccak_trace(O.keccak_inputs(5, 3), 7)
+        pcs_k = product.PcsParams(1, 1, 0, 6, 0, 12, 0)
+        gk = product.prove_multi(ctx, pcs_k, [product.AirWitness(product.AIR_KECCAK, kt)])
+    finally:
+        ctx.close()
+    check_same(gpu, O.prove(pp, pcs_dict(pcs), oinst))
+    check_same(gk, O.prove(pp, pcs_dict(pcs_k), [(O.AIR_KECCAK, kt, None)]))
+    assert O.verify(pp, pcs_dict(pcs), [(a, tt.shape[0], tt.shape[1], kk) for a, tt, kk in oinst],
+                    gpu.proof.fields, gpu.proof.commitments, gpu.digest) == 0
+    default = product.prove_multi(gpu_ctx, pcs, inst)
+    assert not np.array_equal(default.digest, gpu.digest)
+    check_same(default, O.prove(O.default_p2(), pcs_dict(pcs), oinst))
+
+
 def test_device_resident_trace(product, gpu_ctx):
     k, t = O.cubic_trace(6, 8, 5)
     pcs = product.PcsParams(1, 1, 0, 3, 0, 8, 0)

@@ -14,7 +14,11 @@ def rand_mat(rng, h, w):
 
 
 @pytest.mark.parametrize("log_h,w,log_blowup", [(0, 3, 1), (1, 1, 1), (3, 5, 2), (6, 9, 1), (10, 33, 1),
-                                                (11, 2, 3), (12, 64, 3), (13, 17, 1), (21, 3, 1)])
+                                                (11, 2, 3), (12, 64, 3), (13, 17, 1), (21, 3, 1),
+                                                # the headline trace's kernel instances (2^18 rows: two
+                                                # 9-bit ranges, 8-column tiles, blowup 2) and the lifted
+                                                # workload's tallest trace (2^20 rows, blowup 8)
+                                                (18, 16, 1), (20, 8, 3)])
 def test_coset_lde_matches_oracle(product, gpu_ctx, log_h, w, log_blowup):
     rng = np.random.default_rng(log_h * 100 + w)
     t = rand_mat(rng, 1 << log_h, w)
@@ -162,3 +166,17 @@ def test_periodic_lde_matches_full_lde(product, gpu_ctx, log_h, log_blowup, peri
     nat = brev[[_bitrev(i, L) for i in range(h << log_blowup)]]
     for i in range(h << log_blowup):
         assert np.array_equal(nat[i], per[i % per.shape[0]]), i
+
+
+@pytest.mark.parametrize("log_h,log_blowup,periods,shift", [(6, 1, [1, 2, 4, 8], 7), (10, 3, [16, 4], 7),
+                                                            (8, 2, [64, 1, 32], 11), (4, 1, [1], 7)])
+def test_periodic_lde_matches_oracle(product, gpu_ctx, log_h, log_blowup, periods, shift):
+    """p3g_periodic_lde against the oracle's NaiveDft restatement of
+    PeriodicLde::build (periodic.rs:49-81), bit for bit."""
+    rng = np.random.default_rng(log_h * 7 + sum(periods))
+    cols = [rng.integers(0, O.P, size=p, dtype=np.uint64) for p in periods]
+    max_p = max(periods)
+    repeated = np.array([[c[r % len(c)] for c in cols] for r in range(max_p)], dtype=np.uint64)
+    got = product.to_host(product.periodic_lde(gpu_ctx, product.to_device(repeated), log_blowup, log_h, shift))
+    want = O.periodic_lde(repeated, log_blowup, log_h, shift)
+    assert np.array_equal(got, want)

@@ -42,8 +42,12 @@ def test_noalloc_lde_matches_allocating_entry_point(product, gpu_ctx):
     fn, max_words = noalloc_fn(product)
     assert max_words == 1 << 21
     rng = np.random.default_rng(2025)
-    # two calls in a row with different shapes, then a repeat of the first
-    cases = [(12, 96, 1), (7, 5, 3), (12, 96, 1), (20, 2, 1)]
+    # two calls in a row with different shapes, then a repeat of the first;
+    # then the edges of the pass layout: height 1 (a pass of zero bits),
+    # blowup 1 (log_blowup 0), and the widest inputs the scratch admits
+    # (more column tiles than one launch's grid.y holds)
+    cases = [(12, 96, 1), (7, 5, 3), (12, 96, 1), (20, 2, 1),
+             (0, 3, 2), (10, 7, 0), (2, 1 << 19, 1), (1, 1 << 20, 1)]
     for log_h, w, lb in cases:
         t = rng.integers(0, P, size=(1 << log_h, w), dtype=np.uint64)
         shift = int(rng.integers(1, P, dtype=np.uint64))
