@@ -77,6 +77,19 @@ static int cmp_size(const void *a, const void *b) {
     return x < y ? -1 : x > y;
 }
 
+/* LiftedAir properties of an instance: the built-in AIRs declare the
+ * examples' dummy aux (one EF column, one challenge, no aux values,
+ * p3-miden-lifted-examples/src/lib.rs:93-103); symbolic AIRs their own. */
+size_t or_inst_aux_width(const or_instance *I) { return I->air == OR_AIR_SYMBOLIC ? I->sym->aux_width : 1; }
+size_t or_inst_num_randomness(const or_instance *I) { return I->air == OR_AIR_SYMBOLIC ? I->sym->num_randomness : 1; }
+size_t or_inst_num_aux_values(const or_instance *I) { return I->air == OR_AIR_SYMBOLIC ? I->sym->num_aux_values : 0; }
+unsigned or_inst_log_qd(const or_instance *I) {
+    return I->air == OR_AIR_SYMBOLIC ? or_sym_log_quotient_degree(I->sym) : or_air_log_quotient_degree(I->air);
+}
+size_t or_inst_num_constraints(const or_instance *I) {
+    return I->air == OR_AIR_SYMBOLIC ? I->sym->n_constraints : or_air_num_constraints(I->air, I->width);
+}
+
 int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
              or_proof *out) {
     memset(out, 0, sizeof(*out));
@@ -85,12 +98,15 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
     for (size_t i = 0; i < n_inst; i++) {
         if (inst[i].height < 2 || (inst[i].height & (inst[i].height - 1))) return 2;
         if (i && inst[i].height < inst[i - 1].height) return 3;
+        if (inst[i].air == OR_AIR_SYMBOLIC &&
+            (!inst[i].sym || or_sym_validate(inst[i].sym) || inst[i].sym->main_width != inst[i].width))
+            return 5;
     }
     const unsigned log_blowup = pcs->log_blowup;
     const unsigned log_max_h = or_log2(inst[n_inst - 1].height);
     unsigned log_qd = 0;
     for (size_t i = 0; i < n_inst; i++) {
-        unsigned l = or_air_log_quotient_degree(inst[i].air);
+        unsigned l = or_inst_log_qd(&inst[i]);
         if (l > log_qd) log_qd = l;
     }
     if (log_qd > log_blowup) return 4;
@@ -118,21 +134,42 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
     g_stage[0] = t1 - t0;
     t0 = t1;
 
-    /* 2. randomness (max over AIRs of num_randomness = 1) and the dummy aux
-     * traces: one EF column of zeros, flattened to 2 base columns
-     * (p3-miden-lifted-examples/src/lib.rs:93-103, prover/mod.rs:290-345). */
-    or_ef rnd = or_ch_sample_ef(&tr.ch);
-    (void)rnd;
-    uint64_t *auxt[8];
+    /* 2. randomness (max over the AIRs of num_randomness) and the aux
+     * traces from each instance's AuxBuilder, flattened EF -> 2 base columns
+     * (prover/mod.rs:285-345); without a builder the aux trace is all zero
+     * (the examples' dummy builder, p3-miden-lifted-examples/src/lib.rs:93-103). */
+    size_t n_rand = 0;
+    for (size_t i = 0; i < n_inst; i++)
+        if (or_inst_num_randomness(&inst[i]) > n_rand) n_rand = or_inst_num_randomness(&inst[i]);
+    uint64_t *rnd = (uint64_t *)calloc(2 * n_rand + 2, 8);
+    for (size_t r = 0; r < n_rand; r++) {
+        or_ef e = or_ch_sample_ef(&tr.ch);
+        rnd[2 * r] = e.c0, rnd[2 * r + 1] = e.c1;
+    }
+    uint64_t *auxt[8], *auxv[8];
     size_t aw[8];
     for (size_t i = 0; i < n_inst; i++) {
-        auxt[i] = (uint64_t *)calloc(hs[i] * 2, 8);
-        aw[i] = 2;
+        aw[i] = 2 * or_inst_aux_width(&inst[i]);
+        auxt[i] = (uint64_t *)calloc(hs[i] * aw[i] + 1, 8);
+        auxv[i] = (uint64_t *)calloc(2 * or_inst_num_aux_values(&inst[i]) + 2, 8);
+        if (inst[i].aux_build &&
+            inst[i].aux_build(inst[i].aux_user, i, inst[i].trace, rnd, or_inst_num_randomness(&inst[i]), hs[i],
+                              auxt[i], auxv[i]) != 0) {
+            for (size_t k = 0; k <= i; k++) free(auxt[k]), free(auxv[k]);
+            free(rnd);
+            or_tr_free(&tr);
+            committed_free(&mainc);
+            return 6;
+        }
     }
     commit_traces(pp, &auxc, (const uint64_t *const *)auxt, hs, aw, n_inst, log_blowup);
     for (size_t i = 0; i < n_inst; i++) free(auxt[i]);
     or_tree_root(&auxc.tree, out->aux_root);
     or_tr_send_commit(&tr, out->aux_root);
+    /* aux values, per instance in order (prover/mod.rs:347-353) */
+    for (size_t i = 0; i < n_inst; i++)
+        for (size_t k = 0; k < or_inst_num_aux_values(&inst[i]); k++)
+            or_tr_send_ef(&tr, or_ef_make(auxv[i][2 * k], auxv[i][2 * k + 1]));
     t1 = now_s();
     g_stage[1] = t1 - t0;
     t0 = t1;
@@ -168,9 +205,64 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
         /* selectors on the quotient coset (coset.rs:210-247) */
         uint64_t omega_h_inv = or_inv(or_root(log_h));
         uint64_t omega_q = or_root(log_qh);
-        size_t K = or_air_num_constraints(I->air, I->width);
+        size_t K = or_inst_num_constraints(I);
         const uint64_t *lde = mainc.ldes[ii];
         size_t w = I->width;
+        if (I->air == OR_AIR_SYMBOLIC) {
+            /* symbolic AIR: the DAG evaluated per point of gJ (constraints/mod.rs:63-179);
+             * aux rows as EF, periodic values from PeriodicLde on the
+             * quotient coset (periodic.rs:49-98, coset D, read at m mod its height) */
+            const or_sym_air *A = I->sym;
+            const uint64_t *alde = auxc.ldes[ii];
+            const size_t aux_w = A->aux_width, nper = A->num_periodic;
+            size_t max_p = 0;
+            uint64_t *rep = or_sym_periodic_matrix(A, &max_p);
+            uint64_t *plde = NULL;
+            size_t ph = 0;
+            if (rep) {
+                ph = max_p << log_qd;
+                plde = (uint64_t *)malloc(ph * nper * 8);
+                or_periodic_lde(rep, max_p, nper, log_qd, log_h, shift, plde);
+                free(rep);
+            }
+            or_ef *rand_ef = (or_ef *)malloc((A->num_randomness + 1) * sizeof(or_ef));
+            or_ef *auxv_ef = (or_ef *)malloc((A->num_aux_values + 1) * sizeof(or_ef));
+            for (size_t r = 0; r < A->num_randomness; r++) rand_ef[r] = or_ef_make(rnd[2 * r], rnd[2 * r + 1]);
+            for (size_t r = 0; r < A->num_aux_values; r++) auxv_ef[r] = or_ef_make(auxv[ii][2 * r], auxv[ii][2 * r + 1]);
+#pragma omp parallel
+            {
+                or_ef *ml = (or_ef *)malloc((w + 1) * sizeof(or_ef)), *mn = (or_ef *)malloc((w + 1) * sizeof(or_ef));
+                or_ef *al = (or_ef *)malloc((aux_w + 1) * sizeof(or_ef)), *an = (or_ef *)malloc((aux_w + 1) * sizeof(or_ef));
+                or_ef *per = (or_ef *)malloc((nper + 1) * sizeof(or_ef));
+                or_ef *nodes = (or_ef *)malloc((A->n_nodes + 1) * sizeof(or_ef));
+                or_ef *cons = (or_ef *)malloc((K + 1) * sizeof(or_ef));
+#pragma omp for schedule(static)
+                for (size_t m = 0; m < qh; m++) {
+                    uint64_t x = or_mul(shift, or_pow(omega_q, m));
+                    uint64_t zh = or_sub(or_exp2(x, log_h), 1);
+                    or_sym_point pt;
+                    pt.sel[0] = or_ef_from(or_mul(zh, or_inv(or_sub(x, 1))));
+                    pt.sel[1] = or_ef_from(or_mul(zh, or_inv(or_sub(x, omega_h_inv))));
+                    pt.sel[2] = or_ef_from(or_sub(x, omega_h_inv));
+                    size_t rl = or_bitrev(m, log_qh), rn = or_bitrev((m + D) % qh, log_qh);
+                    for (size_t c = 0; c < w; c++) ml[c] = or_ef_from(lde[rl * w + c]), mn[c] = or_ef_from(lde[rn * w + c]);
+                    for (size_t c = 0; c < aux_w; c++) {
+                        al[c] = or_ef_make(alde[rl * 2 * aux_w + 2 * c], alde[rl * 2 * aux_w + 2 * c + 1]);
+                        an[c] = or_ef_make(alde[rn * 2 * aux_w + 2 * c], alde[rn * 2 * aux_w + 2 * c + 1]);
+                    }
+                    for (size_t c = 0; c < nper; c++) per[c] = or_ef_from(plde[(m % ph) * nper + c]);
+                    pt.main_local = ml, pt.main_next = mn, pt.aux_local = al, pt.aux_next = an;
+                    pt.pub = I->public_values, pt.rand = rand_ef, pt.auxv = auxv_ef, pt.periodic = per;
+                    or_sym_eval(A, &pt, nodes, cons);
+                    or_ef f = or_ef_from(0);
+                    for (size_t k = 0; k < K; k++) f = or_ef_add(or_ef_mul(f, alpha), cons[k]);
+                    acc[m] = or_ef_add(acc[m], f);
+                }
+                free(ml), free(mn), free(al), free(an), free(per), free(nodes), free(cons);
+            }
+            free(plde), free(rand_ef), free(auxv_ef);
+            continue;
+        }
 #pragma omp parallel
         {
             uint64_t *cons = (uint64_t *)malloc(K * 8);
@@ -192,6 +284,8 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
             free(cons);
         }
     }
+    for (size_t i = 0; i < n_inst; i++) free(auxv[i]);
+    free(rnd);
     /* 6. divide by Z_H on the max quotient coset (quotient.rs:380-409) */
     {
         uint64_t s_pow_n = or_exp2(OR_GEN, log_max_h);

@@ -178,9 +178,12 @@ int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instanc
     const unsigned lb = pcs->log_blowup;
     const unsigned log_max_h = or_log2(inst[n_inst - 1].height);
     unsigned log_qd = 0;
+    size_t n_rand = 0;
     for (size_t i = 0; i < n_inst; i++) {
-        unsigned d = or_air_log_quotient_degree(inst[i].air);
+        if (inst[i].air == OR_AIR_SYMBOLIC && (!inst[i].sym || or_sym_validate(inst[i].sym))) return OR_VERR_SHAPE;
+        unsigned d = or_inst_log_qd(&inst[i]);
         if (d > log_qd) log_qd = d;
+        if (or_inst_num_randomness(&inst[i]) > n_rand) n_rand = or_inst_num_randomness(&inst[i]);
     }
     if (log_qd > lb) return OR_VERR_SHAPE;
     const size_t D = (size_t)1 << log_qd;
@@ -189,8 +192,14 @@ int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instanc
     /* 1.-5. commitments and challenges in prover order */
     uint64_t main_c[4], aux_c[4], quot_c[4];
     v_commit(&v, main_c, 1);
-    (void)or_ch_sample_ef(&v.ch); /* aux randomness (max num_randomness = 1) */
+    or_ef rnd[64];
+    for (size_t r = 0; r < n_rand && r < 64; r++) rnd[r] = or_ch_sample_ef(&v.ch); /* aux randomness */
     v_commit(&v, aux_c, 1);
+    /* aux values per instance (verifier/mod.rs:230-239) */
+    size_t n_auxv = 0;
+    for (size_t i = 0; i < n_inst; i++) n_auxv += or_inst_num_aux_values(&inst[i]);
+    or_ef *auxv = (or_ef *)malloc((n_auxv + 1) * sizeof(or_ef));
+    for (size_t k = 0; k < n_auxv; k++) auxv[k] = v_ef(&v);
     or_ef alpha = or_ch_sample_ef(&v.ch);
     or_ef beta = or_ch_sample_ef(&v.ch);
     v_commit(&v, quot_c, 1);
@@ -209,7 +218,7 @@ int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instanc
     size_t n_mats = 2 * n_inst + 1, aw[17], ow[17], grp_first[4] = {0, n_inst, 2 * n_inst, 2 * n_inst + 1};
     for (size_t i = 0; i < n_inst; i++) {
         ow[i] = inst[i].width;
-        ow[n_inst + i] = 2;
+        ow[n_inst + i] = 2 * or_inst_aux_width(&inst[i]);
     }
     ow[2 * n_inst] = 2 * D;
     size_t total_aligned = 0;
@@ -336,8 +345,48 @@ int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instanc
     /* 10. constraints at z (local) and z * w (next) per instance, beta accumulation */
     or_ef accumulated = or_ef_from(0);
     if (!err) {
-        size_t off = 0;
+        size_t off = 0, aux_off = 0, auxv_off = 0;
+        for (size_t m = 0; m < n_inst; m++) aux_off += aw[m];
         for (size_t i = 0; i < n_inst; i++) {
+            if (inst[i].air == OR_AIR_SYMBOLIC) {
+                /* ConstraintFolder over the DAG at z (verifier/mod.rs:286-339) */
+                const or_sym_air *A = inst[i].sym;
+                const size_t w = inst[i].width, awi = A->aux_width;
+                const unsigned log_h = or_log2(inst[i].height), lift = log_max_h - log_h;
+                or_ef *ml = (or_ef *)malloc((w + 1) * sizeof(or_ef)), *mn = (or_ef *)malloc((w + 1) * sizeof(or_ef));
+                or_ef *al = (or_ef *)malloc((awi + 1) * sizeof(or_ef)), *an = (or_ef *)malloc((awi + 1) * sizeof(or_ef));
+                or_ef *per = (or_ef *)malloc((A->num_periodic + 1) * sizeof(or_ef));
+                or_ef *nodes = (or_ef *)malloc((A->n_nodes + 1) * sizeof(or_ef));
+                or_ef *cons = (or_ef *)malloc((A->n_constraints + 1) * sizeof(or_ef));
+                for (size_t c = 0; c < w; c++) ml[c] = evals[off + c], mn[c] = evals[total_aligned + off + c];
+                /* aux EF column c = its two base coordinates (row_to_packed_ext) */
+                const or_ef X = or_ef_make(0, 1);
+                for (size_t c = 0; c < awi; c++) {
+                    al[c] = or_ef_add(evals[aux_off + 2 * c], or_ef_mul(X, evals[aux_off + 2 * c + 1]));
+                    an[c] = or_ef_add(evals[total_aligned + aux_off + 2 * c],
+                                      or_ef_mul(X, evals[total_aligned + aux_off + 2 * c + 1]));
+                }
+                or_sym_periodic_at(A, inst[n_inst - 1].height, z, per);
+                or_ef zl = or_ef_exp2(z, lift);
+                or_ef van = or_ef_sub(or_ef_exp2(zl, log_h), or_ef_from(1));
+                uint64_t oinv = or_inv(or_root(log_h));
+                or_sym_point pt;
+                pt.sel[0] = or_ef_mul(van, or_ef_inv(or_ef_sub(zl, or_ef_from(1))));
+                pt.sel[1] = or_ef_mul(van, or_ef_inv(or_ef_sub(zl, or_ef_from(oinv))));
+                pt.sel[2] = or_ef_sub(zl, or_ef_from(oinv));
+                pt.main_local = ml, pt.main_next = mn, pt.aux_local = al, pt.aux_next = an;
+                pt.pub = inst[i].public_values, pt.rand = rnd, pt.auxv = auxv + auxv_off, pt.periodic = per;
+                or_sym_eval(A, &pt, nodes, cons);
+                or_ef folded = or_ef_from(0);
+                for (size_t k = 0; k < A->n_constraints; k++) folded = or_ef_add(or_ef_mul(folded, alpha), cons[k]);
+                accumulated = or_ef_add(or_ef_mul(accumulated, beta), folded);
+                free(ml), free(mn), free(al), free(an), free(per), free(nodes), free(cons);
+                off += aw[i];
+                aux_off += aw[n_inst + i];
+                auxv_off += A->num_aux_values;
+                continue;
+            }
+            aux_off += aw[n_inst + i];
             const size_t w = inst[i].width;
             const unsigned log_h = or_log2(inst[i].height), lift = log_max_h - log_h;
             or_ef *L = (or_ef *)malloc(w * sizeof(or_ef)), *N = (or_ef *)malloc(w * sizeof(or_ef));
@@ -383,6 +432,7 @@ int or_verify(const or_p2_params *pp, const or_pcs_params *pcs, const or_instanc
         if (!or_ef_eq(accumulated, or_ef_mul(qz, vanish))) err = OR_VERR_QUOTIENT;
     }
     free(evals);
+    free(auxv);
     if (!err && v.short_read) err = OR_VERR_TRANSCRIPT;
     /* 13. transcript fully consumed, digest */
     if (!err && (v.pf != v.nf || v.pc != v.nc)) err = OR_VERR_TRANSCRIPT;

@@ -124,17 +124,73 @@ void or_keccak_inputs(uint64_t seed, size_t n_perms, uint64_t *out25);
 /* debug check: returns index of first failing (row*K + constraint) + 1, or 0 */
 size_t or_check_constraints(int air, size_t height, size_t width, const uint64_t *consts, const uint64_t *trace);
 
+/* ------------------------------------------------------- symbolic AIRs
+ * (or_sym.c) constraint DAGs from p3-air's SymbolicAirBuilder */
+enum {
+    OR_SYM_CONST = 0,         /* value */
+    OR_SYM_MAIN = 1,          /* main column a, row offset b (0 local, 1 next) */
+    OR_SYM_AUX = 2,           /* aux EF column a, row offset b */
+    OR_SYM_PUBLIC = 3,        /* public value a */
+    OR_SYM_RANDOMNESS = 4,    /* aux randomness a (EF) */
+    OR_SYM_AUX_VALUE = 5,     /* aux value a (EF) */
+    OR_SYM_PERIODIC = 6,      /* periodic column a */
+    OR_SYM_IS_FIRST_ROW = 7,
+    OR_SYM_IS_LAST_ROW = 8,
+    OR_SYM_IS_TRANSITION = 9,
+    OR_SYM_ADD = 10,
+    OR_SYM_SUB = 11,
+    OR_SYM_MUL = 12,
+    OR_SYM_NEG = 13
+};
+typedef struct {
+    uint32_t op, a, b, pad;
+    uint64_t value;
+} or_sym_node;
+typedef struct {
+    uint32_t main_width, aux_width, num_randomness, num_aux_values, num_public_values, num_periodic;
+    const uint64_t *periodic_lengths; /* num_periodic powers of two */
+    const uint64_t *periodic_values;  /* the columns, concatenated */
+    const or_sym_node *nodes;
+    size_t n_nodes;
+    const uint32_t *constraints; /* node per constraint, emission order */
+    const uint8_t *is_ext;       /* assert_zero_ext (1) or assert_zero (0) */
+    size_t n_constraints;
+} or_sym_air;
+typedef struct {
+    const or_ef *main_local, *main_next, *aux_local, *aux_next;
+    const uint64_t *pub;
+    const or_ef *rand, *auxv, *periodic;
+    or_ef sel[3]; /* is_first_row, is_last_row, is_transition */
+} or_sym_point;
+int or_sym_validate(const or_sym_air *a);
+unsigned or_sym_max_degree(const or_sym_air *a);
+unsigned or_sym_log_quotient_degree(const or_sym_air *a);
+void or_sym_eval(const or_sym_air *a, const or_sym_point *pt, or_ef *scratch_nodes, or_ef *out_constraints);
+uint64_t *or_sym_periodic_matrix(const or_sym_air *a, size_t *max_p);
+void or_sym_periodic_at(const or_sym_air *a, size_t max_trace_height, or_ef z, or_ef *out);
+
 /* --------------------------------------------------------------- prover */
 typedef struct {
     unsigned log_blowup, log_folding_arity, log_final_degree;
     unsigned folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
 } or_pcs_params;
 
+/* AuxBuilder::build_aux_trace (p3-miden-lifted-air/src/auxiliary/builder.rs:16-37):
+ * writes the aux trace (height x aux_width EF, 2 words each, row-major) and
+ * num_aux_values EF values; 0 = success. */
+typedef int (*or_aux_fn)(void *user, uint64_t instance, const uint64_t *main_trace, const uint64_t *randomness,
+                         uint64_t n_randomness, uint64_t height, uint64_t *aux_out, uint64_t *aux_values_out);
+
+enum { OR_AIR_SYMBOLIC = 3 };
 typedef struct {
     int air;
     size_t height, width;
     const uint64_t *trace;  /* row-major height x width */
     const uint64_t *consts; /* AIR constants (cubic: k[width]) */
+    const or_sym_air *sym;  /* OR_AIR_SYMBOLIC */
+    const uint64_t *public_values;
+    or_aux_fn aux_build;    /* NULL: the all-zero aux trace */
+    void *aux_user;
 } or_instance;
 
 typedef struct {
@@ -151,6 +207,11 @@ typedef struct {
 
 int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
              or_proof *out);
+size_t or_inst_aux_width(const or_instance *I);
+size_t or_inst_num_randomness(const or_instance *I);
+size_t or_inst_num_aux_values(const or_instance *I);
+unsigned or_inst_log_qd(const or_instance *I);
+size_t or_inst_num_constraints(const or_instance *I);
 void or_proof_free(or_proof *p);
 
 /* --------------------------------------------------------------- verifier */

@@ -17,12 +17,16 @@ from pathlib import Path
 
 import numpy as np
 
+from . import symbolic
+from .symbolic import AirDesc, SymbolicAirBuilder, build_air
+
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libp3miden_b200.so"
 P = 0xFFFFFFFF00000001
 
 AIR_CUBIC = 1
 AIR_KECCAK = 2
+AIR_SYMBOLIC = 3
 KECCAK_NUM_COLS = 2633
 KECCAK_ROWS_PER_HASH = 24
 
@@ -58,10 +62,25 @@ class PcsParamsC(C.Structure):
         "folding_pow_bits", "deep_pow_bits", "num_queries", "query_pow_bits")]
 
 
+# AuxBuilder::build_aux_trace (include/p3g.h, p3g_aux_build_fn)
+AUX_BUILD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64,
+                           C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+
+
 class InstanceC(C.Structure):
     _fields_ = [("air", C.c_int32), ("trace_on_device", C.c_int32),
                 ("height", C.c_uint64), ("width", C.c_uint64),
-                ("trace", u64p), ("consts", u64p), ("n_consts", C.c_uint64)]
+                ("trace", u64p), ("consts", u64p), ("n_consts", C.c_uint64),
+                ("sym", C.c_void_p), ("public_values", u64p), ("n_public_values", C.c_uint64),
+                ("aux_build", AUX_BUILD_FN), ("aux_user", C.c_void_p)]
+
+
+class AirDescC(C.Structure):
+    _fields_ = [("main_width", C.c_uint32), ("aux_width", C.c_uint32), ("num_randomness", C.c_uint32),
+                ("num_aux_values", C.c_uint32), ("num_public_values", C.c_uint32), ("num_periodic", C.c_uint32),
+                ("periodic_lengths", u64p), ("periodic_values", u64p), ("nodes", C.c_void_p),
+                ("n_nodes", C.c_uint64), ("constraints", C.POINTER(C.c_uint32)), ("is_ext", C.POINTER(C.c_uint8)),
+                ("n_constraints", C.c_uint64)]
 
 
 class ProofC(C.Structure):
@@ -127,6 +146,17 @@ def lib():
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
             "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
                                            C.POINTER(VerifyStatsC)]),
+            "p3g_air_analyse": (C.c_int, [C.POINTER(AirDescC), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                          C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+            "p3g_air_generate_source": (C.c_int, [C.POINTER(AirDescC), C.c_char_p, C.c_uint64,
+                                                  C.POINTER(C.c_uint64)]),
+            "p3g_air_create": (C.c_int, [vp, C.POINTER(AirDescC), C.POINTER(vp)]),
+            "p3g_air_compile_check": (C.c_int, [C.POINTER(AirDescC), C.c_int32, C.POINTER(C.c_uint64)]),
+            "p3g_air_log_quotient_degree": (C.c_uint32, [vp]),
+            "p3g_air_max_degree": (C.c_uint32, [vp]),
+            "p3g_air_num_constraints_of": (C.c_uint64, [vp]),
+            "p3g_air_layout": (C.c_int, [vp, u64p, C.POINTER(C.c_uint64), u64p, C.POINTER(C.c_uint64)]),
+            "p3g_air_free": (None, [vp]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -335,13 +365,145 @@ class PcsParams:
                           self.folding_pow_bits, self.deep_pow_bits, self.num_queries, self.query_pow_bits)
 
 
+def _desc_c(desc, keep) -> AirDescC:
+    """p3g_air_desc of a symbolic.AirDesc (arrays kept alive in `keep`)."""
+    nodes = np.ascontiguousarray(desc.nodes, dtype=symbolic.NODE_DTYPE)
+    cons = np.ascontiguousarray(desc.constraints, dtype=np.uint32)
+    ext = np.ascontiguousarray(desc.is_ext, dtype=np.uint8)
+    pl = np.ascontiguousarray(desc.periodic_lengths, dtype=np.uint64)
+    pv = np.ascontiguousarray(desc.periodic_values, dtype=np.uint64)
+    keep += [nodes, cons, ext, pl, pv]
+    return AirDescC(desc.width, desc.aux_width, desc.num_randomness, desc.num_aux_values, desc.num_public_values,
+                    desc.num_periodic, _ptr(pl) if pl.size else None, _ptr(pv) if pv.size else None,
+                    nodes.ctypes.data if nodes.size else None, nodes.size,
+                    cons.ctypes.data_as(C.POINTER(C.c_uint32)) if cons.size else None,
+                    ext.ctypes.data_as(C.POINTER(C.c_uint8)) if ext.size else None, cons.size)
+
+
+def air_analyse(desc) -> dict:
+    """Degree analysis of a symbolic AIR without a device: the maximal
+    degree multiple, log_quotient_degree (air.rs:225-247) and the numbers of
+    base and extension constraints (ConstraintLayout)."""
+    keep = []
+    d = _desc_c(desc, keep)
+    md, lq, nb, ne = C.c_uint32(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+    _check(lib().p3g_air_analyse(C.byref(d), C.byref(md), C.byref(lq), C.byref(nb), C.byref(ne)))
+    return {"max_degree": md.value, "log_quotient_degree": lq.value, "n_base": nb.value, "n_ext": ne.value}
+
+
+def air_source(desc) -> str:
+    """The CUDA source the library generates for this AIR's constraint kernel."""
+    keep = []
+    d = _desc_c(desc, keep)
+    n = C.c_uint64()
+    lib().p3g_air_generate_source(C.byref(d), None, 0, C.byref(n))
+    buf = C.create_string_buffer(n.value)
+    _check(lib().p3g_air_generate_source(C.byref(d), buf, n.value, C.byref(n)))
+    return buf.value.decode()
+
+
+def air_compile_check(desc, cc: int = 100) -> int:
+    """Generate this AIR's constraint kernel and compile it with NVRTC for
+    sm_<cc>a without a device; returns the cubin size."""
+    keep = []
+    d = _desc_c(desc, keep)
+    n = C.c_uint64()
+    _check(lib().p3g_air_compile_check(C.byref(d), cc, C.byref(n)))
+    return n.value
+
+
+class Air:
+    """A symbolic AIR compiled for one device (p3g_air_create): the DAG of a
+    symbolic.AirDesc, its degree analysis and its generated constraint
+    kernel."""
+
+    def __init__(self, ctx: "Context", desc):
+        self.desc = desc
+        keep = []
+        d = _desc_c(desc, keep)
+        self._h = C.c_void_p()
+        ctx.check(lib().p3g_air_create(ctx.handle, C.byref(d), C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def log_quotient_degree(self) -> int:
+        return int(lib().p3g_air_log_quotient_degree(self._h))
+
+    @property
+    def max_degree(self) -> int:
+        return int(lib().p3g_air_max_degree(self._h))
+
+    def layout(self):
+        """ConstraintLayout: (base_indices, ext_indices) in emission order."""
+        nb, ne = C.c_uint64(self.desc.num_constraints), C.c_uint64(self.desc.num_constraints)
+        b = np.zeros(max(1, nb.value), dtype=np.uint64)
+        e = np.zeros(max(1, ne.value), dtype=np.uint64)
+        _check(lib().p3g_air_layout(self._h, _ptr(b), C.byref(nb), _ptr(e), C.byref(ne)))
+        return b[:nb.value].copy(), e[:ne.value].copy()
+
+    def close(self):
+        if self._h:
+            lib().p3g_air_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def aux_builder_c(fn):
+    """Wrap fn(instance, randomness, height) -> (aux, aux_values) as the
+    C callback (AuxBuilder::build_aux_trace): randomness is a list of
+    (c0, c1) extension elements; aux is height x (2 * aux_width) words (each
+    EF column as its two coordinates), aux_values 2 words per value."""
+    def cb(user, instance, main_trace, rnd, n_rnd, height, aux_out, vals_out):
+        try:
+            r = [(int(rnd[2 * i]), int(rnd[2 * i + 1])) for i in range(n_rnd)]
+            aux, vals = fn(int(instance), r, int(height))
+            aux = np.ascontiguousarray(aux, dtype=np.uint64).reshape(-1)
+            vals = np.ascontiguousarray(vals, dtype=np.uint64).reshape(-1)
+            C.memmove(aux_out, aux.ctypes.data, aux.nbytes)
+            if vals.size:
+                C.memmove(vals_out, vals.ctypes.data, vals.nbytes)
+            return 0
+        except Exception:
+            return 1
+    return AUX_BUILD_FN(cb)
+
+
 @dataclass
 class AirWitness:
-    """One instance: AIR id, row-major trace (numpy host array or torch CUDA
-    tensor of int64 bit patterns) and the AIR's constants (cubic: k[w])."""
-    air: int
+    """One instance: the AIR (a built-in id, or an Air for a symbolic AIR),
+    the row-major trace (numpy host array or torch CUDA tensor of int64 bit
+    patterns), the AIR's constants (cubic: k[w]), its public values and its
+    AuxBuilder, fn(instance, randomness, height) -> (aux, aux_values)
+    (None: the all-zero aux trace)."""
+    air: object
     trace: object
     consts: np.ndarray | None = None
+    public_values: np.ndarray | None = None
+    aux_builder: object = None
+
+
+def _instance_c(air, height, width, trace_ptr, on_dev, consts, public_values, aux_builder, keep) -> InstanceC:
+    c = np.ascontiguousarray(consts if consts is not None else np.zeros(0), dtype=np.uint64)
+    pv = np.ascontiguousarray(public_values if public_values is not None else np.zeros(0), dtype=np.uint64)
+    keep += [c, pv]
+    sym = None
+    if isinstance(air, Air):
+        sym, air = air.handle, AIR_SYMBOLIC
+    cb = AUX_BUILD_FN()
+    if aux_builder is not None:
+        cb = aux_builder_c(aux_builder)
+        keep.append(cb)
+    return InstanceC(air, on_dev, height, width, C.cast(C.c_void_p(trace_ptr), u64p) if trace_ptr else None,
+                     c.ctypes.data_as(u64p) if c.size else None, c.size, sym,
+                     pv.ctypes.data_as(u64p) if pv.size else None, pv.size, cb, None)
 
 
 @dataclass
@@ -422,10 +584,7 @@ def prove_multi(ctx: Context, pcs: PcsParams, instances: list[AirWitness]) -> St
             keep.append(t)
             ptr, on_dev = t.data_ptr(), int(t.is_cuda)
             h, wd = t.shape
-        c = np.ascontiguousarray(w.consts if w.consts is not None else np.zeros(0), dtype=np.uint64)
-        keep.append(c)
-        arr[i] = InstanceC(w.air, on_dev, h, wd, C.cast(C.c_void_p(ptr), u64p),
-                           c.ctypes.data_as(u64p) if c.size else None, c.size)
+        arr[i] = _instance_c(w.air, h, wd, ptr, on_dev, w.consts, w.public_values, w.aux_builder, keep)
     if any(not isinstance(w.trace, np.ndarray) and w.trace.is_cuda for w in instances):
         import torch
         torch.cuda.synchronize(ctx.device)
@@ -455,12 +614,14 @@ VERDICTS = ("accept", "shape", "opening", "root", "pow", "deep", "fri", "final",
 
 @dataclass
 class AirShape:
-    """The verifier's view of one instance: AIR id, trace height and width,
-    and the AIR's constants (cubic: k[w])."""
-    air: int
+    """The verifier's view of one instance: the AIR (built-in id or Air),
+    trace height and width, the AIR's constants (cubic: k[w]) and its public
+    values."""
+    air: object
     height: int
     width: int
     consts: np.ndarray | None = None
+    public_values: np.ndarray | None = None
 
 
 @dataclass
@@ -489,9 +650,7 @@ def verify_multi(ctx: Context, pcs: PcsParams, shapes: list[AirShape], fields: n
     arr = (InstanceC * max(1, n))()
     keep = []
     for i, sh in enumerate(shapes):
-        c = np.ascontiguousarray(sh.consts if sh.consts is not None else np.zeros(0), dtype=np.uint64)
-        keep.append(c)
-        arr[i] = InstanceC(sh.air, 0, sh.height, sh.width, None, c.ctypes.data_as(u64p) if c.size else None, c.size)
+        arr[i] = _instance_c(sh.air, sh.height, sh.width, 0, 0, sh.consts, sh.public_values, None, keep)
     f = np.ascontiguousarray(fields, dtype=np.uint64).reshape(-1)
     cm = np.ascontiguousarray(commitments, dtype=np.uint64).reshape(-1)
     dg = np.ascontiguousarray(digest, dtype=np.uint64).reshape(-1)
@@ -519,10 +678,7 @@ def verify_batch(ctx: Context, items, host_threads: int = 0) -> tuple[list[int],
     for i, (pcs, shapes, fields, commits, digest) in enumerate(items):
         arr = (InstanceC * max(1, len(shapes)))()
         for k, sh in enumerate(shapes):
-            c = np.ascontiguousarray(sh.consts if sh.consts is not None else np.zeros(0), dtype=np.uint64)
-            keep.append(c)
-            arr[k] = InstanceC(sh.air, 0, sh.height, sh.width, None, c.ctypes.data_as(u64p) if c.size else None,
-                               c.size)
+            arr[k] = _instance_c(sh.air, sh.height, sh.width, 0, 0, sh.consts, sh.public_values, None, keep)
         f = np.ascontiguousarray(fields, dtype=np.uint64).reshape(-1)
         cm = np.ascontiguousarray(commits, dtype=np.uint64).reshape(-1)
         dg = np.ascontiguousarray(digest, dtype=np.uint64).reshape(-1)
@@ -622,10 +778,7 @@ def _instances_c(instances, keep):
             ptr, on_dev = t.data_ptr(), int(t.is_cuda)
         keep.append(t)
         h, wd = t.shape
-        c = np.ascontiguousarray(w.consts if w.consts is not None else np.zeros(0), dtype=np.uint64)
-        keep.append(c)
-        arr[i] = InstanceC(w.air, on_dev, h, wd, C.cast(C.c_void_p(ptr), u64p),
-                           c.ctypes.data_as(u64p) if c.size else None, c.size)
+        arr[i] = _instance_c(w.air, h, wd, ptr, on_dev, w.consts, w.public_values, w.aux_builder, keep)
     keep.append(arr)
     return arr
 

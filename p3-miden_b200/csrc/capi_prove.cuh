@@ -12,6 +12,9 @@ struct p3g_pcs_params_c {
     uint32_t log_blowup, log_folding_arity, log_final_degree;
     uint32_t folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
 };
+struct p3g_air {
+    sym::Air a;
+};
 struct p3g_instance_c {
     int32_t air;
     int32_t trace_on_device;
@@ -19,6 +22,11 @@ struct p3g_instance_c {
     const uint64_t *trace;
     const uint64_t *consts;
     uint64_t n_consts;
+    const p3g_air *sym;
+    const uint64_t *public_values;
+    uint64_t n_public_values;
+    p3g::AuxFn aux_build;
+    void *aux_user;
 };
 struct p3g_proof_c {
     uint64_t *fields;
@@ -54,6 +62,34 @@ inline void upload_keccak_tables() {
     CK(cudaMemcpyToSymbol(tgen::c_rot, rot, sizeof(rot)));
 }
 
+inline Instance to_instance(const p3g_instance_c &I) {
+    Instance r{I.air, I.trace_on_device, I.height, I.width, I.trace, I.consts, I.n_consts};
+    r.sym = I.sym ? &I.sym->a : nullptr;
+    r.pub = I.public_values;
+    r.n_pub = I.n_public_values;
+    r.aux_build = I.aux_build;
+    r.aux_user = I.aux_user;
+    return r;
+}
+// The AIR-specific shape checks (width, constants, public values): the
+// WidthMismatch / public-values checks of AirWitness and AirInstance
+// (p3-miden-lifted-air/src/instance.rs:93-115).
+inline int validate_air(const p3g_instance_c &I) {
+    if (I.air == AIR_KECCAK) {
+        if (I.width != (uint64_t)keccak::NCOLS) return ERR_VALIDATION;
+    } else if (I.air == AIR_CUBIC) {
+        if (I.width == 0 || !I.consts || I.n_consts != I.width) return ERR_VALIDATION;
+    } else if (I.air == AIR_SYMBOLIC) {
+        if (!I.sym) return ERR_INVALID;
+        const sym::Desc &d = I.sym->a.d;
+        if (I.width != d.main_width) return ERR_VALIDATION;
+        if (I.n_public_values != d.num_public_values || (d.num_public_values && !I.public_values))
+            return ERR_VALIDATION;
+    } else {
+        return ERR_VALIDATION;
+    }
+    return OK;
+}
 // Validation mirroring prove_multi's checks (prover/mod.rs:238-264,
 // p3-miden-lifted-air/src/instance.rs:93-115) and PcsParams::new
 // (p3-miden-lifted-fri/src/params.rs:170-204).
@@ -70,18 +106,13 @@ inline int validate(const p3g_pcs_params_c *pcs, const p3g_instance_c *inst, uin
         if (I.height == 0 || (I.height & (I.height - 1))) return ERR_VALIDATION;
         if (I.height < prev) return ERR_VALIDATION;  // not ascending
         prev = I.height;
-        if (I.air == AIR_KECCAK) {
-            if (I.width != (uint64_t)keccak::NCOLS) return ERR_VALIDATION;
-        } else if (I.air == AIR_CUBIC) {
-            if (I.width == 0 || !I.consts || I.n_consts != I.width) return ERR_VALIDATION;
-        } else {
-            return ERR_VALIDATION;
-        }
+        if (int v = validate_air(I)) return v;
     }
     if (prev < 2) return ERR_VALIDATION;  // max trace height must be >= 2
     uint32_t log_qd = 0;
-    for (uint64_t i = 0; i < n; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
+    for (uint64_t i = 0; i < n; i++) log_qd = std::max(log_qd, inst_log_qd(to_instance(inst[i])));
     if (log_qd > pcs->log_blowup) return ERR_VALIDATION;  // ConstraintDegreeTooHigh
+    if (log_qd > 3) return ERR_VALIDATION;  // this library's bound: at most 8 quotient chunks (degree <= 9)
     if (log2u(prev) + pcs->log_blowup > 32) return ERR_INVALID;  // two-adicity of Goldilocks
     return OK;
 }
@@ -101,9 +132,7 @@ P3G_API int p3g_prove(p3g_ctx *x, const p3g_pcs_params_c *pcs, const p3g_instanc
         p3g::bind_p2(x->c);
         p3g::ensure_keccak_tables(x->c.device);
         std::vector<p3g::Instance> ins(n);
-        for (uint64_t i = 0; i < n; i++)
-            ins[i] = {inst[i].air, inst[i].trace_on_device, inst[i].height, inst[i].width, inst[i].trace, inst[i].consts,
-                      inst[i].n_consts};
+        for (uint64_t i = 0; i < n; i++) ins[i] = p3g::to_instance(inst[i]);
         p3g::PcsParams pp{pcs->log_blowup,     pcs->log_folding_arity, pcs->log_final_degree, pcs->folding_pow_bits,
                           pcs->deep_pow_bits,  pcs->num_queries,       pcs->query_pow_bits};
         p3g::ProofOut po;
@@ -298,3 +327,133 @@ P3G_API int p3g_lmcs_prove_batch(p3g_ctx *x, const p3g_tree *t, const uint64_t *
         *n_commits = oc;
     })
 }
+
+// ------------------------------------------------------------ symbolic AIRs
+struct p3g_sym_node_c {
+    uint32_t op, a, b, pad;
+    uint64_t value;
+};
+struct p3g_air_desc_c {
+    uint32_t main_width, aux_width, num_randomness, num_aux_values, num_public_values, num_periodic;
+    const uint64_t *periodic_lengths;
+    const uint64_t *periodic_values;
+    const p3g_sym_node_c *nodes;
+    uint64_t n_nodes;
+    const uint32_t *constraints;
+    const uint8_t *is_ext;
+    uint64_t n_constraints;
+};
+namespace p3g {
+inline int desc_from_c(const p3g_air_desc_c *c, sym::Desc &d, std::string &why) {
+    if (!c || (c->n_nodes && !c->nodes) || (c->n_constraints && (!c->constraints || !c->is_ext)) ||
+        (c->num_periodic && (!c->periodic_lengths || !c->periodic_values)) || c->n_nodes > (1ull << 24) ||
+        c->n_constraints > (1ull << 24) || c->num_periodic > 4096)
+        return ERR_INVALID;
+    d.main_width = c->main_width, d.aux_width = c->aux_width, d.num_randomness = c->num_randomness;
+    d.num_aux_values = c->num_aux_values, d.num_public_values = c->num_public_values, d.num_periodic = c->num_periodic;
+    d.periodic_lengths.assign(c->periodic_lengths, c->periodic_lengths + c->num_periodic);
+    uint64_t total = 0;
+    for (uint64_t p : d.periodic_lengths) {
+        if (p > (1ull << 30)) return ERR_INVALID;
+        total += p;
+    }
+    d.periodic_values.assign(c->periodic_values, c->periodic_values + total);
+    d.nodes.resize(c->n_nodes);
+    if (c->n_nodes) memcpy(d.nodes.data(), c->nodes, c->n_nodes * sizeof(sym::Node));
+    d.constraints.assign(c->constraints, c->constraints + c->n_constraints);
+    d.is_ext.assign(c->is_ext, c->is_ext + c->n_constraints);
+    if (const char *e = sym::validate(d)) {
+        why = e;
+        return ERR_VALIDATION;
+    }
+    return OK;
+}
+}  // namespace p3g
+
+// The analysis alone (no device, no compilation): degree and layout.
+P3G_API int p3g_air_analyse(const p3g_air_desc_c *desc, uint32_t *max_degree, uint32_t *log_quotient_degree,
+                            uint64_t *n_base, uint64_t *n_ext) {
+    sym::Air A;
+    std::string why;
+    if (int v = p3g::desc_from_c(desc, A.d, why)) return v;
+    sym::analyse(A);
+    if (max_degree) *max_degree = A.max_degree;
+    if (log_quotient_degree) *log_quotient_degree = A.log_qd;
+    if (n_base) *n_base = A.base_idx.size();
+    if (n_ext) *n_ext = A.ext_idx.size();
+    return p3g::OK;
+}
+
+// The generated kernel source of an AIR (no device needed); *len = its size
+// plus the terminating zero, P3G_ERR_INVALID when cap is smaller.
+P3G_API int p3g_air_generate_source(const p3g_air_desc_c *desc, char *buf, uint64_t cap, uint64_t *len) {
+    if (!len) return p3g::ERR_INVALID;
+    sym::Air A;
+    std::string why;
+    if (int v = p3g::desc_from_c(desc, A.d, why)) return v;
+    sym::analyse(A);
+    const std::string src = sym::generate(A);
+    *len = src.size() + 1;
+    if (!buf || cap < *len) return p3g::ERR_INVALID;
+    memcpy(buf, src.c_str(), src.size() + 1);
+    return p3g::OK;
+}
+
+// Generate and compile (NVRTC, sm_<cc>) without a device: 0 when the
+// kernel compiles; *cubin_bytes receives its size.
+P3G_API int p3g_air_compile_check(const p3g_air_desc_c *desc, int32_t cc, uint64_t *cubin_bytes) {
+    sym::Air A;
+    std::string why;
+    if (int v = p3g::desc_from_c(desc, A.d, why)) return v;
+    try {
+        sym::analyse(A);
+        A.source = sym::generate(A);
+        sym::nvrtc_cubin(A.source, cc, A.cubin, A.log);
+    } catch (const p3g::CudaError &e) {
+        return e.status;
+    }
+    if (cubin_bytes) *cubin_bytes = A.cubin.size();
+    return p3g::OK;
+}
+
+P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_air **out) {
+    if (!x || !out) return p3g::ERR_INVALID;
+    *out = nullptr;
+    p3g_air *a = new p3g_air();
+    std::string why;
+    if (int v = p3g::desc_from_c(desc, a->a.d, why)) {
+        x->c.last_error = "symbolic AIR rejected: " + why;
+        delete a;
+        return v;
+    }
+    try {
+        CK(cudaSetDevice(x->c.device));
+        sym::analyse(a->a);
+        a->a.source = sym::generate(a->a);
+        sym::compile(a->a, x->c.device);
+    } catch (const p3g::CudaError &e) {
+        x->c.last_error = e.what;
+        delete a;
+        return e.status;
+    }
+    *out = a;
+    return p3g::OK;
+}
+P3G_API uint32_t p3g_air_log_quotient_degree(const p3g_air *a) { return a ? a->a.log_qd : 0; }
+P3G_API uint32_t p3g_air_max_degree(const p3g_air *a) { return a ? a->a.max_degree : 0; }
+P3G_API uint64_t p3g_air_num_constraints_of(const p3g_air *a) { return a ? a->a.d.constraints.size() : 0; }
+// ConstraintLayout: base_indices / ext_indices in emission order; *n_base and
+// *n_ext are capacities on entry and counts on return.
+P3G_API int p3g_air_layout(const p3g_air *a, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext) {
+    if (!a || !n_base || !n_ext) return p3g::ERR_INVALID;
+    const uint64_t nb = a->a.base_idx.size(), ne = a->a.ext_idx.size();
+    if ((nb && (!base_idx || *n_base < nb)) || (ne && (!ext_idx || *n_ext < ne))) {
+        *n_base = nb, *n_ext = ne;
+        return p3g::ERR_INVALID;
+    }
+    if (nb) memcpy(base_idx, a->a.base_idx.data(), nb * 8);
+    if (ne) memcpy(ext_idx, a->a.ext_idx.data(), ne * 8);
+    *n_base = nb, *n_ext = ne;
+    return p3g::OK;
+}
+P3G_API void p3g_air_free(p3g_air *a) { delete a; }

@@ -49,7 +49,7 @@ inline std::unique_ptr<ServerJob> make_job(const p3g_job_c &j) {
                          j.pcs.deep_pow_bits, j.pcs.num_queries,       j.pcs.query_pow_bits};
     for (uint64_t i = 0; i < j.n_instances; i++) {
         const p3g_instance_c &I = j.instances[i];
-        job->inst.push_back({I.air, I.trace_on_device, I.height, I.width, I.trace, I.consts, I.n_consts});
+        job->inst.push_back(to_instance(I));
     }
     job->arrival_s = j.arrival_s;
     return job;

@@ -70,16 +70,6 @@ P3G_API int p3g_coset_lde(p3g_ctx *x, const uint64_t *d_in, uint64_t height, uin
     })
 }
 
-namespace p3g {
-// out[r] = in[bitrev(r)] for the rows of an n x w matrix (n = 2^L)
-__global__ void bitrev_rows_kernel(const uint64_t *in, uint64_t *out, uint32_t L, uint64_t w) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >> L >= w) return;
-    const uint64_t r = i / w, c = i % w;
-    out[r * w + c] = in[gl::bitrev(r, L) * w + c];
-}
-}  // namespace p3g
-
 // PeriodicLde::build (p3-miden-lifted-stark/src/prover/periodic.rs:49-81):
 // the periodic columns repeated to the largest period (max_period x width,
 // row-major, on the device) extended on the coset of shift

@@ -29,13 +29,7 @@ inline int verify_args_ok(const p3g_pcs_params_c *pcs, const p3g_instance_c *ins
     for (uint64_t i = 0; i < n; i++) {
         const p3g_instance_c &I = inst[i];
         if (I.height > (1ull << 30)) return ERR_INVALID;
-        if (I.air == AIR_KECCAK) {
-            if (I.width != (uint64_t)keccak::NCOLS) return ERR_VALIDATION;
-        } else if (I.air == AIR_CUBIC) {
-            if (I.width == 0 || !I.consts || I.n_consts != I.width) return ERR_VALIDATION;
-        } else {
-            return ERR_VALIDATION;
-        }
+        if (int v = validate_air(I)) return v;
     }
     if (scan_words && !(words_canonical(fields, n_fields) && words_canonical(commits, 4 * n_commits) &&
                         words_canonical(digest12, 12)))
@@ -45,7 +39,7 @@ inline int verify_args_ok(const p3g_pcs_params_c *pcs, const p3g_instance_c *ins
 inline std::vector<Instance> shapes_of(const p3g_instance_c *inst, uint64_t n) {
     std::vector<Instance> ins(n);
     for (uint64_t i = 0; i < n; i++)
-        ins[i] = {inst[i].air, 0, inst[i].height, inst[i].width, nullptr, inst[i].consts, inst[i].n_consts};
+        ins[i] = to_instance(inst[i]), ins[i].trace_on_device = 0, ins[i].trace = nullptr;
     return ins;
 }
 inline PcsParams pcs_of(const p3g_pcs_params_c *pcs) {

@@ -185,6 +185,14 @@ inline void bind_p2(const Ctx &ctx) {
     b.assign(ctx.p2, ctx.p2 + p2::N_PARAMS);
 }
 
+// out[r] = in[bitrev(r)] for the rows of an n x w matrix (n = 2^L)
+__global__ void bitrev_rows_kernel(const uint64_t *in, uint64_t *out, uint32_t L, uint64_t w) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >> L >= w) return;
+    const uint64_t r = i / w, c = i % w;
+    out[r * w + c] = in[gl::bitrev(r, L) * w + c];
+}
+
 // Host-built two-level power table of v for exponents < 2^L.
 inline void pow_table(uint64_t v, uint32_t L, uint32_t lo_bits, std::vector<uint64_t> &out_lo,
                       std::vector<uint64_t> &out_hi) {

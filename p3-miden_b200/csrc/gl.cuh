@@ -4,7 +4,16 @@
 // All values are kept canonical (< p). Multiplication reduces the 128-bit
 // product with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p).
 #pragma once
+#if defined(__CUDACC_RTC__)
+// compiled at run time by NVRTC as the prelude of generated constraint
+// kernels (symair.cuh): no standard headers there
+typedef unsigned long long uint64_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef int int32_t;
+#else
 #include <cstdint>
+#endif
 
 #if defined(__CUDACC__)
 #define GL_HD __host__ __device__ __forceinline__

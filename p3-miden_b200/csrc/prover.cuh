@@ -10,11 +10,19 @@
 #include "deep.cuh"
 #include "fri.cuh"
 #include "quotient.cuh"
+#include "symair.cuh"
 #include "transcript.cuh"
 
 namespace p3g {
 
-enum Air : int { AIR_CUBIC = 1, AIR_KECCAK = 2 };
+enum Air : int { AIR_CUBIC = 1, AIR_KECCAK = 2, AIR_SYMBOLIC = 3 };
+
+// AuxBuilder::build_aux_trace (p3-miden-lifted-air/src/auxiliary/builder.rs:16-37):
+// writes the instance's aux trace (height x aux_width EF, 2 words each,
+// row-major, host memory the library provides) and its aux values
+// (num_aux_values EF); 0 = success.
+typedef int (*AuxFn)(void *user, uint64_t instance, const uint64_t *main_trace, const uint64_t *randomness,
+                     uint64_t n_randomness, uint64_t height, uint64_t *aux_out, uint64_t *aux_values_out);
 
 struct PcsParams {
     uint32_t log_blowup, log_folding_arity, log_final_degree;
@@ -28,7 +36,19 @@ struct Instance {
     const uint64_t *trace;
     const uint64_t *consts;
     uint64_t n_consts;
+    const sym::Air *sym = nullptr;     // AIR_SYMBOLIC
+    const uint64_t *pub = nullptr;     // AirWitness::public_values
+    uint64_t n_pub = 0;
+    AuxFn aux_build = nullptr;         // null: the all-zero aux trace
+    void *aux_user = nullptr;
 };
+
+// LiftedAir properties. The built-in AIRs declare the examples' dummy aux
+// trace: one EF column, one challenge, no aux values
+// (p3-miden-lifted-examples/src/lib.rs:93-103).
+inline uint64_t inst_aux_width(const Instance &I) { return I.air == AIR_SYMBOLIC ? I.sym->d.aux_width : 1; }
+inline uint64_t inst_num_randomness(const Instance &I) { return I.air == AIR_SYMBOLIC ? I.sym->d.num_randomness : 1; }
+inline uint64_t inst_num_aux_values(const Instance &I) { return I.air == AIR_SYMBOLIC ? I.sym->d.num_aux_values : 0; }
 
 struct ProofOut {
     std::vector<uint64_t> fields, commits;
@@ -42,11 +62,17 @@ inline uint64_t air_num_constraints(int air, uint64_t width) {
     if (air == AIR_KECCAK) return 3182;
     return 0;
 }
-// Both AIRs have maximal constraint degree 3 (is_transition counts 0,
-// is_first_row 1): log2_ceil(3 - 1) = 1 (p3-miden-lifted-air/src/air.rs:267-289).
+// Both built-in AIRs have maximal constraint degree 3 (is_transition counts
+// 0, is_first_row 1): log2_ceil(3 - 1) = 1 (p3-miden-lifted-air/src/air.rs:225-247).
 inline uint32_t air_log_quotient_degree(int air) {
     (void)air;
     return 1;
+}
+inline uint32_t inst_log_qd(const Instance &I) {
+    return I.air == AIR_SYMBOLIC ? I.sym->log_qd : air_log_quotient_degree(I.air);
+}
+inline uint64_t inst_num_constraints(const Instance &I) {
+    return I.air == AIR_SYMBOLIC ? I.sym->d.constraints.size() : air_num_constraints(I.air, I.width);
 }
 
 struct Launcher {
@@ -262,13 +288,78 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
     cudaEventDestroy(ev_leaf[1]);
 }
 
+// Constraint evaluation of a symbolic AIR on gJ with its generated kernel
+// (symair.cuh): one thread per point, acc[m] += sum_k alpha^{K-1-k} C_k(x_m).
+// Periodic columns: PeriodicLde::build on the quotient coset (blowup D,
+// shift (g^{2^lift})^{h / max_period}, natural order; periodic.rs:49-98).
+inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde, const uint64_t *aux_lde,
+                          uint32_t log_h, uint32_t log_qd, uint32_t log_max_h, const std::vector<uint64_t> &rnd,
+                          const std::vector<uint64_t> &auxv, const std::vector<uint64_t> &alpha_pows, uint64_t *acc) {
+    const sym::Air &A = *I.sym;
+    const sym::Desc &d = A.d;
+    if (A.device != ctx.device) throw CudaError{ERR_INVALID, "symbolic AIR compiled for another device"};
+    std::vector<uint64_t> k(A.kl.words, 0);
+    for (uint64_t i = 0; i < d.num_public_values; i++) k[A.kl.pub + i] = I.pub[i] % gl::P;
+    for (uint64_t i = 0; i < 2ull * d.num_randomness; i++) k[A.kl.rnd + i] = rnd[i];
+    for (uint64_t i = 0; i < 2ull * d.num_aux_values; i++) k[A.kl.auxv + i] = auxv[i];
+    for (size_t i = 0; i < alpha_pows.size(); i++) k[A.kl.alpha + i] = alpha_pows[i];
+    DBuf dk = ctx.upload(k.empty() ? std::vector<uint64_t>{0} : k);
+    const uint64_t h = 1ull << log_h, qh = h << log_qd, D = 1ull << log_qd;
+    const uint64_t shift = gl::exp2k(gl::GEN, log_max_h - log_h);
+    DBuf per_nat;
+    uint64_t per_h = 0;
+    if (d.num_periodic) {
+        uint64_t max_p = 0;
+        std::vector<uint64_t> rep = sym::periodic_matrix(d, max_p);
+        const uint32_t log_p = log2u(max_p);
+        per_h = max_p << log_qd;
+        DBuf drep = ctx.upload(rep), brev = ctx.alloc(per_h * d.num_periodic), tmp = ctx.alloc(max_p * d.num_periodic);
+        per_nat = ctx.alloc(per_h * d.num_periodic);
+        coset_lde(ctx, drep.p, d.num_periodic, max_p, d.num_periodic, log_qd, gl::exp2k(shift, log_h - log_p), brev.p,
+                  tmp.p);
+        const uint64_t n = per_h * d.num_periodic;
+        bitrev_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx.stream>>>(brev.p, per_nat.p, log_p + log_qd,
+                                                                                 d.num_periodic);
+        CK(cudaGetLastError());
+        ctx.launches++;
+        ctx.sync();
+    }
+    const TwTables &twq = ctx.twiddles(log_h + log_qd);
+    sym::KArgs a{};
+    a.main = main_lde;
+    a.main_w = I.width;
+    a.aux = aux_lde;
+    a.aux_w2 = 2 * d.aux_width;
+    a.per = per_nat.p;
+    a.per_h = per_h ? per_h : 1;
+    a.per_w = d.num_periodic;
+    a.k = dk.p;
+    a.qh = qh;
+    a.log_qh = log_h + log_qd;
+    a.D = D;
+    a.shift = shift;
+    a.wq_lo = twq.fwd_lo.p;
+    a.wq_hi = twq.fwd_hi.p;
+    a.wq_lo_bits = twq.lo_bits;
+    a.omega_h_inv = gl::inv(gl::root(log_h));
+    {
+        uint64_t s_pow_n = gl::exp2k(shift, log_h), wd = gl::root(log_qd), x = 1;
+        for (uint64_t t = 0; t < D && t < 8; t++) a.zh[t] = gl::sub(gl::mul(s_pow_n, x), 1), x = gl::mul(x, wd);
+    }
+    a.acc = acc;
+    void *args[] = {&a};
+    CK(cudaLaunchKernel((const void *)A.kernel, dim3((unsigned)((qh + 127) / 128)), dim3(128), args, 0, ctx.stream));
+    ctx.launches++;
+    ctx.sync();  // keep the constant block and the periodic table alive until the kernel ran
+}
+
 inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, ProofOut &po) {
     using clk = std::chrono::steady_clock;
     Launcher L{ctx};
     const uint32_t lb = pcs.log_blowup;
     const uint32_t log_max_h = log2u(inst[n_inst - 1].height);
     uint32_t log_qd = 0;
-    for (size_t i = 0; i < n_inst; i++) log_qd = std::max(log_qd, air_log_quotient_degree(inst[i].air));
+    for (size_t i = 0; i < n_inst; i++) log_qd = std::max(log_qd, inst_log_qd(inst[i]));
     const uint64_t D = 1ull << log_qd;
     const uint32_t log_lde = log_max_h + lb;
     const uint64_t n = 1ull << log_lde;
@@ -280,7 +371,8 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
 
     // ---- 1. main traces: coset LDE on g^(2^lift) K, bit-reversed; aligned tree
     uint64_t max_hw = 0;
-    for (size_t i = 0; i < n_inst; i++) max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, 2));
+    for (size_t i = 0; i < n_inst; i++)
+        max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, 2 * inst_aux_width(inst[i])));
     max_hw = std::max(max_hw, inst[n_inst - 1].height * 2 * D);
     DBuf tmp = ctx.alloc(max_hw);
     std::vector<DBuf> main_lde(n_inst), aux_lde(n_inst);
@@ -291,22 +383,63 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     tr.send_commit(main_tree.root);
     CK(cudaEventRecord(ev[2], ctx.stream));
 
-    // ---- 2. randomness (max num_randomness over the AIRs = 1) and the
-    // dummy aux traces: one EF column of zeros, flattened to 2 base columns
-    // (p3-miden-lifted-examples/src/lib.rs:93-103). The LDE of a zero trace
-    // on any coset is zero, and its tree has one digest per layer
-    // (build_zero_tree): both are produced exactly, without transforms or
-    // per-leaf hashing.
-    (void)tr.ch.sample_ef();
+    // ---- 2. randomness (max num_randomness over the AIRs) and the aux
+    // traces from each instance's AuxBuilder, EF flattened to 2 base columns
+    // (prover/mod.rs:285-345). Without any builder every aux trace is zero:
+    // the LDE of a zero trace on any coset is zero, and its tree has one
+    // digest per layer (build_zero_tree), so both are produced exactly,
+    // without transforms or per-leaf hashing.
+    uint64_t n_rand = 0;
+    for (size_t i = 0; i < n_inst; i++) n_rand = std::max(n_rand, inst_num_randomness(inst[i]));
+    std::vector<uint64_t> rnd(2 * n_rand);
+    for (uint64_t r = 0; r < n_rand; r++) {
+        gl::ef e = tr.ch.sample_ef();
+        rnd[2 * r] = e.c0, rnd[2 * r + 1] = e.c1;
+    }
+    std::vector<std::vector<uint64_t>> aux_vals(n_inst);
+    bool any_builder = false;
     for (size_t i = 0; i < n_inst; i++) {
-        uint64_t h = inst[i].height;
-        aux_lde[i] = ctx.alloc((h << lb) * 2);
-        CK(cudaMemsetAsync(aux_lde[i].p, 0, (h << lb) * 16, ctx.stream));
-        aux_mats.push_back({aux_lde[i].p, h << lb, 2});
+        aux_vals[i].assign(2 * inst_num_aux_values(inst[i]), 0);
+        any_builder |= inst[i].aux_build != nullptr;
     }
     Tree aux_tree;
-    build_zero_tree(ctx, aux_tree, aux_mats, 8);
+    if (!any_builder) {
+        for (size_t i = 0; i < n_inst; i++) {
+            const uint64_t h = inst[i].height, aw2 = 2 * inst_aux_width(inst[i]);
+            aux_lde[i] = ctx.alloc((h << lb) * aw2);
+            CK(cudaMemsetAsync(aux_lde[i].p, 0, (h << lb) * aw2 * 8, ctx.stream));
+            aux_mats.push_back({aux_lde[i].p, h << lb, aw2});
+        }
+        build_zero_tree(ctx, aux_tree, aux_mats, 8);
+    } else {
+        for (size_t i = 0; i < n_inst; i++) {
+            const Instance &I = inst[i];
+            const uint64_t h = I.height, aw2 = 2 * inst_aux_width(I);
+            aux_lde[i] = ctx.alloc((h << lb) * aw2);
+            aux_mats.push_back({aux_lde[i].p, h << lb, aw2});
+            if (!I.aux_build) {
+                CK(cudaMemsetAsync(aux_lde[i].p, 0, (h << lb) * aw2 * 8, ctx.stream));
+                continue;
+            }
+            std::vector<uint64_t> host(h * aw2, 0);
+            if (I.aux_build(I.aux_user, i, I.trace, rnd.data(), inst_num_randomness(I), h, host.data(),
+                            aux_vals[i].data()) != 0)
+                throw CudaError{ERR_VALIDATION, "aux builder failed for instance " + std::to_string(i)};
+            for (uint64_t v : host)
+                if (v >= gl::P) throw CudaError{ERR_INVALID, "aux builder wrote a non-canonical word"};
+            for (uint64_t v : aux_vals[i])
+                if (v >= gl::P) throw CudaError{ERR_INVALID, "aux builder wrote a non-canonical aux value"};
+            DBuf up = ctx.alloc(h * aw2);
+            CK(cudaMemcpyAsync(up.p, host.data(), h * aw2 * 8, cudaMemcpyHostToDevice, ctx.stream));
+            po.h2d += h * aw2 * 8;
+            coset_lde(ctx, up.p, aw2, h, aw2, lb, gl::exp2k(gl::GEN, log_max_h - log2u(h)), aux_lde[i].p, tmp.p);
+            ctx.sync();  // `host` and `up` are released at the end of this iteration
+        }
+        build_tree(ctx, aux_tree, aux_mats, 8);
+    }
     tr.send_commit(aux_tree.root);
+    for (size_t i = 0; i < n_inst; i++)  // aux values, per instance (prover/mod.rs:347-353)
+        for (size_t k = 0; k < aux_vals[i].size(); k += 2) tr.send_ef(gl::ef{aux_vals[i][k], aux_vals[i][k + 1]});
     CK(cudaEventRecord(ev[3], ctx.stream));
 
     // ---- 4./5. alpha, beta; constraints with cyclic extension
@@ -327,12 +460,18 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             if (qh > acc_len) L(quot::tile_ef_kernel, blocks_for(qh - acc_len, 256), 256, 0, acc.p, acc_len, qh);
         }
         acc_len = qh;
-        const uint64_t K = air_num_constraints(I.air, I.width);
+        const uint64_t K = inst_num_constraints(I);
         std::vector<uint64_t> ap(2 * K);
         gl::ef p = gl::ef_one();
         for (uint64_t k = K; k-- > 0;) {
             ap[2 * k] = p.c0, ap[2 * k + 1] = p.c1;
             p = gl::ef_mul(p, alpha);
+        }
+        if (I.air == AIR_SYMBOLIC) {
+            eval_symbolic(ctx, I, main_lde[ii].p, aux_lde[ii].p, log_h, log_qd, log_max_h, rnd, aux_vals[ii], ap,
+                          acc.p);
+            L.n++;
+            continue;
         }
         DBuf d_ap = ctx.upload(ap);
         DBuf d_consts;

@@ -454,6 +454,7 @@ struct Prepared {
     uint64_t dg[12];
     gl::ef alpha, beta, z, ac, bp, red_open[2], zs[2];
     std::vector<gl::ef> evals;
+    std::vector<gl::ef> rnd, auxv;  // aux randomness; aux values of every instance, in order
     std::vector<uint64_t> aw;
     uint64_t total_aligned = 0, D = 1, rounds = 0, final_deg = 1, arity = 2, nq = 0;
     uint32_t log_max_h = 0, log_qd = 0, log_lde = 0, log_a = 1;
@@ -470,18 +471,47 @@ struct Prepared {
 inline bool quotient_identity(const Prepared &v) {
     const size_t n_inst = v.inst.size();
     gl::ef accumulated = gl::ef_zero();
-    uint64_t off = 0;
+    uint64_t off = 0, aux_off = 0, auxv_off = 0;
+    for (size_t i = 0; i < n_inst; i++) aux_off += v.aw[i];
     for (size_t i = 0; i < n_inst; i++) {
-        const uint32_t log_h = log2u(v.inst[i].height), lift = v.log_max_h - log_h;
+        const Instance &I = v.inst[i];
+        const uint32_t log_h = log2u(I.height), lift = v.log_max_h - log_h;
         const gl::ef zl = gl::ef_exp2k(v.z, lift);
         const gl::ef van = gl::ef_sub(gl::ef_exp2k(zl, log_h), gl::ef_one());
         const uint64_t oinv = gl::inv(gl::root(log_h));
         const gl::ef first = gl::ef_mul(van, gl::ef_inv(gl::ef_sub(zl, gl::ef_one())));
         const gl::ef trans = gl::ef_sub(zl, gl::ef{oinv, 0});
-        const gl::ef folded =
-            folded_constraints(v.inst[i], &v.evals[off], &v.evals[v.total_aligned + off], first, trans, v.alpha);
+        gl::ef folded;
+        if (I.air == AIR_SYMBOLIC) {  // ConstraintFolder over the DAG (verifier/mod.rs:286-339)
+            const sym::Desc &d = I.sym->d;
+            const gl::ef X{0, 1};
+            std::vector<gl::ef> al(d.aux_width), an(d.aux_width), per;
+            const uint64_t T = v.total_aligned;
+            for (uint32_t c = 0; c < d.aux_width; c++) {  // row_to_packed_ext
+                al[c] = gl::ef_add(v.evals[aux_off + 2 * c], gl::ef_mul(X, v.evals[aux_off + 2 * c + 1]));
+                an[c] = gl::ef_add(v.evals[T + aux_off + 2 * c], gl::ef_mul(X, v.evals[T + aux_off + 2 * c + 1]));
+            }
+            sym::periodic_at(d, 1ull << v.log_max_h, v.z, per);
+            sym::Point pt{};
+            pt.main_local = &v.evals[off];
+            pt.main_next = &v.evals[T + off];
+            pt.aux_local = al.data();
+            pt.aux_next = an.data();
+            pt.pub = I.pub;
+            pt.rand = v.rnd.data();
+            pt.auxv = v.auxv.data() + auxv_off;
+            pt.periodic = per.data();
+            pt.sel[0] = first;
+            pt.sel[1] = gl::ef_mul(van, gl::ef_inv(gl::ef_sub(zl, gl::ef{oinv, 0})));
+            pt.sel[2] = trans;
+            folded = sym::fold_at(*I.sym, pt, v.alpha);
+        } else {
+            folded = folded_constraints(I, &v.evals[off], &v.evals[v.total_aligned + off], first, trans, v.alpha);
+        }
         accumulated = gl::ef_add(gl::ef_mul(accumulated, v.beta), folded);
         off += v.aw[i];
+        aux_off += v.aw[n_inst + i];
+        auxv_off += inst_num_aux_values(I);
     }
     uint64_t qoff = 0;
     for (size_t m = 0; m < 2 * n_inst; m++) qoff += v.aw[m];
@@ -524,7 +554,12 @@ inline void prepare(const uint64_t *p2, const PcsParams &pcs, const Instance *in
     r.f = fields, r.nf = n_fields, r.c = commits, r.nc = n_commits;
     const uint32_t lb = pcs.log_blowup;
     v.log_max_h = log2u(inst[n_inst - 1].height);
-    for (size_t i = 0; i < n_inst; i++) v.log_qd = std::max(v.log_qd, air_log_quotient_degree(inst[i].air));
+    uint64_t n_rand = 0, n_auxv = 0;
+    for (size_t i = 0; i < n_inst; i++) {
+        v.log_qd = std::max(v.log_qd, inst_log_qd(inst[i]));
+        n_rand = std::max(n_rand, inst_num_randomness(inst[i]));
+        n_auxv += inst_num_aux_values(inst[i]);
+    }
     if (v.log_qd > lb) {
         v.early = V_SHAPE;
         return;
@@ -536,8 +571,11 @@ inline void prepare(const uint64_t *p2, const PcsParams &pcs, const Instance *in
     // commitments and challenges in prover order
     uint64_t main_c[4], aux_c[4], quot_c[4];
     r.commit(main_c, true);
-    (void)r.ch.sample_ef();  // aux randomness
+    v.rnd.resize(n_rand);
+    for (auto &e : v.rnd) e = r.ch.sample_ef();  // aux randomness
     r.commit(aux_c, true);
+    v.auxv.resize(n_auxv);
+    for (auto &e : v.auxv) e = r.ef();  // aux values (verifier/mod.rs:230-239)
     v.alpha = r.ch.sample_ef();
     v.beta = r.ch.sample_ef();
     r.commit(quot_c, true);
@@ -554,7 +592,7 @@ inline void prepare(const uint64_t *p2, const PcsParams &pcs, const Instance *in
     // matrices: main (one per instance), aux (2 columns each), quotient (2D)
     std::vector<uint64_t> ow;
     for (size_t i = 0; i < n_inst; i++) ow.push_back(inst[i].width);
-    for (size_t i = 0; i < n_inst; i++) ow.push_back(2);
+    for (size_t i = 0; i < n_inst; i++) ow.push_back(2 * inst_aux_width(inst[i]));
     ow.push_back(2 * v.D);
     for (uint64_t w : ow) v.aw.push_back((w + 7) / 8 * 8), v.total_aligned += v.aw.back();
     const uint64_t T = v.total_aligned;

@@ -29,9 +29,24 @@ class PcsParams(C.Structure):
         "folding_pow_bits", "deep_pow_bits", "num_queries", "query_pow_bits")]
 
 
+AIR_SYMBOLIC = 3
+# or_aux_fn: the AuxBuilder callback (same signature as the product's)
+AUX_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.c_uint64,
+                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+
+
+class SymAir(C.Structure):
+    _fields_ = [("main_width", C.c_uint32), ("aux_width", C.c_uint32), ("num_randomness", C.c_uint32),
+                ("num_aux_values", C.c_uint32), ("num_public_values", C.c_uint32), ("num_periodic", C.c_uint32),
+                ("periodic_lengths", u64p), ("periodic_values", u64p), ("nodes", C.c_void_p),
+                ("n_nodes", C.c_size_t), ("constraints", C.POINTER(C.c_uint32)), ("is_ext", C.POINTER(C.c_uint8)),
+                ("n_constraints", C.c_size_t)]
+
+
 class Instance(C.Structure):
     _fields_ = [("air", C.c_int), ("height", C.c_size_t), ("width", C.c_size_t),
-                ("trace", u64p), ("consts", u64p)]
+                ("trace", u64p), ("consts", u64p), ("sym", C.POINTER(SymAir)), ("public_values", u64p),
+                ("aux_build", AUX_FN), ("aux_user", C.c_void_p)]
 
 
 class Proof(C.Structure):
@@ -132,6 +147,9 @@ def lib():
             ("or_last_stage_seconds", C.c_double, [C.c_int]),
             ("or_verify", C.c_int, [C.POINTER(P2Params), C.POINTER(PcsParams), C.POINTER(Instance), C.c_size_t,
                                     u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
+            ("or_sym_validate", C.c_int, [C.POINTER(SymAir)]),
+            ("or_sym_max_degree", C.c_uint, [C.POINTER(SymAir)]),
+            ("or_sym_log_quotient_degree", C.c_uint, [C.POINTER(SymAir)]),
         ]:
             fn = getattr(L, name)
             fn.restype = res
@@ -262,15 +280,75 @@ def check_constraints(air: int, trace: np.ndarray, consts=None) -> int:
     return int(lib().or_check_constraints(air, h, w, ptr(c), ptr(t)))
 
 
+def sym_air(desc, keep) -> SymAir:
+    """The oracle's view of a symbolic AIR description (the product's
+    symbolic.AirDesc: the same node layout)."""
+    nodes = np.ascontiguousarray(desc.nodes)
+    cons = np.ascontiguousarray(desc.constraints, dtype=np.uint32)
+    ext = np.ascontiguousarray(desc.is_ext, dtype=np.uint8)
+    pl = np.ascontiguousarray(desc.periodic_lengths, dtype=np.uint64)
+    pv = np.ascontiguousarray(desc.periodic_values, dtype=np.uint64)
+    keep += [nodes, cons, ext, pl, pv]
+    a = SymAir(desc.width, desc.aux_width, desc.num_randomness, desc.num_aux_values, desc.num_public_values,
+               pl.size, ptr(pl) if pl.size else None, ptr(pv) if pv.size else None, nodes.ctypes.data,
+               nodes.size, cons.ctypes.data_as(C.POINTER(C.c_uint32)), ext.ctypes.data_as(C.POINTER(C.c_uint8)),
+               cons.size)
+    keep.append(a)
+    return a
+
+
+def sym_degree(desc):
+    keep = []
+    a = sym_air(desc, keep)
+    return int(lib().or_sym_max_degree(C.byref(a))), int(lib().or_sym_log_quotient_degree(C.byref(a)))
+
+
+def aux_fn(fn, keep):
+    """fn(instance, randomness [(c0, c1)], height) -> (aux words h x 2*aux_width, aux value words)."""
+    def cb(user, instance, main_trace, rnd, n_rnd, height, aux_out, vals_out):
+        try:
+            r = [(int(rnd[2 * i]), int(rnd[2 * i + 1])) for i in range(n_rnd)]
+            aux, vals = fn(int(instance), r, int(height))
+            aux = np.ascontiguousarray(aux, dtype=np.uint64).reshape(-1)
+            vals = np.ascontiguousarray(vals, dtype=np.uint64).reshape(-1)
+            C.memmove(aux_out, aux.ctypes.data, aux.nbytes)
+            if vals.size:
+                C.memmove(vals_out, vals.ctypes.data, vals.nbytes)
+            return 0
+        except Exception:
+            return 1
+    f = AUX_FN(cb)
+    keep.append(f)
+    return f
+
+
+def _instance(air, h, w, trace_ptr, consts, extra, keep) -> Instance:
+    """extra: None, or a dict with 'sym' (AirDesc), 'public_values', 'aux_builder'."""
+    c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
+    keep.append(c)
+    extra = extra or {}
+    sym = None
+    if extra.get("sym") is not None:
+        sym = C.pointer(sym_air(extra["sym"], keep))
+        air = AIR_SYMBOLIC
+    pv = np.ascontiguousarray(extra.get("public_values") if extra.get("public_values") is not None
+                              else np.zeros(1), dtype=np.uint64)
+    keep.append(pv)
+    fb = aux_fn(extra["aux_builder"], keep) if extra.get("aux_builder") is not None else AUX_FN()
+    return Instance(air, h, w, trace_ptr, ptr(c), sym, ptr(pv), fb, None)
+
+
 def prove(pp: P2Params, pcs: dict, instances):
-    """instances: list of (air, trace ndarray, consts ndarray|None). Returns a dict."""
+    """instances: list of (air, trace ndarray, consts ndarray|None[, extra])
+    where extra holds a symbolic AIR ('sym'), its 'public_values' and its
+    'aux_builder'. Returns a dict."""
     keep = []
     arr = (Instance * len(instances))()
-    for i, (air, trace, consts) in enumerate(instances):
+    for i, inst in enumerate(instances):
+        air, trace, consts = inst[:3]
         t = np.ascontiguousarray(trace, dtype=np.uint64)
-        c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
-        keep += [t, c]
-        arr[i] = Instance(air, t.shape[0], t.shape[1], ptr(t), ptr(c))
+        keep.append(t)
+        arr[i] = _instance(air, t.shape[0], t.shape[1], ptr(t), consts, inst[3] if len(inst) > 3 else None, keep)
     pr = PcsParams(**pcs)
     proof = Proof()
     rc = lib().or_prove(C.byref(pp), C.byref(pr), arr, len(instances), C.byref(proof))
@@ -291,6 +369,7 @@ def prove(pp: P2Params, pcs: dict, instances):
 VERIFY_ERRORS = {0: "accepted", 1: "shape", 2: "opening index", 3: "LMCS root", 4: "proof of work",
                  5: "DEEP point on domain", 6: "FRI row", 7: "final polynomial", 8: "quotient identity",
                  9: "transcript length", 10: "digest"}
+VERIFY_ERRORS_CODE = {v: k for k, v in VERIFY_ERRORS.items()}
 
 
 def verify(pp: P2Params, pcs: dict, instances, fields, commits, digest) -> int:
@@ -300,10 +379,9 @@ def verify(pp: P2Params, pcs: dict, instances, fields, commits, digest) -> int:
     keep = []
     arr = (Instance * len(instances))()
     dummy = np.zeros(1, dtype=np.uint64)
-    for i, (air, h, w, consts) in enumerate(instances):
-        c = np.ascontiguousarray(consts if consts is not None else np.zeros(1), dtype=np.uint64)
-        keep.append(c)
-        arr[i] = Instance(air, h, w, ptr(dummy), ptr(c))
+    for i, inst in enumerate(instances):
+        air, h, w, consts = inst[:4]
+        arr[i] = _instance(air, h, w, ptr(dummy), consts, inst[4] if len(inst) > 4 else None, keep)
     f = np.ascontiguousarray(fields, dtype=np.uint64)
     cm = np.ascontiguousarray(np.asarray(commits, dtype=np.uint64).reshape(-1))
     d = np.ascontiguousarray(digest, dtype=np.uint64)

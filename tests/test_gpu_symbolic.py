@@ -1,0 +1,125 @@
+"""Symbolic AIRs on the GPU: proofs made with the generated constraint
+kernels (NVRTC, sm_100a) and caller-built aux traces are bit-identical to the
+oracle's, and the device verifier accepts them. The AIRs are the reference's
+own test and example AIRs (TinyAir, BusTestAir, DummyMidenAir) and the cubic
+AIR written symbolically, which must also reproduce the hand-written cubic
+kernel's proof."""
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+import sym_airs as S
+
+pytestmark = pytest.mark.gpu
+
+
+def pcs_dict(p):
+    return dict(log_blowup=p.log_blowup, log_folding_arity=p.log_folding_arity,
+                log_final_degree=p.log_final_degree, folding_pow_bits=p.folding_pow_bits,
+                deep_pow_bits=p.deep_pow_bits, num_queries=p.num_queries, query_pow_bits=p.query_pow_bits)
+
+
+def check_same(gpu, orc):
+    assert np.array_equal(gpu.proof.commitments, orc["commits"]), "commitments differ"
+    assert len(gpu.proof.fields) == len(orc["fields"])
+    diff = np.nonzero(gpu.proof.fields != orc["fields"])[0]
+    assert diff.size == 0, f"first differing field at {diff[:5]}"
+    assert np.array_equal(gpu.digest, orc["digest"])
+
+
+def test_symbolic_cubic_matches_builtin_kernel(product, gpu_ctx):
+    k, t = O.cubic_trace(7, 16, 31)
+    k2, t2 = O.cubic_trace(9, 8, 32)
+    pcs = product.PcsParams(2, 2, 0, 4, 1, 16, 1)
+    a1 = product.Air(gpu_ctx, product.build_air(S.cubic_eval(k), 16))
+    a2 = product.Air(gpu_ctx, product.build_air(S.cubic_eval(k2), 8))
+    assert (a1.log_quotient_degree, a1.max_degree) == (1, 3)
+    sym = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(a1, t), product.AirWitness(a2, t2)])
+    builtin = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k),
+                                                 product.AirWitness(product.AIR_CUBIC, t2, k2)])
+    assert np.array_equal(sym.proof.fields, builtin.proof.fields)
+    assert np.array_equal(sym.digest, builtin.digest)
+    check_same(sym, O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_CUBIC, t, k), (O.AIR_CUBIC, t2, k2)]))
+    shapes = [product.AirShape(a1, t.shape[0], 16), product.AirShape(a2, t2.shape[0], 8)]
+    assert product.verify_output(gpu_ctx, pcs, shapes, sym).ok
+
+
+@pytest.mark.parametrize("periods,heights", [((), (8,)), ((4,), (16,)), ((2, 4), (4, 8)),
+                                             ((2, 4), (4, 8, 16)), ((8,), (1024, 4096))])
+def test_tiny_air_matches_oracle(product, gpu_ctx, periods, heights):
+    """TinyAir (tests/tiny_air.rs): periodic columns, an aux trace from a
+    caller's AuxBuilder (challenge^(4^row), extension field), an aux value,
+    a public value per instance; lifted traces of several heights."""
+    desc = product.build_air(S.tiny_eval, 1, num_public_values=1, num_aux_values=1,
+                             periodic_columns=S.tiny_periodic(periods))
+    air = product.Air(gpu_ctx, desc)
+    assert air.log_quotient_degree == 2
+    wits, oinst, shapes = [], [], []
+    for i, h in enumerate(heights):
+        t = S.tiny_trace(i + 2, h)
+        pv = np.array([i + 2], dtype=np.uint64)
+        wits.append(product.AirWitness(air, t, public_values=pv, aux_builder=S.tiny_aux))
+        oinst.append((O.AIR_SYMBOLIC, t, None, {"sym": desc, "public_values": pv, "aux_builder": S.tiny_aux}))
+        shapes.append(product.AirShape(air, h, 1, public_values=pv))
+    pcs = product.PcsParams(2, 1, 0, 3, 0, 12, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, wits)
+    check_same(gpu, O.prove(O.default_p2(), pcs_dict(pcs), oinst))
+    assert product.verify_output(gpu_ctx, pcs, shapes, gpu).ok
+    bad = gpu.proof.fields.copy()
+    bad[3] = (int(bad[3]) + 1) % O.P
+    assert not product.verify_multi(gpu_ctx, pcs, shapes, bad, gpu.proof.commitments, gpu.digest).ok
+
+
+def test_bus_air_matches_oracle(product, gpu_ctx):
+    """BusTestAir (tests/bus_test.rs): extension-field constraints on two aux
+    columns built from two challenges, three public values, two aux values."""
+    desc = product.build_air(S.bus_eval, 1, aux_width=2, num_randomness=2, num_aux_values=2, num_public_values=3)
+    air = product.Air(gpu_ctx, desc)
+    base, ext = air.layout()
+    assert base.size == 2 and ext.size == 6
+    pv = np.array([2, 42, 67], dtype=np.uint64)
+    t = S.tiny_trace(2, 64)
+    pcs = product.PcsParams(2, 2, 0, 4, 0, 20, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(air, t, public_values=pv,
+                                                                aux_builder=S.bus_aux(42, 67))])
+    extra = {"sym": desc, "public_values": pv, "aux_builder": S.bus_aux(42, 67)}
+    check_same(gpu, O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_SYMBOLIC, t, None, extra)]))
+    assert product.verify_output(gpu_ctx, pcs, [product.AirShape(air, 64, 1, public_values=pv)], gpu).ok
+
+
+def test_miden_dummy_air_matches_oracle(product, gpu_ctx):
+    """DummyMidenAir (p3-miden-lifted-examples/src/miden.rs): a degree-9
+    constraint, eight quotient chunks (log_blowup 3), eight all-zero aux EF
+    columns and aux values, two traces of 51 and 20 columns (the example's
+    widths) at reduced heights."""
+    d1 = product.build_air(S.miden_eval, 51, aux_width=8, num_randomness=2, num_aux_values=8)
+    d2 = product.build_air(S.miden_eval, 20, aux_width=8, num_randomness=2, num_aux_values=8)
+    a1, a2 = product.Air(gpu_ctx, d1), product.Air(gpu_ctx, d2)
+    assert a1.log_quotient_degree == 3
+    t1, t2 = S.miden_trace(51, 10, 1), S.miden_trace(20, 11, 2)
+    pcs = product.PcsParams(3, 2, 0, 8, 0, 24, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(a1, t1), product.AirWitness(a2, t2)])
+    check_same(gpu, O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_SYMBOLIC, t1, None, {"sym": d1}),
+                                                               (O.AIR_SYMBOLIC, t2, None, {"sym": d2})]))
+    shapes = [product.AirShape(a1, 1 << 10, 51), product.AirShape(a2, 1 << 11, 20)]
+    assert product.verify_output(gpu_ctx, pcs, shapes, gpu).ok
+
+
+def test_mixed_builtin_and_symbolic_instances(product, gpu_ctx):
+    """A Keccak instance (hand-written kernel, dummy aux) lifted with a
+    TinyAir instance (generated kernel, caller aux) in one proof."""
+    desc = product.build_air(S.tiny_eval, 1, num_public_values=1, num_aux_values=1,
+                             periodic_columns=S.tiny_periodic((4,)))
+    air = product.Air(gpu_ctx, desc)
+    tt = S.tiny_trace(5, 64)
+    pv = np.array([5], dtype=np.uint64)
+    kt = O.keccak_trace(O.keccak_inputs(4, 5), 7)
+    pcs = product.PcsParams(2, 1, 0, 4, 0, 16, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(air, tt, public_values=pv, aux_builder=S.tiny_aux),
+                                             product.AirWitness(product.AIR_KECCAK, kt)])
+    orc = O.prove(O.default_p2(), pcs_dict(pcs), [
+        (O.AIR_SYMBOLIC, tt, None, {"sym": desc, "public_values": pv, "aux_builder": S.tiny_aux}),
+        (O.AIR_KECCAK, kt, None)])
+    check_same(gpu, orc)
+    shapes = [product.AirShape(air, 64, 1, public_values=pv), product.AirShape(product.AIR_KECCAK, 128, kt.shape[1])]
+    assert product.verify_output(gpu_ctx, pcs, shapes, gpu).ok
