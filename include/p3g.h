@@ -40,12 +40,80 @@ enum p3g_status {
 };
 
 enum p3g_air {
-    P3G_AIR_CUBIC = 1,  /* c_i[r+1] = c_i[r]^3 + c_{(i+1) mod w}[r] + k_i, degree 3 */
-    P3G_AIR_KECCAK = 2  /* Keccak-f[1600] AIR, 2633 columns, 24 rows per permutation */
+    P3G_AIR_CUBIC = 1,   /* c_i[r+1] = c_i[r]^3 + c_{(i+1) mod w}[r] + k_i, degree 3 */
+    P3G_AIR_KECCAK = 2,  /* Keccak-f[1600] AIR, 2633 columns, 24 rows per permutation */
+    P3G_AIR_SYMBOLIC = 3 /* any AIR given as symbolic constraints (p3g_air_create) */
 };
 
 typedef struct p3g_ctx p3g_ctx;
 typedef struct p3g_tree p3g_tree;
+typedef struct p3g_air p3g_air;
+
+/* ------------------------------------------------------- symbolic AIRs
+ * LiftedAir (p3-miden-lifted-air/src/air.rs:42-319) through its symbolic
+ * form: the expression DAG p3-air's SymbolicAirBuilder records when eval()
+ * runs on it (the reference's own symbolic pass, air.rs:225-247; the types
+ * are re-exported at p3-miden-lifted-air/src/lib.rs:34-37). Nodes are in
+ * topological order (operands before the node). Leaves: constants, main
+ * trace cells (column a, row offset b: 0 local, 1 next), aux (permutation)
+ * trace cells (extension field), public values, aux randomness (permutation
+ * challenges, extension), aux values (permutation values, extension),
+ * periodic columns and the three selectors; inner nodes: +, -, *, negation.
+ * The constraint list gives the node each assert_zero (is_ext 0) or
+ * assert_zero_ext (is_ext 1) asserted, in emission order. */
+enum p3g_sym_op {
+    P3G_SYM_CONST = 0, P3G_SYM_MAIN = 1, P3G_SYM_AUX = 2, P3G_SYM_PUBLIC = 3, P3G_SYM_RANDOMNESS = 4,
+    P3G_SYM_AUX_VALUE = 5, P3G_SYM_PERIODIC = 6, P3G_SYM_IS_FIRST_ROW = 7, P3G_SYM_IS_LAST_ROW = 8,
+    P3G_SYM_IS_TRANSITION = 9, P3G_SYM_ADD = 10, P3G_SYM_SUB = 11, P3G_SYM_MUL = 12, P3G_SYM_NEG = 13
+};
+typedef struct {
+    uint32_t op, a, b, pad; /* enum p3g_sym_op; operands or variable index / row offset */
+    uint64_t value;         /* P3G_SYM_CONST: a canonical field element */
+} p3g_sym_node;
+/* AirLayout (air.rs:150-163) plus the periodic columns (LiftedAir::
+ * periodic_columns, air.rs:51-57) and the constraint DAG. */
+typedef struct {
+    uint32_t main_width, aux_width, num_randomness, num_aux_values, num_public_values, num_periodic;
+    const uint64_t *periodic_lengths; /* num_periodic powers of two */
+    const uint64_t *periodic_values;  /* the periodic columns, concatenated */
+    const p3g_sym_node *nodes;
+    uint64_t n_nodes;
+    const uint32_t *constraints; /* node per constraint, emission order */
+    const uint8_t *is_ext;       /* 1: assert_zero_ext, 0: assert_zero */
+    uint64_t n_constraints;
+} p3g_air_desc;
+/* Validates the DAG (operand order; variable indices inside the declared
+ * dimensions, the bounds LiftedAir::is_valid_builder checks), derives the
+ * degree multiples and log_quotient_degree = log2_ceil(max(M, 2) - 1)
+ * (air.rs:225-247) and the base/extension ConstraintLayout
+ * (constraints/layout.rs:27-37), generates the constraint kernel for gJ
+ * (constraints/mod.rs:63-179) and compiles it with NVRTC for the context's
+ * device. P3G_ERR_VALIDATION for a malformed DAG (p3g_last_error says why). */
+int p3g_air_create(p3g_ctx *ctx, const p3g_air_desc *desc, p3g_air **out);
+void p3g_air_free(p3g_air *air);
+uint32_t p3g_air_log_quotient_degree(const p3g_air *air);
+uint32_t p3g_air_max_degree(const p3g_air *air);
+uint64_t p3g_air_num_constraints_of(const p3g_air *air);
+/* ConstraintLayout: base_indices / ext_indices; *n_base and *n_ext are
+ * capacities on entry and counts on return. */
+int p3g_air_layout(const p3g_air *air, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext);
+/* No device needed: the analysis, the generated kernel source (*len = size
+ * with the terminating zero), and an NVRTC compile for sm_<cc>a. */
+int p3g_air_analyse(const p3g_air_desc *desc, uint32_t *max_degree, uint32_t *log_quotient_degree,
+                    uint64_t *n_base, uint64_t *n_ext);
+int p3g_air_generate_source(const p3g_air_desc *desc, char *buf, uint64_t cap, uint64_t *len);
+int p3g_air_compile_check(const p3g_air_desc *desc, int32_t cc, uint64_t *cubin_bytes);
+
+/* AuxBuilder::build_aux_trace (p3-miden-lifted-air/src/auxiliary/builder.rs:
+ * 16-37), called once per instance after the main commitment with the
+ * instance's num_randomness challenges (2 words each). It writes the aux
+ * trace, height x aux_width extension elements (2 words each, row-major)
+ * into aux_out and num_aux_values extension elements into aux_values_out
+ * (host memory the library provides), and returns 0; any other value ends
+ * the proof with P3G_ERR_VALIDATION. main_trace is the instance's trace
+ * pointer as given (host or device). */
+typedef int (*p3g_aux_build_fn)(void *user, uint64_t instance, const uint64_t *main_trace, const uint64_t *randomness,
+                                uint64_t n_randomness, uint64_t height, uint64_t *aux_out, uint64_t *aux_values_out);
 
 /* PcsParams::new(log_blowup, log_folding_arity, log_final_degree,
  * folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits)
@@ -65,6 +133,15 @@ typedef struct {
     const uint64_t *trace;   /* row-major height x width */
     const uint64_t *consts;  /* host; cubic AIR: k[width]; Keccak: NULL */
     uint64_t n_consts;
+    const p3g_air *sym;      /* P3G_AIR_SYMBOLIC: the compiled AIR */
+    const uint64_t *public_values; /* AirWitness::public_values (host) */
+    uint64_t n_public_values;
+    /* The instance's AuxBuilder; NULL: an all-zero aux trace (the examples'
+     * dummy builder: one EF column for the built-in AIRs, aux_width columns
+     * and num_aux_values zero values for a symbolic AIR). The built-in AIRs
+     * declare aux_width 1, num_randomness 1, num_aux_values 0. */
+    p3g_aux_build_fn aux_build;
+    void *aux_user;
 } p3g_instance;
 
 /* StarkOutput { digest, proof: TranscriptData { fields, commitments } }
@@ -165,6 +242,37 @@ int p3g_lmcs_layer(p3g_ctx *ctx, const p3g_tree *tree, uint32_t level, uint64_t 
 int p3g_lmcs_prove_batch(p3g_ctx *ctx, const p3g_tree *tree, const uint64_t *indices, uint64_t n,
                          uint64_t *fields_out, uint64_t *n_fields, uint64_t *commits_out, uint64_t *n_commits);
 void p3g_lmcs_free(p3g_tree *tree);
+
+/* LmcsTree::rows (p3-miden-lmcs/src/lib.rs:277, lifted_tree.rs:127-138): the
+ * row of each committed matrix at leaf `index` (lifted), each zero-padded to
+ * the tree's alignment, concatenated; *n_words is the capacity on entry and
+ * the count on return. */
+int p3g_lmcs_rows(p3g_ctx *ctx, const p3g_tree *tree, uint64_t index, uint64_t *out, uint64_t *n_words);
+
+/* One FRI round's fold (FriFold::fold_matrix, p3-miden-lifted-fri/src/fri/
+ * fold/mod.rs:119-181, arity{2,4,8}.rs:32-148): d_in holds a layer of 2^log_n
+ * EF values, bit-reversed; d_out receives the 2^(log_n - log_arity) folded
+ * values with challenge beta2. The round's commitment (FriPolys::new,
+ * fri/prover.rs:143-150) is p3g_lmcs_build of d_in viewed as
+ * (n / a) x 2a base words with alignment 1. */
+int p3g_fri_fold(p3g_ctx *ctx, const uint64_t *d_in, uint32_t log_n, uint32_t log_arity, const uint64_t *beta2,
+                 uint64_t *d_out);
+
+/* DEEP at the stage seam, over committed matrices (bit-reversed LDEs on g*K,
+ * ascending heights; the tallest is the LDE domain), at the points
+ * z4 = (z_0, z_1) (2 EF). p3g_deep_evals: PointQuotients::new and
+ * batch_eval_lifted (p3-miden-lifted-fri/src/deep/interpolate.rs:81-201),
+ * f(z_0), f(z_1) of every column into evals_out (host, 4 words per column,
+ * matrix by matrix). p3g_deep_quotient: DeepPoly::from_evals +
+ * accumulate_matrices (deep/prover.rs:106-364) with the column challenge
+ * alpha2 and the point challenge beta2, columns padded to `alignment`
+ * (the LMCS alignment); d_out receives the quotient's n EF values
+ * (bit-reversed), the first FRI layer. */
+int p3g_deep_evals(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
+                   uint64_t n_mats, uint32_t log_blowup, const uint64_t *z4, uint64_t *evals_out);
+int p3g_deep_quotient(p3g_ctx *ctx, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
+                      uint64_t n_mats, uint32_t log_blowup, uint32_t alignment, const uint64_t *z4,
+                      const uint64_t *evals, const uint64_t *alpha2, const uint64_t *beta2, uint64_t *d_out);
 
 /* The configuration's permutation (Poseidon2Goldilocks<12>::permute_mut) on
  * n device states of 12 words, in place. */

@@ -90,6 +90,138 @@ size_t or_inst_num_constraints(const or_instance *I) {
     return I->air == OR_AIR_SYMBOLIC ? I->sym->n_constraints : or_air_num_constraints(I->air, I->width);
 }
 
+/* DEEP openings (PointQuotients::new, p3-miden-lifted-fri/src/deep/interpolate.rs:81-109,
+ * and batch_eval_lifted, :123-201): f(z_j) of every column of every matrix
+ * (bit-reversed LDEs on g*K, ascending heights, the largest the LDE domain),
+ * matrix by matrix, 4 words per column: z_0 (c0, c1), z_1 (c0, c1). The first
+ * d_m = h_m / B rows of a bit-reversed LDE are the trace domain's points in
+ * bit-reversed order, so f(z) = s(z) sum_i w_i(z) f(x_i) with barycentric
+ * weights folded by blocks for shorter matrices. */
+void or_deep_evals(const or_matrix *mats, size_t n_mats, unsigned log_blowup, const or_ef zs[2], uint64_t *out) {
+    const size_t n_lde = mats[n_mats - 1].height;
+    const unsigned log_lde = or_log2(n_lde);
+    uint64_t *xs = (uint64_t *)malloc(n_lde * 8);
+    uint64_t wn = or_root(log_lde);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n_lde; i++) xs[i] = or_mul(OR_GEN, or_pow(wn, or_bitrev(i, log_lde)));
+    size_t d = n_lde >> log_blowup;
+    or_ef *q = (or_ef *)malloc(d * 2 * sizeof(or_ef));
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < d; i++)
+        for (int j = 0; j < 2; j++) q[2 * i + j] = or_ef_inv(or_ef_sub(zs[j], or_ef_from(xs[i])));
+    unsigned log_d = or_log2(d);
+    or_ef sj[2];
+    for (int j = 0; j < 2; j++) {
+        or_ef t = or_ef_sub(or_ef_exp2(or_ef_mulf(zs[j], or_inv(OR_GEN)), log_d), or_ef_from(1));
+        sj[j] = or_ef_mulf(t, or_inv((uint64_t)d));
+    }
+    or_ef *wts = (or_ef *)malloc(d * 2 * sizeof(or_ef));
+    size_t off = 0;
+    for (size_t m = 0; m < n_mats; m++) {
+        const or_matrix *M = &mats[m];
+        size_t dm = M->height >> log_blowup, ratio = d / dm;
+        for (size_t i = 0; i < dm; i++)
+            for (int j = 0; j < 2; j++) {
+                or_ef s = or_ef_from(0);
+                for (size_t c = 0; c < ratio; c++) {
+                    size_t ii = i * ratio + c;
+                    s = or_ef_add(s, or_ef_mulf(q[2 * ii + j], xs[ii]));
+                }
+                wts[2 * i + j] = s;
+            }
+#pragma omp parallel for schedule(static)
+        for (size_t col = 0; col < M->width; col++)
+            for (int j = 0; j < 2; j++) {
+                or_ef s = or_ef_from(0);
+                for (size_t i = 0; i < dm; i++) s = or_ef_add(s, or_ef_mulf(wts[2 * i + j], M->data[i * M->width + col]));
+                or_ef e = or_ef_mul(s, sj[j]);
+                out[4 * (off + col) + 2 * j] = e.c0;
+                out[4 * (off + col) + 2 * j + 1] = e.c1;
+            }
+        off += M->width;
+    }
+    free(wts);
+    free(q);
+    free(xs);
+}
+
+/* The DEEP quotient (DeepPoly::from_evals + accumulate_matrices,
+ * p3-miden-lifted-fri/src/deep/prover.rs:106-364): columns padded to
+ * `alignment` with zeros; f_red(z_j) = Horner in ac over the padded
+ * evaluations (z_j), coefficients -ac^{W-1-c}; for each LDE point x_i
+ * (bit-reversed), Q = sum_j bp^j (f_red(z_j) - f_red(x_i)) / (z_j - x_i),
+ * rows of shorter matrices read lifted (i >> lift). out: 2 words per point. */
+void or_deep_quotient(const or_matrix *mats, size_t n_mats, unsigned log_blowup, size_t alignment, const or_ef zs[2],
+                      const uint64_t *evals4, or_ef ac, or_ef bp, uint64_t *out) {
+    (void)log_blowup;
+    const size_t n_lde = mats[n_mats - 1].height;
+    const unsigned log_lde = or_log2(n_lde);
+    size_t total_aligned = 0;
+    size_t *aligned_w = (size_t *)malloc(n_mats * sizeof(size_t));
+    for (size_t m = 0; m < n_mats; m++) {
+        aligned_w[m] = (mats[m].width + alignment - 1) / alignment * alignment;
+        total_aligned += aligned_w[m];
+    }
+    or_ef fred[2] = {or_ef_from(0), or_ef_from(0)};
+    size_t src = 0;
+    for (size_t m = 0; m < n_mats; m++)
+        for (size_t c = 0; c < aligned_w[m]; c++) {
+            for (int j = 0; j < 2; j++) {
+                or_ef v = c < mats[m].width ? or_ef_make(evals4[4 * (src + c) + 2 * j], evals4[4 * (src + c) + 2 * j + 1])
+                                            : or_ef_from(0);
+                fred[j] = or_ef_add(or_ef_mul(fred[j], ac), v);
+            }
+            if (c + 1 == aligned_w[m]) src += mats[m].width;
+        }
+    or_ef *coef = (or_ef *)malloc((total_aligned + 1) * sizeof(or_ef));
+    {
+        or_ef p = or_ef_from(OR_P - 1);
+        for (size_t c = total_aligned; c-- > 0;) {
+            coef[c] = p;
+            p = or_ef_mul(p, ac);
+        }
+    }
+    uint64_t wn = or_root(log_lde);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n_lde; i++) {
+        uint64_t x = or_mul(OR_GEN, or_pow(wn, or_bitrev(i, log_lde)));
+        or_ef negf = or_ef_from(0);
+        size_t off = 0;
+        for (size_t m = 0; m < n_mats; m++) {
+            const or_matrix *M = &mats[m];
+            unsigned liftm = log_lde - or_log2(M->height);
+            const uint64_t *row = M->data + (i >> liftm) * M->width;
+            for (size_t col = 0; col < M->width; col++) negf = or_ef_add(negf, or_ef_mulf(coef[off + col], row[col]));
+            off += aligned_w[m];
+        }
+        or_ef q0 = or_ef_inv(or_ef_sub(zs[0], or_ef_from(x))), q1 = or_ef_inv(or_ef_sub(zs[1], or_ef_from(x)));
+        or_ef r = or_ef_mul(q0, or_ef_add(fred[0], negf));
+        r = or_ef_add(r, or_ef_mul(bp, or_ef_mul(q1, or_ef_add(fred[1], negf))));
+        out[2 * i] = r.c0;
+        out[2 * i + 1] = r.c1;
+    }
+    free(coef);
+    free(aligned_w);
+}
+
+/* FriFold::fold_matrix (p3-miden-lifted-fri/src/fri/fold/mod.rs:119-181): a
+ * layer of n = 2^log_n EF values (bit-reversed), rows of a = 2^log_a values;
+ * row k is the coset s*<w_a>, s = w_n^{bitrev_{log n - log a}(k)}. */
+void or_fri_fold(const uint64_t *in, unsigned log_n, unsigned log_a, const uint64_t beta2[2], uint64_t *out) {
+    const size_t a = (size_t)1 << log_a, nf = ((size_t)1 << log_n) / a;
+    const unsigned ls = log_n - log_a;
+    const uint64_t ginv = or_inv(or_root(log_n));
+    const or_ef b = or_ef_make(beta2[0], beta2[1]);
+    or_ef *row = (or_ef *)malloc(a * sizeof(or_ef));
+    for (size_t k = 0; k < nf; k++) {
+        for (size_t t = 0; t < a; t++) row[t] = or_ef_make(in[2 * (k * a + t)], in[2 * (k * a + t) + 1]);
+        or_ef r = fold_row(row, log_a, or_pow(ginv, or_bitrev(k, ls)), b);
+        out[2 * k] = r.c0;
+        out[2 * k + 1] = r.c1;
+    }
+    free(row);
+}
+
 int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
              or_proof *out) {
     memset(out, 0, sizeof(*out));
@@ -351,56 +483,23 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
     const or_matrix *allm[24];
     for (int g = 0; g < 3; g++)
         for (size_t m = 0; m < trees[g]->tree.n_mats; m++) allm[n_mats_total++] = &trees[g]->tree.mats[m];
-    /* coset points gK, bit-reversed */
-    uint64_t *xs = (uint64_t *)malloc(n_lde * 8);
+    size_t total_aligned = 0;
+    for (size_t m = 0; m < n_mats_total; m++) total_aligned += (allm[m]->width + 7) / 8 * 8;
+    or_matrix mats_flat[24];
+    for (size_t m = 0; m < n_mats_total; m++) mats_flat[m] = *allm[m];
+    size_t total_w = 0;
+    for (size_t m = 0; m < n_mats_total; m++) total_w += allm[m]->width;
+    uint64_t *ev4 = (uint64_t *)malloc((total_w + 1) * 32);
+    or_deep_evals(mats_flat, n_mats_total, log_blowup, zs, ev4);
+    /* the aligned flat columns [col][j]: zero beyond each matrix's width */
+    or_ef *evals = (or_ef *)calloc(total_aligned * 2 + 2, sizeof(or_ef));
     {
-        uint64_t wn = or_root(log_lde);
-#pragma omp parallel for schedule(static)
-        for (size_t i = 0; i < n_lde; i++) xs[i] = or_mul(OR_GEN, or_pow(wn, or_bitrev(i, log_lde)));
-    }
-    or_ef *q = (or_ef *)malloc(n_lde * 2 * sizeof(or_ef));
-#pragma omp parallel for schedule(static)
-    for (size_t i = 0; i < n_lde; i++)
-        for (int j = 0; j < 2; j++) q[2 * i + j] = or_ef_inv(or_ef_sub(zs[j], or_ef_from(xs[i])));
-    /* barycentric evaluation of the first d_m rows of each LDE */
-    size_t d = n_lde >> log_blowup;
-    unsigned log_d = or_log2(d);
-    or_ef sj[2];
-    for (int j = 0; j < 2; j++) {
-        or_ef t = or_ef_sub(or_ef_exp2(or_ef_mulf(zs[j], or_inv(OR_GEN)), log_d), or_ef_from(1));
-        sj[j] = or_ef_mulf(t, or_inv((uint64_t)d));
-    }
-    size_t total_aligned = 0, aligned_w[24];
-    for (size_t m = 0; m < n_mats_total; m++) {
-        aligned_w[m] = (allm[m]->width + 7) / 8 * 8;
-        total_aligned += aligned_w[m];
-    }
-    or_ef *evals = (or_ef *)calloc(total_aligned * 2, sizeof(or_ef)); /* [col][j] */
-    {
-        or_ef *wts = (or_ef *)malloc(d * 2 * sizeof(or_ef));
-        size_t off = 0;
+        size_t off = 0, src = 0;
         for (size_t m = 0; m < n_mats_total; m++) {
-            const or_matrix *M = allm[m];
-            size_t dm = M->height >> log_blowup, ratio = d / dm;
-            for (size_t i = 0; i < dm; i++)
-                for (int j = 0; j < 2; j++) {
-                    or_ef s = or_ef_from(0);
-                    for (size_t c = 0; c < ratio; c++) {
-                        size_t ii = i * ratio + c;
-                        s = or_ef_add(s, or_ef_mulf(q[2 * ii + j], xs[ii]));
-                    }
-                    wts[2 * i + j] = s;
-                }
-#pragma omp parallel for schedule(static)
-            for (size_t col = 0; col < M->width; col++)
-                for (int j = 0; j < 2; j++) {
-                    or_ef s = or_ef_from(0);
-                    for (size_t i = 0; i < dm; i++) s = or_ef_add(s, or_ef_mulf(wts[2 * i + j], M->data[i * M->width + col]));
-                    evals[2 * (off + col) + j] = or_ef_mul(s, sj[j]);
-                }
-            off += aligned_w[m];
+            for (size_t col = 0; col < allm[m]->width; col++, src++)
+                for (int j = 0; j < 2; j++) evals[2 * (off + col) + j] = or_ef_make(ev4[4 * src + 2 * j], ev4[4 * src + 2 * j + 1]);
+            off += (allm[m]->width + 7) / 8 * 8;
         }
-        free(wts);
     }
     for (int j = 0; j < 2; j++)
         for (size_t c = 0; c < total_aligned; c++) or_tr_send_ef(&tr, evals[2 * c + j]);
@@ -409,38 +508,10 @@ int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance
     or_ef bp = or_ch_sample_ef(&tr.ch);
     out->deep_alpha[0] = ac.c0, out->deep_alpha[1] = ac.c1;
     out->deep_beta[0] = bp.c0, out->deep_beta[1] = bp.c1;
-    or_ef fred[2] = {or_ef_from(0), or_ef_from(0)};
-    for (size_t c = 0; c < total_aligned; c++)
-        for (int j = 0; j < 2; j++) fred[j] = or_ef_add(or_ef_mul(fred[j], ac), evals[2 * c + j]);
-    /* coefficients -alpha^{W-1-c} */
-    or_ef *coef = (or_ef *)malloc(total_aligned * sizeof(or_ef));
-    {
-        or_ef p = or_ef_from(OR_P - 1);
-        for (size_t c = total_aligned; c-- > 0;) {
-            coef[c] = p;
-            p = or_ef_mul(p, ac);
-        }
-    }
     or_ef *deep = (or_ef *)malloc(n_lde * sizeof(or_ef));
-#pragma omp parallel for schedule(static)
-    for (size_t i = 0; i < n_lde; i++) {
-        or_ef negf = or_ef_from(0);
-        size_t off = 0;
-        for (size_t m = 0; m < n_mats_total; m++) {
-            const or_matrix *M = allm[m];
-            unsigned liftm = log_lde - or_log2(M->height);
-            const uint64_t *row = M->data + (i >> liftm) * M->width;
-            for (size_t col = 0; col < M->width; col++) negf = or_ef_add(negf, or_ef_mulf(coef[off + col], row[col]));
-            off += aligned_w[m];
-        }
-        or_ef r = or_ef_mul(q[2 * i], or_ef_add(fred[0], negf));
-        r = or_ef_add(r, or_ef_mul(bp, or_ef_mul(q[2 * i + 1], or_ef_add(fred[1], negf))));
-        deep[i] = r;
-    }
-    free(coef);
+    or_deep_quotient(mats_flat, n_mats_total, log_blowup, 8, zs, ev4, ac, bp, (uint64_t *)deep);
+    free(ev4);
     free(evals);
-    free(q);
-    free(xs);
     t1 = now_s();
     g_stage[4] = t1 - t0;
     t0 = t1;

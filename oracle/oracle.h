@@ -207,6 +207,10 @@ typedef struct {
 
 int or_prove(const or_p2_params *pp, const or_pcs_params *pcs, const or_instance *inst, size_t n_inst,
              or_proof *out);
+void or_deep_evals(const or_matrix *mats, size_t n_mats, unsigned log_blowup, const or_ef zs[2], uint64_t *out);
+void or_deep_quotient(const or_matrix *mats, size_t n_mats, unsigned log_blowup, size_t alignment, const or_ef zs[2],
+                      const uint64_t *evals4, or_ef ac, or_ef bp, uint64_t *out);
+void or_fri_fold(const uint64_t *in, unsigned log_n, unsigned log_a, const uint64_t beta2[2], uint64_t *out);
 size_t or_inst_aux_width(const or_instance *I);
 size_t or_inst_num_randomness(const or_instance *I);
 size_t or_inst_num_aux_values(const or_instance *I);

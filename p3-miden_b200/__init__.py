@@ -146,6 +146,11 @@ def lib():
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
             "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
                                            C.POINTER(VerifyStatsC)]),
+            "p3g_lmcs_rows": (C.c_int, [vp, vp, C.c_uint64, u64p, C.POINTER(C.c_uint64)]),
+            "p3g_fri_fold": (C.c_int, [vp, C.c_void_p, C.c_uint32, C.c_uint32, u64p, C.c_void_p]),
+            "p3g_deep_evals": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32, u64p, u64p]),
+            "p3g_deep_quotient": (C.c_int, [vp, C.POINTER(C.c_void_p), u64p, u64p, C.c_uint64, C.c_uint32, C.c_uint32,
+                                            u64p, u64p, u64p, u64p, C.c_void_p]),
             "p3g_air_analyse": (C.c_int, [C.POINTER(AirDescC), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "p3g_air_generate_source": (C.c_int, [C.POINTER(AirDescC), C.c_char_p, C.c_uint64,
@@ -305,6 +310,15 @@ class LmcsTree:
         self.ctx.check(lib().p3g_lmcs_layer(self.ctx.handle, self._h, level, _ptr(out)))
         return out
 
+    def rows(self, index: int) -> np.ndarray:
+        """LmcsTree::rows (p3-miden-lmcs/src/lifted_tree.rs:127-138): the row of
+        every matrix at this leaf (lifted), each padded to the alignment."""
+        n = C.c_uint64(0)
+        lib().p3g_lmcs_rows(self.ctx.handle, self._h, index, _ptr(np.zeros(1, dtype=np.uint64)), C.byref(n))
+        out = np.zeros(max(1, n.value), dtype=np.uint64)
+        self.ctx.check(lib().p3g_lmcs_rows(self.ctx.handle, self._h, index, _ptr(out), C.byref(n)))
+        return out[:n.value]
+
     def prove_batch(self, indices):
         idx = np.array(sorted(set(int(i) for i in indices)), dtype=np.uint64)
         cap_f = len(idx) * (sum(((m.shape[1] + 7) // 8) * 8 for m in self._keep) + self.salt_width) + 16
@@ -339,6 +353,56 @@ class LmcsTree:
                 lib().p3g_lmcs_free(self._h)
         except Exception:
             pass
+
+
+def fri_fold(ctx: Context, layer_dev, log_arity: int, beta) -> object:
+    """FriFold::fold_matrix (p3-miden-lifted-fri/src/fri/fold/mod.rs:119-181) of a
+    bit-reversed layer of n EF values (device tensor n x 2) with challenge beta
+    (c0, c1): the n / 2^log_arity folded values."""
+    n = layer_dev.shape[0]
+    log_n = n.bit_length() - 1
+    assert n == 1 << log_n and layer_dev.shape[1] == 2
+    out = empty_device((n >> log_arity, 2), ctx.device)
+    b = np.array(beta, dtype=np.uint64)
+    import torch
+    torch.cuda.synchronize(ctx.device)
+    ctx.check(lib().p3g_fri_fold(ctx.handle, layer_dev.data_ptr(), log_n, log_arity, _ptr(b), out.data_ptr()))
+    return out
+
+
+def _mat_args(mats_dev):
+    ptrs = (C.c_void_p * len(mats_dev))(*[m.data_ptr() for m in mats_dev])
+    hs = np.array([m.shape[0] for m in mats_dev], dtype=np.uint64)
+    ws = np.array([m.shape[1] for m in mats_dev], dtype=np.uint64)
+    return ptrs, hs, ws
+
+
+def deep_evals(ctx: Context, mats_dev, log_blowup: int, zs) -> np.ndarray:
+    """DEEP openings: f(z_0), f(z_1) of every column of the committed
+    (bit-reversed LDE) matrices, ascending heights; (total columns, 2 points, 2)."""
+    import torch
+    torch.cuda.synchronize(ctx.device)
+    ptrs, hs, ws = _mat_args(mats_dev)
+    z = np.array([zs[0][0], zs[0][1], zs[1][0], zs[1][1]], dtype=np.uint64)
+    out = np.zeros(4 * int(ws.sum()), dtype=np.uint64)
+    ctx.check(lib().p3g_deep_evals(ctx.handle, ptrs, _ptr(hs), _ptr(ws), len(mats_dev), log_blowup, _ptr(z), _ptr(out)))
+    return out.reshape(-1, 2, 2)
+
+
+def deep_quotient(ctx: Context, mats_dev, log_blowup: int, alignment: int, zs, evals, alpha, beta):
+    """The DEEP quotient over the committed matrices (n EF on the LDE domain,
+    bit-reversed; device tensor n x 2)."""
+    import torch
+    torch.cuda.synchronize(ctx.device)
+    ptrs, hs, ws = _mat_args(mats_dev)
+    z = np.array([zs[0][0], zs[0][1], zs[1][0], zs[1][1]], dtype=np.uint64)
+    ev = np.ascontiguousarray(evals, dtype=np.uint64).reshape(-1)
+    a = np.array(alpha, dtype=np.uint64)
+    b = np.array(beta, dtype=np.uint64)
+    out = empty_device((int(hs[-1]), 2), ctx.device)
+    ctx.check(lib().p3g_deep_quotient(ctx.handle, ptrs, _ptr(hs), _ptr(ws), len(mats_dev), log_blowup, alignment,
+                                      _ptr(z), _ptr(ev), _ptr(a), _ptr(b), out.data_ptr()))
+    return out
 
 
 def poseidon2_permute_batch(ctx: Context, states_dev):

@@ -328,6 +328,140 @@ P3G_API int p3g_lmcs_prove_batch(p3g_ctx *x, const p3g_tree *t, const uint64_t *
     })
 }
 
+// LmcsTree::rows (p3-miden-lmcs/src/lifted_tree.rs:127-138): the row of each
+// committed matrix at leaf `index` (lifted: row index >> log2(H / h)), each
+// padded with zeros to the tree's alignment, concatenated into out; *n_words
+// is the capacity on entry and the count on return.
+P3G_API int p3g_lmcs_rows(p3g_ctx *x, const p3g_tree *t, uint64_t index, uint64_t *out, uint64_t *n_words) {
+    if (!x || !t || !out || !n_words || index >= t->t.H) return p3g::ERR_INVALID;
+    uint64_t need = 0;
+    for (const p3g::Mat &m : t->t.mats) need += (m.w + t->t.alignment - 1) / t->t.alignment * t->t.alignment;
+    if (need > *n_words) {
+        *n_words = need;
+        return p3g::ERR_INVALID;
+    }
+    P3G_TRY(x, {
+        uint64_t off = 0;
+        for (const p3g::Mat &m : t->t.mats) {
+            const uint64_t r = index >> (t->t.depth - p3g::log2u(m.h));
+            const uint64_t pad = (m.w + t->t.alignment - 1) / t->t.alignment * t->t.alignment;
+            CK(cudaMemcpyAsync(out + off, m.d + r * m.w, m.w * 8, cudaMemcpyDeviceToHost, x->c.stream));
+            for (uint64_t k = m.w; k < pad; k++) out[off + k] = 0;
+            off += pad;
+        }
+        x->c.sync();
+        *n_words = off;
+    })
+}
+
+// FriFold::fold_matrix (p3-miden-lifted-fri/src/fri/fold/mod.rs:119-181,
+// arity{2,4,8}.rs): d_in holds n = 2^log_n EF values of a FRI layer in
+// bit-reversed order; row k (its 2^log_arity consecutive values) is the coset
+// s*<w_a> with s = w_n^{bitrev(k)}, and folds with beta to
+// (1/a) sum_j (beta/s)^j sum_t y_t w_a^{-jt} in d_out[k] (n / a EF). The
+// layer's commitment is p3g_lmcs_build of d_in viewed as (n/a) x 2a with
+// alignment 1 (fri/prover.rs:143-150).
+P3G_API int p3g_fri_fold(p3g_ctx *x, const uint64_t *d_in, uint32_t log_n, uint32_t log_arity, const uint64_t *beta2,
+                         uint64_t *d_out) {
+    if (!x || !d_in || !d_out || !beta2 || log_arity < 1 || log_arity > 3 || log_n < log_arity || log_n > 32 ||
+        beta2[0] >= gl::P || beta2[1] >= gl::P)
+        return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        const p3g::TwTables &tw = x->c.twiddles(log_n);
+        fri::FoldArgs fa{};
+        fa.in = d_in;
+        fa.n_out = 1ull << (log_n - log_arity);
+        fa.log_a = log_arity;
+        fa.log_nin = log_n;
+        fa.log_n0 = log_n;
+        fa.w0inv = ntt::PowTab{tw.inv_lo.p, tw.inv_hi.p, tw.lo_bits};
+        fa.beta = gl::ef{beta2[0], beta2[1]};
+        fa.beta_dev = nullptr;
+        const uint64_t wi = gl::inv(gl::root(log_arity));
+        uint64_t w = 1;
+        for (int i = 0; i < 8; i++) fa.winv_a[i] = w, w = gl::mul(w, wi);
+        fa.inv_a = gl::inv(1ull << log_arity);
+        fa.out = d_out;
+        fa.digests = nullptr;
+        const uint64_t threads = (fa.n_out + (1ull << log_arity) - 1) >> log_arity;
+        fri::fold_hash_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, x->c.stream>>>(fa);
+        CK(cudaGetLastError());
+        x->c.launches++;
+        x->c.sync();
+    })
+}
+
+// DEEP, the openings at the two out-of-domain points z_0, z_1
+// (PointQuotients::new, p3-miden-lifted-fri/src/deep/interpolate.rs:81-109,
+// and batch_eval_lifted, :123-201) over committed matrices: bit-reversed LDEs
+// on g*K (heights h_m = the LDE heights, ascending; the largest is the LDE
+// domain), log_blowup B. evals_out (host) receives 4 words per column, matrix
+// by matrix: f(z_0) (c0, c1), f(z_1) (c0, c1).
+P3G_API int p3g_deep_evals(p3g_ctx *x, const uint64_t *const *d_mats, const uint64_t *heights, const uint64_t *widths,
+                           uint64_t n_mats, uint32_t log_blowup, const uint64_t *z4, uint64_t *evals_out) {
+    if (!x || !d_mats || !heights || !widths || !z4 || !evals_out || n_mats == 0 || n_mats > 64 || log_blowup > 8)
+        return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n_mats; i++)
+        if (heights[i] == 0 || (heights[i] & (heights[i] - 1)) || (i && heights[i] < heights[i - 1]) ||
+            (heights[i] >> log_blowup) == 0 || !d_mats[i] || widths[i] == 0)
+            return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<p3g::Mat> mats;
+        std::vector<const p3g::Mat *> all;
+        for (uint64_t i = 0; i < n_mats; i++) mats.push_back({d_mats[i], heights[i], widths[i]});
+        for (auto &m : mats) all.push_back(&m);
+        const gl::ef zs[2] = {gl::ef{z4[0], z4[1]}, gl::ef{z4[2], z4[3]}};
+        p3g::Launcher L{x->c};
+        p3g::DeepOpen st;
+        std::vector<uint64_t> ev = p3g::deep_evals(x->c, L, all, log_blowup, p3g::log2u(heights[n_mats - 1]), zs, 1,
+                                                   st, nullptr);
+        memcpy(evals_out, ev.data(), ev.size() * 8);
+        x->c.launches += L.n;
+    })
+}
+
+// DEEP, the quotient polynomial (DeepPoly::from_evals + accumulate_matrices,
+// p3-miden-lifted-fri/src/deep/prover.rs:106-364): with evals from
+// p3g_deep_evals, the column challenge alpha2 and the point challenge beta2,
+// the reduced openings f_red(z_j) and coefficients -alpha^{W-1-c} run over
+// the columns padded to `alignment` (the LMCS alignment; padding columns are
+// zero), and d_out receives Q(x) = sum_j beta^j (f_red(z_j) - f_red(x)) /
+// (z_j - x) on the LDE domain, bit-reversed (n EF, n = the largest height).
+P3G_API int p3g_deep_quotient(p3g_ctx *x, const uint64_t *const *d_mats, const uint64_t *heights,
+                              const uint64_t *widths, uint64_t n_mats, uint32_t log_blowup, uint32_t alignment,
+                              const uint64_t *z4, const uint64_t *evals, const uint64_t *alpha2,
+                              const uint64_t *beta2, uint64_t *d_out) {
+    if (!x || !d_mats || !heights || !widths || !z4 || !evals || !alpha2 || !beta2 || !d_out || n_mats == 0 ||
+        n_mats > 16 || log_blowup > 8 || alignment == 0 || alignment > 64)
+        return p3g::ERR_INVALID;
+    for (uint64_t i = 0; i < n_mats; i++)
+        if (heights[i] == 0 || (heights[i] & (heights[i] - 1)) || (i && heights[i] < heights[i - 1]) ||
+            (heights[i] >> log_blowup) == 0 || !d_mats[i] || widths[i] == 0)
+            return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<p3g::Mat> mats;
+        std::vector<const p3g::Mat *> all;
+        uint64_t total_w = 0;
+        for (uint64_t i = 0; i < n_mats; i++) mats.push_back({d_mats[i], heights[i], widths[i]}), total_w += widths[i];
+        for (auto &m : mats) all.push_back(&m);
+        const gl::ef zs[2] = {gl::ef{z4[0], z4[1]}, gl::ef{z4[2], z4[3]}};
+        const uint32_t log_lde = p3g::log2u(heights[n_mats - 1]);
+        p3g::Launcher L{x->c};
+        p3g::DeepOpen st;
+        // the point quotients and weights of the opening, then the assembly
+        (void)p3g::deep_evals(x->c, L, all, log_blowup, log_lde, zs, alignment, st, nullptr);
+        std::vector<uint64_t> ev(evals, evals + 4 * total_w);
+        p3g::DBuf layer = p3g::deep_assemble(x->c, L, all, log_lde, ev, gl::ef{alpha2[0], alpha2[1]},
+                                             gl::ef{beta2[0], beta2[1]}, st);
+        CK(cudaMemcpyAsync(d_out, layer.p, (2ull << log_lde) * 8, cudaMemcpyDeviceToDevice, x->c.stream));
+        x->c.sync();
+        x->c.launches += L.n;
+    })
+}
+
 // ------------------------------------------------------------ symbolic AIRs
 struct p3g_sym_node_c {
     uint32_t op, a, b, pad;

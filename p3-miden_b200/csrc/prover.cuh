@@ -353,6 +353,160 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde,
     ctx.sync();  // keep the constant block and the periodic table alive until the kernel ran
 }
 
+// DEEP, the opening at the two out-of-domain points: PointQuotients::new
+// (p3-miden-lifted-fri/src/deep/interpolate.rs:81-109) and batch_eval_lifted
+// (:123-201). Returns f(z_j) of every column of every matrix (in order), 4
+// words per column: z_0 (c0, c1), z_1 (c0, c1). `st` keeps the point
+// quotients and weights for deep_assemble, and the aligned widths.
+struct DeepOpen {
+    DBuf q;
+    std::map<uint64_t, DBuf> weights;
+    std::vector<uint64_t> aligned_w;
+    uint64_t total_aligned = 0;
+};
+inline std::vector<uint64_t> deep_evals(Ctx &ctx, Launcher &L, const std::vector<const Mat *> &all, uint32_t lb,
+                                        uint32_t log_lde, const gl::ef zs[2], uint32_t alignment, DeepOpen &st,
+                                        uint64_t *d2h) {
+    const TwTables &twn = ctx.twiddles(log_lde);
+    const uint64_t n = 1ull << log_lde;
+    const uint64_t ginv = gl::inv(gl::GEN);
+    st.q = ctx.alloc(4 * n);
+    DBuf &q = st.q;
+    {
+        deep::PQArgs a{};
+        a.n = n;
+        a.log_n = log_lde;
+        a.wn = ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits};
+        a.z[0] = zs[0];
+        a.z[1] = zs[1];
+        a.q = q.p;
+        L(deep::point_quotients_kernel, blocks_for((n + deep::CHUNK - 1) / deep::CHUNK, 128), 128, 0, a);
+    }
+    const uint64_t d = n >> lb;
+    const uint32_t log_d = log2u(d);
+    std::map<uint64_t, DBuf> &weights = st.weights;
+    weights[d] = ctx.alloc(4 * d);
+    L(deep::top_weights_kernel, blocks_for(d, 256), 256, 0, q.p, d, log_lde,
+      ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits}, weights[d].p);
+    for (const Mat *m : all) {
+        uint64_t dm = m->h >> lb;
+        if (weights.count(dm)) continue;
+        weights[dm] = ctx.alloc(4 * dm);
+        L(deep::fold_weights_kernel, blocks_for(dm, 256), 256, 0, weights[d].p, dm, d / dm, weights[dm].p);
+    }
+    gl::ef sj[2];
+    for (int j = 0; j < 2; j++) {
+        gl::ef t = gl::ef_sub(gl::ef_exp2k(gl::ef_mulf(zs[j], ginv), log_d), gl::ef_one());
+        sj[j] = gl::ef_mulf(t, gl::inv(d % gl::P));
+    }
+    std::vector<uint64_t> &aligned_w = st.aligned_w;
+    uint64_t total_w = 0;
+    for (const Mat *m : all) {
+        aligned_w.push_back((m->w + alignment - 1) / alignment * alignment);
+        st.total_aligned += aligned_w.back();
+        total_w += m->w;
+    }
+    DBuf evals = ctx.alloc(4 * total_w);
+    {
+        uint64_t off = 0;
+        for (const Mat *m : all) {
+            uint64_t dm = m->h >> lb;
+            uint64_t col_tiles = (m->w + 31) / 32;
+            uint64_t target_blocks = 4 * 148;
+            uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, (target_blocks + col_tiles - 1) / col_tiles));
+            uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
+            n_chunks = (dm + rpc - 1) / rpc;
+            DBuf part = ctx.alloc(n_chunks * m->w * 4);
+            L(deep::colsum_kernel, dim3((unsigned)col_tiles, (unsigned)n_chunks), 256, 0, m->d, m->w, dm,
+              weights[dm].p, rpc, part.p);
+            L(deep::colsum_finish_kernel, blocks_for(m->w, 128), 128, 0, part.p, n_chunks, m->w, sj[0], sj[1],
+              evals.p + 4 * off);
+            off += m->w;
+        }
+    }
+    std::vector<uint64_t> h_evals(4 * total_w);
+    ctx.d2h(h_evals.data(), evals.p, 4 * total_w);
+    ctx.sync();
+    if (d2h) *d2h += 32 * total_w;
+    return h_evals;
+}
+
+// DEEP, the quotient: DeepPoly::from_evals and accumulate_matrices
+// (p3-miden-lifted-fri/src/deep/prover.rs:106-364) with the column challenge
+// ac and the point challenge bp: the reduced openings f_red(z_j), coefficients
+// -ac^{W-1-c} over the aligned columns, one row dot product per matrix
+// (read lifted), and Q(x) = sum_j bp^j (f_red(z_j) - f_red(x)) / (z_j - x).
+// Returns the n EF values of Q on the LDE domain (bit-reversed).
+inline DBuf deep_assemble(Ctx &ctx, Launcher &L, const std::vector<const Mat *> &all, uint32_t log_lde,
+                          const std::vector<uint64_t> &h_evals, gl::ef ac, gl::ef bp, DeepOpen &st) {
+    const std::vector<uint64_t> &aligned_w_ = st.aligned_w;
+    gl::ef fred[2] = {gl::ef_zero(), gl::ef_zero()};
+    {
+        uint64_t off = 0;
+        for (size_t mi = 0; mi < all.size(); mi++) {
+            for (uint64_t c = 0; c < aligned_w_[mi]; c++)
+                for (int j = 0; j < 2; j++) {
+                    gl::ef v = c < all[mi]->w ? gl::ef{h_evals[4 * (off + c) + 2 * j], h_evals[4 * (off + c) + 2 * j + 1]}
+                                              : gl::ef_zero();
+                    fred[j] = gl::ef_add(gl::ef_mul(fred[j], ac), v);
+                }
+            off += all[mi]->w;
+        }
+    }
+    // coefficients -alpha^{W-1-c} over the aligned flat columns
+    const uint64_t total_aligned = st.total_aligned, n = 1ull << log_lde;
+    const std::vector<uint64_t> &aligned_w = st.aligned_w;
+    DBuf &q = st.q;
+    std::map<uint64_t, DBuf> &weights = st.weights;
+    std::vector<uint64_t> coef(2 * total_aligned);
+    {
+        gl::ef p = gl::ef{gl::P - 1, 0};
+        for (uint64_t c = total_aligned; c-- > 0;) {
+            coef[2 * c] = p.c0, coef[2 * c + 1] = p.c1;
+            p = gl::ef_mul(p, ac);
+        }
+    }
+    DBuf d_coef = ctx.upload(coef);
+    std::vector<DBuf> dots(all.size());
+    deep::AssembleArgs aa{};
+    {
+        uint64_t off = 0;
+        for (size_t mi = 0; mi < all.size(); mi++) {
+            const Mat *m = all[mi];
+            dots[mi] = ctx.alloc(2 * m->h);
+            const uint64_t *cf = d_coef.p + 2 * off;
+            if (m->w >= 16) {
+                size_t smem = 16 * m->w;
+                static std::once_flag attr_once;
+                std::call_once(attr_once, [] {
+                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            200 * 1024));
+                });
+                unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(m->h * 32, 256), 148 * 16);
+                L(deep::rowdot_warp_kernel, grid, 256, smem, m->d, m->h, m->w, cf, dots[mi].p);
+            } else {
+                L(deep::rowdot_thread_kernel, blocks_for(m->h, 256), 256, 0, m->d, m->h, m->w, cf, dots[mi].p);
+            }
+            aa.dots[mi] = dots[mi].p;
+            aa.lift[mi] = log_lde - log2u(m->h);
+            off += aligned_w[mi];
+        }
+    }
+    aa.n_dots = (int)all.size();
+    aa.q = q.p;
+    aa.n = n;
+    aa.fred[0] = fred[0];
+    aa.fred[1] = fred[1];
+    aa.beta = bp;
+    DBuf layer = ctx.alloc(2 * n);
+    aa.out = layer.p;
+    L(deep::assemble_kernel, blocks_for(n, 256), 256, 0, aa);
+    q.release();
+    weights.clear();
+    dots.clear();
+    return layer;
+}
+
 inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n_inst, ProofOut &po) {
     using clk = std::chrono::steady_clock;
     Launcher L{ctx};
@@ -550,64 +704,9 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     for (auto &m : main_tree.mats) all.push_back(&m);
     for (auto &m : aux_tree.mats) all.push_back(&m);
     for (auto &m : quot_tree.mats) all.push_back(&m);
-    const TwTables &twn = ctx.twiddles(log_lde);
-    DBuf q = ctx.alloc(4 * n);
-    {
-        deep::PQArgs a{};
-        a.n = n;
-        a.log_n = log_lde;
-        a.wn = ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits};
-        a.z[0] = zs[0];
-        a.z[1] = zs[1];
-        a.q = q.p;
-        L(deep::point_quotients_kernel, blocks_for((n + deep::CHUNK - 1) / deep::CHUNK, 128), 128, 0, a);
-    }
-    const uint64_t d = n >> lb;
-    const uint32_t log_d = log2u(d);
-    std::map<uint64_t, DBuf> weights;
-    weights[d] = ctx.alloc(4 * d);
-    L(deep::top_weights_kernel, blocks_for(d, 256), 256, 0, q.p, d, log_lde,
-      ntt::PowTab{twn.fwd_lo.p, twn.fwd_hi.p, twn.lo_bits}, weights[d].p);
-    for (const Mat *m : all) {
-        uint64_t dm = m->h >> lb;
-        if (weights.count(dm)) continue;
-        weights[dm] = ctx.alloc(4 * dm);
-        L(deep::fold_weights_kernel, blocks_for(dm, 256), 256, 0, weights[d].p, dm, d / dm, weights[dm].p);
-    }
-    gl::ef sj[2];
-    for (int j = 0; j < 2; j++) {
-        gl::ef t = gl::ef_sub(gl::ef_exp2k(gl::ef_mulf(zs[j], ginv), log_d), gl::ef_one());
-        sj[j] = gl::ef_mulf(t, gl::inv(d % gl::P));
-    }
-    std::vector<uint64_t> aligned_w;
-    uint64_t total_aligned = 0, total_w = 0;
-    for (const Mat *m : all) {
-        aligned_w.push_back((m->w + 7) / 8 * 8);
-        total_aligned += aligned_w.back();
-        total_w += m->w;
-    }
-    DBuf evals = ctx.alloc(4 * total_w);
-    {
-        uint64_t off = 0;
-        for (const Mat *m : all) {
-            uint64_t dm = m->h >> lb;
-            uint64_t col_tiles = (m->w + 31) / 32;
-            uint64_t target_blocks = 4 * 148;
-            uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, (target_blocks + col_tiles - 1) / col_tiles));
-            uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
-            n_chunks = (dm + rpc - 1) / rpc;
-            DBuf part = ctx.alloc(n_chunks * m->w * 4);
-            L(deep::colsum_kernel, dim3((unsigned)col_tiles, (unsigned)n_chunks), 256, 0, m->d, m->w, dm,
-              weights[dm].p, rpc, part.p);
-            L(deep::colsum_finish_kernel, blocks_for(m->w, 128), 128, 0, part.p, n_chunks, m->w, sj[0], sj[1],
-              evals.p + 4 * off);
-            off += m->w;
-        }
-    }
-    std::vector<uint64_t> h_evals(4 * total_w);
-    ctx.d2h(h_evals.data(), evals.p, 4 * total_w);
-    ctx.sync();
-    po.d2h += 32 * total_w;
+    DeepOpen dopen;
+    std::vector<uint64_t> h_evals = deep_evals(ctx, L, all, lb, log_lde, zs, 8, dopen, &po.d2h);
+    const std::vector<uint64_t> &aligned_w = dopen.aligned_w;
     // send aligned evals per point (deep/prover.rs:271-277)
     for (int j = 0; j < 2; j++) {
         uint64_t off = 0;
@@ -653,66 +752,8 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     grind(pcs.deep_pow_bits);
     const gl::ef ac = tr.ch.sample_ef();
     const gl::ef bp = tr.ch.sample_ef();
-    gl::ef fred[2] = {gl::ef_zero(), gl::ef_zero()};
-    {
-        uint64_t off = 0;
-        for (size_t mi = 0; mi < all.size(); mi++) {
-            for (uint64_t c = 0; c < aligned_w[mi]; c++)
-                for (int j = 0; j < 2; j++) {
-                    gl::ef v = c < all[mi]->w ? gl::ef{h_evals[4 * (off + c) + 2 * j], h_evals[4 * (off + c) + 2 * j + 1]}
-                                              : gl::ef_zero();
-                    fred[j] = gl::ef_add(gl::ef_mul(fred[j], ac), v);
-                }
-            off += all[mi]->w;
-        }
-    }
-    // coefficients -alpha^{W-1-c} over the aligned flat columns
-    std::vector<uint64_t> coef(2 * total_aligned);
-    {
-        gl::ef p = gl::ef{gl::P - 1, 0};
-        for (uint64_t c = total_aligned; c-- > 0;) {
-            coef[2 * c] = p.c0, coef[2 * c + 1] = p.c1;
-            p = gl::ef_mul(p, ac);
-        }
-    }
-    DBuf d_coef = ctx.upload(coef);
-    std::vector<DBuf> dots(all.size());
-    deep::AssembleArgs aa{};
-    {
-        uint64_t off = 0;
-        for (size_t mi = 0; mi < all.size(); mi++) {
-            const Mat *m = all[mi];
-            dots[mi] = ctx.alloc(2 * m->h);
-            const uint64_t *cf = d_coef.p + 2 * off;
-            if (m->w >= 16) {
-                size_t smem = 16 * m->w;
-                static std::once_flag attr_once;
-                std::call_once(attr_once, [] {
-                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            200 * 1024));
-                });
-                unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(m->h * 32, 256), 148 * 16);
-                L(deep::rowdot_warp_kernel, grid, 256, smem, m->d, m->h, m->w, cf, dots[mi].p);
-            } else {
-                L(deep::rowdot_thread_kernel, blocks_for(m->h, 256), 256, 0, m->d, m->h, m->w, cf, dots[mi].p);
-            }
-            aa.dots[mi] = dots[mi].p;
-            aa.lift[mi] = log_lde - log2u(m->h);
-            off += aligned_w[mi];
-        }
-    }
-    aa.n_dots = (int)all.size();
-    aa.q = q.p;
-    aa.n = n;
-    aa.fred[0] = fred[0];
-    aa.fred[1] = fred[1];
-    aa.beta = bp;
-    DBuf layer = ctx.alloc(2 * n);
-    aa.out = layer.p;
-    L(deep::assemble_kernel, blocks_for(n, 256), 256, 0, aa);
-    q.release();
-    weights.clear();
-    dots.clear();
+    DBuf layer = deep_assemble(ctx, L, all, log_lde, h_evals, ac, bp, dopen);
+    dopen = DeepOpen();
     CK(cudaEventRecord(ev[6], ctx.stream));
 
     // ---- FRI commit phase

@@ -35,6 +35,10 @@ AUX_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_
                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
 
 
+class EF(C.Structure):
+    _fields_ = [("c0", C.c_uint64), ("c1", C.c_uint64)]
+
+
 class SymAir(C.Structure):
     _fields_ = [("main_width", C.c_uint32), ("aux_width", C.c_uint32), ("num_randomness", C.c_uint32),
                 ("num_aux_values", C.c_uint32), ("num_public_values", C.c_uint32), ("num_periodic", C.c_uint32),
@@ -148,6 +152,10 @@ def lib():
             ("or_verify", C.c_int, [C.POINTER(P2Params), C.POINTER(PcsParams), C.POINTER(Instance), C.c_size_t,
                                     u64p, C.c_size_t, u64p, C.c_size_t, u64p]),
             ("or_sym_validate", C.c_int, [C.POINTER(SymAir)]),
+            ("or_deep_evals", None, [C.POINTER(Matrix), C.c_size_t, C.c_uint, u64p, u64p]),
+            ("or_deep_quotient", None, [C.POINTER(Matrix), C.c_size_t, C.c_uint, C.c_size_t, u64p, u64p,
+                                        EF, EF, u64p]),
+            ("or_fri_fold", None, [u64p, C.c_uint, C.c_uint, u64p, u64p]),
             ("or_sym_max_degree", C.c_uint, [C.POINTER(SymAir)]),
             ("or_sym_log_quotient_degree", C.c_uint, [C.POINTER(SymAir)]),
         ]:
@@ -388,6 +396,44 @@ def verify(pp: P2Params, pcs: dict, instances, fields, commits, digest) -> int:
     pr = PcsParams(**pcs)
     return int(lib().or_verify(C.byref(pp), C.byref(pr), arr, len(instances), ptr(f), f.size,
                                ptr(cm) if cm.size else ptr(dummy), cm.size // 4, ptr(d)))
+
+
+def _mats(mats, keep):
+    arr = (Matrix * len(mats))()
+    for i, m in enumerate(mats):
+        a = np.ascontiguousarray(m, dtype=np.uint64)
+        keep.append(a)
+        arr[i] = Matrix(ptr(a), a.shape[0], a.shape[1])
+    return arr
+
+
+def deep_evals(mats, log_blowup: int, zs) -> np.ndarray:
+    """or_deep_evals: (total columns, 2 points, 2 words)."""
+    keep = []
+    arr = _mats(mats, keep)
+    z = np.array([zs[0][0], zs[0][1], zs[1][0], zs[1][1]], dtype=np.uint64)
+    out = np.zeros(4 * sum(m.shape[1] for m in mats), dtype=np.uint64)
+    lib().or_deep_evals(arr, len(mats), log_blowup, ptr(z), ptr(out))
+    return out.reshape(-1, 2, 2)
+
+
+def deep_quotient(mats, log_blowup: int, alignment: int, zs, evals, alpha, beta) -> np.ndarray:
+    keep = []
+    arr = _mats(mats, keep)
+    z = np.array([zs[0][0], zs[0][1], zs[1][0], zs[1][1]], dtype=np.uint64)
+    ev = np.ascontiguousarray(evals, dtype=np.uint64).reshape(-1)
+    out = np.zeros((mats[-1].shape[0], 2), dtype=np.uint64)
+    lib().or_deep_quotient(arr, len(mats), log_blowup, alignment, ptr(z), ptr(ev), EF(*alpha), EF(*beta), ptr(out))
+    return out
+
+
+def fri_fold(layer: np.ndarray, log_arity: int, beta) -> np.ndarray:
+    l = np.ascontiguousarray(layer, dtype=np.uint64)
+    n = l.shape[0]
+    out = np.zeros((n >> log_arity, 2), dtype=np.uint64)
+    b = np.array(beta, dtype=np.uint64)
+    lib().or_fri_fold(ptr(l), n.bit_length() - 1, log_arity, ptr(b), ptr(out))
+    return out
 
 
 def set_threads(n: int):

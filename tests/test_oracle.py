@@ -241,3 +241,42 @@ def test_hiding_tree_is_one_more_absorb():
     f, c = hid.prove_batch([3, 9])
     assert f.size == 2 * (8 + 8 + 16 + 5)
     assert np.array_equal(f[8 + 8 + 16:8 + 8 + 16 + 5], salt[3])
+
+
+def test_deep_evals_are_polynomial_evaluations():
+    """The oracle's batch_eval_lifted restatement returns p(z) for the
+    polynomial p interpolating each trace column on the trace domain, also
+    for a lifted (shorter) matrix, which reads z^(lift ratio)."""
+    import sym_airs as S
+    rng = np.random.default_rng(3)
+    lb = 2
+    t_small, t_big = rng.integers(0, O.P, size=(8, 2), dtype=np.uint64), rng.integers(0, O.P, size=(32, 3), dtype=np.uint64)
+    mats = [O.coset_lde_bitrev(t_small, lb, pow(7, 4, O.P)), O.coset_lde_bitrev(t_big, lb, 7)]
+    z = (int(rng.integers(0, O.P, dtype=np.uint64)), int(rng.integers(0, O.P, dtype=np.uint64)))
+    w = pow(7, (O.P - 1) // 32, O.P)
+    zs = [z, (z[0] * w % O.P, z[1] * w % O.P)]
+    ev = O.deep_evals(mats, lb, zs)
+
+    def ef_pow(a, e):
+        r = (1, 0)
+        while e:
+            if e & 1:
+                r = S.ef_mul(r, a)
+            a = S.ef_mul(a, a)
+            e >>= 1
+        return r
+
+    def poly_at(col, x):
+        c = np.ascontiguousarray(col, dtype=np.uint64).copy()
+        O.lib().or_intt(O.ptr(c), c.size)
+        acc = (0, 0)
+        for k in reversed(range(c.size)):
+            acc = S.ef_add(S.ef_mul(acc, x), (int(c[k]), 0))
+        return acc
+
+    k = 0
+    for t, ratio in ((t_small, 4), (t_big, 1)):
+        for col in range(t.shape[1]):
+            for j in range(2):
+                assert tuple(int(v) for v in ev[k, j]) == poly_at(t[:, col], ef_pow(zs[j], ratio)), (k, j)
+            k += 1
