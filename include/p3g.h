@@ -47,7 +47,7 @@ enum p3g_air {
 
 typedef struct p3g_ctx p3g_ctx;
 typedef struct p3g_tree p3g_tree;
-typedef struct p3g_air p3g_air;
+typedef struct p3g_sym_air p3g_sym_air;
 
 /* ------------------------------------------------------- symbolic AIRs
  * LiftedAir (p3-miden-lifted-air/src/air.rs:42-319) through its symbolic
@@ -89,14 +89,14 @@ typedef struct {
  * (constraints/layout.rs:27-37), generates the constraint kernel for gJ
  * (constraints/mod.rs:63-179) and compiles it with NVRTC for the context's
  * device. P3G_ERR_VALIDATION for a malformed DAG (p3g_last_error says why). */
-int p3g_air_create(p3g_ctx *ctx, const p3g_air_desc *desc, p3g_air **out);
-void p3g_air_free(p3g_air *air);
-uint32_t p3g_air_log_quotient_degree(const p3g_air *air);
-uint32_t p3g_air_max_degree(const p3g_air *air);
-uint64_t p3g_air_num_constraints_of(const p3g_air *air);
+int p3g_air_create(p3g_ctx *ctx, const p3g_air_desc *desc, p3g_sym_air **out);
+void p3g_air_free(p3g_sym_air *air);
+uint32_t p3g_air_log_quotient_degree(const p3g_sym_air *air);
+uint32_t p3g_air_max_degree(const p3g_sym_air *air);
+uint64_t p3g_air_num_constraints_of(const p3g_sym_air *air);
 /* ConstraintLayout: base_indices / ext_indices; *n_base and *n_ext are
  * capacities on entry and counts on return. */
-int p3g_air_layout(const p3g_air *air, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext);
+int p3g_air_layout(const p3g_sym_air *air, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext);
 /* No device needed: the analysis, the generated kernel source (*len = size
  * with the terminating zero), and an NVRTC compile for sm_<cc>a. */
 int p3g_air_analyse(const p3g_air_desc *desc, uint32_t *max_degree, uint32_t *log_quotient_degree,
@@ -133,7 +133,7 @@ typedef struct {
     const uint64_t *trace;   /* row-major height x width */
     const uint64_t *consts;  /* host; cubic AIR: k[width]; Keccak: NULL */
     uint64_t n_consts;
-    const p3g_air *sym;      /* P3G_AIR_SYMBOLIC: the compiled AIR */
+    const p3g_sym_air *sym;      /* P3G_AIR_SYMBOLIC: the compiled AIR */
     const uint64_t *public_values; /* AirWitness::public_values (host) */
     uint64_t n_public_values;
     /* The instance's AuxBuilder; NULL: an all-zero aux trace (the examples'

@@ -12,7 +12,7 @@ struct p3g_pcs_params_c {
     uint32_t log_blowup, log_folding_arity, log_final_degree;
     uint32_t folding_pow_bits, deep_pow_bits, num_queries, query_pow_bits;
 };
-struct p3g_air {
+struct p3g_sym_air {
     sym::Air a;
 };
 struct p3g_instance_c {
@@ -22,7 +22,7 @@ struct p3g_instance_c {
     const uint64_t *trace;
     const uint64_t *consts;
     uint64_t n_consts;
-    const p3g_air *sym;
+    const p3g_sym_air *sym;
     const uint64_t *public_values;
     uint64_t n_public_values;
     p3g::AuxFn aux_build;
@@ -541,19 +541,22 @@ P3G_API int p3g_air_compile_check(const p3g_air_desc_c *desc, int32_t cc, uint64
     if (int v = p3g::desc_from_c(desc, A.d, why)) return v;
     try {
         sym::analyse(A);
-        A.source = sym::generate(A);
-        sym::nvrtc_cubin(A.source, cc, A.cubin, A.log);
+        sym::split_chunks(A);
+        sym::compile_cubins(A, cc);
     } catch (const p3g::CudaError &e) {
         return e.status;
     }
-    if (cubin_bytes) *cubin_bytes = A.cubin.size();
+    if (cubin_bytes) {
+        *cubin_bytes = 0;
+        for (auto &c : A.cubins) *cubin_bytes += c.size();
+    }
     return p3g::OK;
 }
 
-P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_air **out) {
+P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_sym_air **out) {
     if (!x || !out) return p3g::ERR_INVALID;
     *out = nullptr;
-    p3g_air *a = new p3g_air();
+    p3g_sym_air *a = new p3g_sym_air();
     std::string why;
     if (int v = p3g::desc_from_c(desc, a->a.d, why)) {
         x->c.last_error = "symbolic AIR rejected: " + why;
@@ -563,7 +566,7 @@ P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_air **out
     try {
         CK(cudaSetDevice(x->c.device));
         sym::analyse(a->a);
-        a->a.source = sym::generate(a->a);
+        sym::split_chunks(a->a);
         sym::compile(a->a, x->c.device);
     } catch (const p3g::CudaError &e) {
         x->c.last_error = e.what;
@@ -573,12 +576,12 @@ P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_air **out
     *out = a;
     return p3g::OK;
 }
-P3G_API uint32_t p3g_air_log_quotient_degree(const p3g_air *a) { return a ? a->a.log_qd : 0; }
-P3G_API uint32_t p3g_air_max_degree(const p3g_air *a) { return a ? a->a.max_degree : 0; }
-P3G_API uint64_t p3g_air_num_constraints_of(const p3g_air *a) { return a ? a->a.d.constraints.size() : 0; }
+P3G_API uint32_t p3g_air_log_quotient_degree(const p3g_sym_air *a) { return a ? a->a.log_qd : 0; }
+P3G_API uint32_t p3g_air_max_degree(const p3g_sym_air *a) { return a ? a->a.max_degree : 0; }
+P3G_API uint64_t p3g_air_num_constraints_of(const p3g_sym_air *a) { return a ? a->a.d.constraints.size() : 0; }
 // ConstraintLayout: base_indices / ext_indices in emission order; *n_base and
 // *n_ext are capacities on entry and counts on return.
-P3G_API int p3g_air_layout(const p3g_air *a, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext) {
+P3G_API int p3g_air_layout(const p3g_sym_air *a, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext) {
     if (!a || !n_base || !n_ext) return p3g::ERR_INVALID;
     const uint64_t nb = a->a.base_idx.size(), ne = a->a.ext_idx.size();
     if ((nb && (!base_idx || *n_base < nb)) || (ne && (!ext_idx || *n_ext < ne))) {
@@ -590,4 +593,4 @@ P3G_API int p3g_air_layout(const p3g_air *a, uint64_t *base_idx, uint64_t *n_bas
     *n_base = nb, *n_ext = ne;
     return p3g::OK;
 }
-P3G_API void p3g_air_free(p3g_air *a) { delete a; }
+P3G_API void p3g_air_free(p3g_sym_air *a) { delete a; }

@@ -348,8 +348,10 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde,
     }
     a.acc = acc;
     void *args[] = {&a};
-    CK(cudaLaunchKernel((const void *)A.kernel, dim3((unsigned)((qh + 127) / 128)), dim3(128), args, 0, ctx.stream));
-    ctx.launches++;
+    for (cudaKernel_t k : A.kernels) {  // one launch per constraint chunk, each adding its part of the fold
+        CK(cudaLaunchKernel((const void *)k, dim3((unsigned)((qh + 127) / 128)), dim3(128), args, 0, ctx.stream));
+        ctx.launches++;
+    }
     ctx.sync();  // keep the constant block and the periodic table alive until the kernel ran
 }
 

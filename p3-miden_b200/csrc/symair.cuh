@@ -37,6 +37,7 @@
 #include <cstring>
 #include <mutex>
 #include <sstream>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -83,13 +84,14 @@ struct Air {
     bool uses_first = false, uses_last = false, uses_trans = false;
     std::vector<uint64_t> base_idx, ext_idx;  // ConstraintLayout
     KLayout kl;
+    std::vector<std::vector<uint32_t>> chunks;  // constraint indices of each generated kernel
     std::string source, log;
-    std::vector<char> cubin;
-    cudaLibrary_t lib = nullptr;
-    cudaKernel_t kernel = nullptr;
+    std::vector<std::vector<char>> cubins;  // one per compiled group of chunks
+    std::vector<cudaLibrary_t> libs;
+    std::vector<cudaKernel_t> kernels;  // one per chunk: p3g_sym_eval_<c>
     int device = -1;
     ~Air() {
-        if (lib) cudaLibraryUnload(lib);
+        for (cudaLibrary_t l : libs) cudaLibraryUnload(l);
     }
 };
 
@@ -203,11 +205,58 @@ struct KArgs {
     uint64_t *acc;         // EF accumulator, += the folded numerator
 };
 
-inline std::string generate(const Air &A) {
+// Constraints are split into chunks of bounded code size (at most
+// kChunkNodes DAG nodes each, shared subexpressions counted once per chunk);
+// each chunk is one kernel that adds its part of the fold into acc. The fold
+// is linear, so launching the chunks one after another on the same stream
+// gives the same sum. A small AIR is one chunk.
+constexpr size_t kChunkNodes = 400;
+
+inline void split_chunks(Air &A) {
+    const Desc &d = A.d;
+    const size_t n = d.nodes.size();
+    A.chunks.assign(1, {});
+    std::vector<uint32_t> owner(n, 0), seen(n, 0), st, walk;
+    uint32_t cid = 1, epoch = 0;
+    size_t in_chunk = 0;
+    // the nodes under `root` that the current chunk does not hold yet
+    auto collect = [&](uint32_t root) {
+        walk.clear();
+        st.assign(1, root);
+        ++epoch;
+        while (!st.empty()) {
+            const uint32_t i = st.back();
+            st.pop_back();
+            if (owner[i] == cid || seen[i] == epoch) continue;
+            seen[i] = epoch;
+            walk.push_back(i);
+            const Node &x = d.nodes[i];
+            if (x.op == ADD || x.op == SUB || x.op == MUL) st.push_back(x.a), st.push_back(x.b);
+            if (x.op == NEG) st.push_back(x.a);
+        }
+    };
+    for (size_t k = 0; k < d.constraints.size(); k++) {
+        collect(d.constraints[k]);
+        if (!A.chunks.back().empty() && in_chunk + walk.size() > kChunkNodes) {
+            A.chunks.emplace_back();
+            cid++;
+            in_chunk = 0;
+            collect(d.constraints[k]);
+        }
+        for (uint32_t i : walk) owner[i] = cid;
+        in_chunk += walk.size();
+        A.chunks.back().push_back((uint32_t)k);
+    }
+}
+
+// The source of the kernels of chunks [c0, c1): the field arithmetic
+// (gl.cuh), the argument block and one kernel per chunk.
+inline std::string generate_range(const Air &A, size_t c0, size_t c1) {
     const Desc &d = A.d;
     std::ostringstream o;
     o << "// generated by libp3miden_b200 (symair.cuh) from a symbolic AIR: " << d.nodes.size() << " nodes, "
-      << d.constraints.size() << " constraints, max degree " << A.max_degree << "\n";
+      << d.constraints.size() << " constraints in " << A.chunks.size() << " kernels (here " << c0 << ".." << c1
+      << "), max degree " << A.max_degree << "\n";
     o << kGlSource << "\n";
     o << R"K(
 struct KArgs {
@@ -222,8 +271,28 @@ struct KArgs {
     uint64_t zh[8];
     uint64_t *acc;
 };
-extern "C" __global__ void __launch_bounds__(128) p3g_sym_eval(const __grid_constant__ KArgs a) {
-    const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+)K";
+    const size_t n = d.nodes.size();
+    auto as_ef = [&](uint32_t j) {
+        std::string v = "v" + std::to_string(j);
+        return A.ext[j] ? v : "gl::ef{" + v + ", 0}";
+    };
+    std::vector<uint8_t> live(n);
+    for (size_t c = c0; c < c1; c++) {
+        const std::vector<uint32_t> &ks = A.chunks[c];
+        std::fill(live.begin(), live.end(), 0);
+        for (uint32_t k : ks) live[d.constraints[k]] = 1;
+        bool first = false, last = false, trans = false;
+        for (size_t i = n; i-- > 0;) {
+            if (!live[i]) continue;
+            const Node &x = d.nodes[i];
+            if (x.op == ADD || x.op == SUB || x.op == MUL) live[x.a] = live[x.b] = 1;
+            if (x.op == NEG) live[x.a] = 1;
+            first |= x.op == IS_FIRST_ROW, last |= x.op == IS_LAST_ROW, trans |= x.op == IS_TRANSITION;
+        }
+        o << "extern \"C\" __global__ void __launch_bounds__(128) p3g_sym_eval_" << c
+          << "(const __grid_constant__ KArgs a) {\n";
+        o << R"K(    const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.qh) return;
     const uint64_t rl = gl::bitrev(m, a.log_qh), rn = gl::bitrev((m + a.D) & (a.qh - 1), a.log_qh);
     const uint64_t *ML = a.main + rl * a.main_w, *MN = a.main + rn * a.main_w;
@@ -232,94 +301,87 @@ extern "C" __global__ void __launch_bounds__(128) p3g_sym_eval(const __grid_cons
     const uint64_t *K = a.k;
     (void)ML; (void)MN; (void)AL; (void)AN; (void)PR; (void)K;
 )K";
-    if (A.uses_first || A.uses_last || A.uses_trans) {
-        o << "    const uint64_t mlo = m & ((1ull << a.wq_lo_bits) - 1), mhi = m >> a.wq_lo_bits;\n"
-             "    uint64_t wm = __ldg(a.wq_lo + mlo);\n"
-             "    if (mhi) wm = gl::mul(wm, __ldg(a.wq_hi + mhi));\n"
-             "    const uint64_t x = gl::mul(a.shift, wm);\n";
-        if (A.uses_first || A.uses_last) o << "    const uint64_t zh = a.zh[m & (a.D - 1)];\n";
-        if (A.uses_first) o << "    const uint64_t s_first = gl::mul(zh, gl::inv(gl::sub(x, 1)));\n";
-        if (A.uses_last) o << "    const uint64_t s_last = gl::mul(zh, gl::inv(gl::sub(x, a.omega_h_inv)));\n";
-        if (A.uses_trans) o << "    const uint64_t s_trans = gl::sub(x, a.omega_h_inv);\n";
-    }
-    // live nodes in order
-    const size_t n = d.nodes.size();
-    std::vector<uint8_t> live(n, 0);
-    for (uint32_t c : d.constraints) live[c] = 1;
-    for (size_t i = n; i-- > 0;) {
-        if (!live[i]) continue;
-        const Node &x = d.nodes[i];
-        if (x.op == ADD || x.op == SUB || x.op == MUL) live[x.a] = live[x.b] = 1;
-        if (x.op == NEG) live[x.a] = 1;
-    }
-    auto as_ef = [&](uint32_t j) {
-        std::string v = "v" + std::to_string(j);
-        return A.ext[j] ? v : "gl::ef{" + v + ", 0}";
-    };
-    for (size_t i = 0; i < n; i++) {
-        if (!live[i]) continue;
-        const Node &x = d.nodes[i];
-        const std::string v = "v" + std::to_string(i);
-        const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
-        o << "    " << ty << v << " = ";
-        switch (x.op) {
-            case CONST: o << x.value << "ull"; break;
-            case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + " << x.a << ")"; break;
-            case AUX:
-                o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + " << 2 * x.a << "), __ldg(" << (x.b ? "AN" : "AL")
-                  << " + " << 2 * x.a + 1 << ")}";
-                break;
-            case PUBLIC: o << "__ldg(K + " << A.kl.pub + x.a << ")"; break;
-            case RANDOMNESS:
-                o << "gl::ef{__ldg(K + " << A.kl.rnd + 2 * x.a << "), __ldg(K + " << A.kl.rnd + 2 * x.a + 1 << ")}";
-                break;
-            case AUX_VALUE:
-                o << "gl::ef{__ldg(K + " << A.kl.auxv + 2 * x.a << "), __ldg(K + " << A.kl.auxv + 2 * x.a + 1 << ")}";
-                break;
-            case PERIODIC: o << "__ldg(PR + " << x.a << ")"; break;
-            case IS_FIRST_ROW: o << "s_first"; break;
-            case IS_LAST_ROW: o << "s_last"; break;
-            case IS_TRANSITION: o << "s_trans"; break;
-            case ADD: case SUB: {
-                const char *f = x.op == ADD ? "add" : "sub";
-                if (A.ext[i]) o << "gl::ef_" << f << "(" << as_ef(x.a) << ", " << as_ef(x.b) << ")";
-                else o << "gl::" << f << "(v" << x.a << ", v" << x.b << ")";
-                break;
+        if (first || last || trans) {
+            o << "    const uint64_t mlo = m & ((1ull << a.wq_lo_bits) - 1), mhi = m >> a.wq_lo_bits;\n"
+                 "    uint64_t wm = __ldg(a.wq_lo + mlo);\n"
+                 "    if (mhi) wm = gl::mul(wm, __ldg(a.wq_hi + mhi));\n"
+                 "    const uint64_t x = gl::mul(a.shift, wm);\n";
+            if (first || last) o << "    const uint64_t zh = a.zh[m & (a.D - 1)];\n";
+            if (first) o << "    const uint64_t s_first = gl::mul(zh, gl::inv(gl::sub(x, 1)));\n";
+            if (last) o << "    const uint64_t s_last = gl::mul(zh, gl::inv(gl::sub(x, a.omega_h_inv)));\n";
+            if (trans) o << "    const uint64_t s_trans = gl::sub(x, a.omega_h_inv);\n";
+        }
+        for (size_t i = 0; i < n; i++) {
+            if (!live[i]) continue;
+            const Node &x = d.nodes[i];
+            const std::string v = "v" + std::to_string(i);
+            const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
+            o << "    " << ty << v << " = ";
+            switch (x.op) {
+                case CONST: o << x.value << "ull"; break;
+                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + " << x.a << ")"; break;
+                case AUX:
+                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + " << 2 * x.a << "), __ldg(" << (x.b ? "AN" : "AL")
+                      << " + " << 2 * x.a + 1 << ")}";
+                    break;
+                case PUBLIC: o << "__ldg(K + " << A.kl.pub + x.a << ")"; break;
+                case RANDOMNESS:
+                    o << "gl::ef{__ldg(K + " << A.kl.rnd + 2 * x.a << "), __ldg(K + " << A.kl.rnd + 2 * x.a + 1 << ")}";
+                    break;
+                case AUX_VALUE:
+                    o << "gl::ef{__ldg(K + " << A.kl.auxv + 2 * x.a << "), __ldg(K + " << A.kl.auxv + 2 * x.a + 1
+                      << ")}";
+                    break;
+                case PERIODIC: o << "__ldg(PR + " << x.a << ")"; break;
+                case IS_FIRST_ROW: o << "s_first"; break;
+                case IS_LAST_ROW: o << "s_last"; break;
+                case IS_TRANSITION: o << "s_trans"; break;
+                case ADD: case SUB: {
+                    const char *f = x.op == ADD ? "add" : "sub";
+                    if (A.ext[i]) o << "gl::ef_" << f << "(" << as_ef(x.a) << ", " << as_ef(x.b) << ")";
+                    else o << "gl::" << f << "(v" << x.a << ", v" << x.b << ")";
+                    break;
+                }
+                case MUL:
+                    if (!A.ext[i]) o << "gl::mul(v" << x.a << ", v" << x.b << ")";
+                    else if (!A.ext[x.a]) o << "gl::ef_mulf(v" << x.b << ", v" << x.a << ")";
+                    else if (!A.ext[x.b]) o << "gl::ef_mulf(v" << x.a << ", v" << x.b << ")";
+                    else o << "gl::ef_mul(v" << x.a << ", v" << x.b << ")";
+                    break;
+                default:  // NEG
+                    o << (A.ext[i] ? "gl::ef_neg(v" : "gl::neg(v") << x.a << ")";
+                    break;
             }
-            case MUL:
-                if (!A.ext[i]) o << "gl::mul(v" << x.a << ", v" << x.b << ")";
-                else if (!A.ext[x.a]) o << "gl::ef_mulf(v" << x.b << ", v" << x.a << ")";
-                else if (!A.ext[x.b]) o << "gl::ef_mulf(v" << x.a << ", v" << x.b << ")";
-                else o << "gl::ef_mul(v" << x.a << ", v" << x.b << ")";
-                break;
-            default:  // NEG
-                o << (A.ext[i] ? "gl::ef_neg(v" : "gl::neg(v") << x.a << ")";
-                break;
+            o << ";\n";
         }
-        o << ";\n";
-    }
-    // fold: base constraints on two lazy accumulators (one per coordinate of
-    // alpha^{K-1-k}), extension constraints as extension products
-    o << "    gl::Acc f0, f1;\n    gl::ef fe = gl::ef_zero();\n";
-    const size_t K = d.constraints.size();
-    for (size_t k = 0; k < K; k++) {
-        const uint32_t c = d.constraints[k];
-        const uint64_t ap = A.kl.alpha + 2 * k;
-        if (!A.ext[c]) {
-            o << "    f0.mac(v" << c << ", __ldg(K + " << ap << ")); f1.mac(v" << c << ", __ldg(K + " << ap + 1
-              << "));\n";
-        } else {
-            o << "    fe = gl::ef_add(fe, gl::ef_mul(v" << c << ", gl::ef{__ldg(K + " << ap << "), __ldg(K + " << ap + 1
-              << ")}));\n";
+        // this chunk's part of the fold: base constraints on two lazy
+        // accumulators (one per coordinate of alpha^{K-1-k}), extension
+        // constraints as extension products
+        o << "    gl::Acc f0, f1;\n    gl::ef fe = gl::ef_zero();\n";
+        for (uint32_t k : ks) {
+            const uint32_t cn = d.constraints[k];
+            const uint64_t ap = A.kl.alpha + 2ull * k;
+            if (!A.ext[cn])
+                o << "    f0.mac(v" << cn << ", __ldg(K + " << ap << ")); f1.mac(v" << cn << ", __ldg(K + " << ap + 1
+                  << "));\n";
+            else
+                o << "    fe = gl::ef_add(fe, gl::ef_mul(v" << cn << ", gl::ef{__ldg(K + " << ap << "), __ldg(K + "
+                  << ap + 1 << ")}));\n";
         }
-    }
-    o << R"K(    const gl::ef r = gl::ef_add(gl::ef{f0.reduce(), f1.reduce()}, fe);
+        o << R"K(    const gl::ef r = gl::ef_add(gl::ef{f0.reduce(), f1.reduce()}, fe);
     uint64_t *out = a.acc + 2 * m;
     out[0] = gl::add(out[0], r.c0);
     out[1] = gl::add(out[1], r.c1);
 }
 )K";
+    }
     return o.str();
+}
+
+// The whole generated program (every chunk's kernel); splits the chunks.
+inline std::string generate(Air &A) {
+    split_chunks(A);
+    return generate_range(A, 0, A.chunks.size());
 }
 
 struct CompileError {
@@ -350,13 +412,46 @@ inline void nvrtc_cubin(const std::string &source, int cc, std::vector<char> &cu
     nvrtcDestroyProgram(&prog);
 }
 
+// Compile the chunks in groups, one NVRTC program per group, on up to one
+// host thread per core (compile time grows faster than linearly in the size
+// of a straight-line kernel, and groups compile independently).
+inline void compile_cubins(Air &A, int cc) {
+    const size_t nch = A.chunks.size();
+    unsigned hw = std::thread::hardware_concurrency();
+    const size_t groups = std::max<size_t>(1, std::min<size_t>(nch, hw ? hw : 4));
+    A.cubins.assign(groups, {});
+    std::vector<std::string> logs(groups);
+    std::vector<std::string> errs(groups);
+    std::vector<std::thread> th;
+    for (size_t g = 0; g < groups; g++)
+        th.emplace_back([&, g] {
+            const size_t c0 = nch * g / groups, c1 = nch * (g + 1) / groups;
+            try {
+                nvrtc_cubin(generate_range(A, c0, c1), cc, A.cubins[g], logs[g]);
+            } catch (const p3g::CudaError &e) {
+                errs[g] = e.what;
+            }
+        });
+    for (auto &t : th) t.join();
+    for (size_t g = 0; g < groups; g++)
+        if (!errs[g].empty()) throw p3g::CudaError{p3g::ERR_CUDA, errs[g]};
+    A.log = logs[0];
+}
+
 inline void compile(Air &A, int device) {
     int major = 0, minor = 0;
     CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     CK(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
-    nvrtc_cubin(A.source, major * 10 + minor, A.cubin, A.log);
-    CK(cudaLibraryLoadData(&A.lib, A.cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
-    CK(cudaLibraryGetKernel(&A.kernel, A.lib, "p3g_sym_eval"));
+    compile_cubins(A, major * 10 + minor);
+    const size_t nch = A.chunks.size(), groups = A.cubins.size();
+    A.kernels.resize(nch);
+    for (size_t g = 0; g < groups; g++) {
+        cudaLibrary_t lib = nullptr;
+        CK(cudaLibraryLoadData(&lib, A.cubins[g].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        A.libs.push_back(lib);
+        for (size_t c = nch * g / groups; c < nch * (g + 1) / groups; c++)
+            CK(cudaLibraryGetKernel(&A.kernels[c], lib, ("p3g_sym_eval_" + std::to_string(c)).c_str()));
+    }
     A.device = device;
 }
 

@@ -132,3 +132,19 @@ def test_malformed_dags_rejected(product):
     bad2.nodes[j]["a"] = 5
     with pytest.raises(product.P3gError):
         product.air_analyse(bad2)
+
+
+def test_oracle_symbolic_keccak_equals_builtin(product):
+    """The Keccak-f[1600] AIR written against the symbolic builder (3182
+    constraints, degree 3) drives the oracle to its hand-written Keccak
+    AIR's proof, bit for bit: the DAG carries the same constraints in the
+    same order."""
+    desc = product.build_air(S.keccak_eval, S.KC_NCOLS)
+    assert desc.num_constraints == 3182
+    assert product.air_analyse(desc)["log_quotient_degree"] == 1
+    t = O.keccak_trace(O.keccak_inputs(1, 5), 7)
+    pcs = pcs_d(1, 1, fpow=4, nq=10)
+    a = O.prove(O.default_p2(), pcs, [(O.AIR_KECCAK, t, None)])
+    b = O.prove(O.default_p2(), pcs, [(O.AIR_KECCAK, t, None, {"sym": desc})])
+    for key in ("fields", "commits", "digest"):
+        assert np.array_equal(a[key], b[key]), key
