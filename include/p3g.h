@@ -408,6 +408,13 @@ int p3g_keccak_inputs(uint64_t seed, uint64_t n_perms, uint64_t *out25);
 /* Cubic AIR trace: k then row 0 drawn from SmallRng(seed), forward iteration. */
 int p3g_cubic_trace(uint32_t log_height, uint64_t width, uint64_t seed, uint64_t *consts_out, uint64_t *trace_out);
 uint64_t p3g_air_num_constraints(int32_t air, uint64_t width);
+/* The cubic AIR's trace generated on the device: k and row 0 from
+ * SmallRng(seed) (as p3g_cubic_trace), the forward iteration on the device
+ * into d_out (device, 2^log_height x width, row-major, width <= 8192);
+ * consts_out (host) receives k. Bit-identical to p3g_cubic_trace; the caller
+ * uploads nothing. */
+int p3g_cubic_trace_device(p3g_ctx *ctx, uint32_t log_height, uint64_t width, uint64_t seed, uint64_t *consts_out,
+                           uint64_t *d_out);
 
 #ifdef __cplusplus
 }

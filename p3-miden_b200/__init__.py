@@ -142,6 +142,7 @@ def lib():
             "p3g_keccak_inputs": (C.c_int, [C.c_uint64, C.c_uint64, u64p]),
             "p3g_cubic_trace": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, u64p, u64p]),
             "p3g_air_num_constraints": (C.c_uint64, [C.c_int32, C.c_uint64]),
+            "p3g_cubic_trace_device": (C.c_int, [vp, C.c_uint32, C.c_uint64, C.c_uint64, u64p, C.c_void_p]),
             "p3g_verify": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, u64p, C.c_uint64,
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
             "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
@@ -788,6 +789,18 @@ def generate_keccak_trace_device(ctx: Context, inputs_dev, log_h: int | None = N
     ctx.check(lib().p3g_keccak_trace_device(ctx.handle, inputs_dev.data_ptr() if n else None, n, log_h,
                                             out.data_ptr()))
     return out
+
+
+def generate_cubic_trace_device(ctx: Context, log_h: int, width: int, seed: int, out=None):
+    """The cubic AIR's trace generated on the device (forward iteration there;
+    k and row 0 from the seeded RNG): returns (k, device tensor)."""
+    if out is None:
+        out = empty_device((1 << log_h, width), ctx.device)
+    k = np.zeros(width, dtype=np.uint64)
+    import torch
+    torch.cuda.synchronize(ctx.device)
+    ctx.check(lib().p3g_cubic_trace_device(ctx.handle, log_h, width, seed, _ptr(k), out.data_ptr()))
+    return k, out
 
 
 def generate_cubic_trace(log_h: int, width: int, seed: int, out: np.ndarray | None = None):

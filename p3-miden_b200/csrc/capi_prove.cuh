@@ -262,6 +262,33 @@ P3G_API int p3g_cubic_trace(uint32_t log_height, uint64_t width, uint64_t seed, 
     p3g::cubic_trace(log_height, width, seed, consts_out, trace_out);
     return p3g::OK;
 }
+// The cubic AIR's trace generated on the device: k and row 0 drawn from
+// SmallRng(seed) on the host (as p3g_cubic_trace), the forward iteration on
+// the device into d_out (2^log_height x width, row-major); consts_out (host)
+// receives k. Bit-identical to p3g_cubic_trace.
+P3G_API int p3g_cubic_trace_device(p3g_ctx *x, uint32_t log_height, uint64_t width, uint64_t seed,
+                                   uint64_t *consts_out, uint64_t *d_out) {
+    if (!x || !consts_out || !d_out || width == 0 || width > tgen::kCubicMaxWidth || log_height > 30)
+        return p3g::ERR_INVALID;
+    P3G_TRY(x, {
+        CK(cudaSetDevice(x->c.device));
+        std::vector<uint64_t> kr(2 * width);
+        p3g::cubic_trace(0, width, seed, kr.data(), kr.data() + width);  // k, then row 0
+        memcpy(consts_out, kr.data(), width * 8);
+        p3g::DBuf d = x->c.upload(kr);
+        const int threads = (int)std::min<uint64_t>(1024, (width + 31) / 32 * 32);
+        const size_t smem = 2 * width * 8;
+        static std::once_flag attr_once;
+        std::call_once(attr_once, [] {
+            CK(cudaFuncSetAttribute(tgen::cubic_trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(2 * tgen::kCubicMaxWidth * 8)));
+        });
+        tgen::cubic_trace_kernel<<<1, threads, smem, x->c.stream>>>(d.p + width, d.p, width, 1ull << log_height, d_out);
+        CK(cudaGetLastError());
+        x->c.launches++;
+        x->c.sync();
+    })
+}
 P3G_API uint64_t p3g_air_num_constraints(int32_t air, uint64_t width) { return p3g::air_num_constraints(air, width); }
 
 // Proof-of-work witness search for a challenger state (GrindingChallenger::grind).

@@ -27,14 +27,16 @@ namespace p3g {
 
 // Upper bound of the device bytes prove() allocates for a job.
 inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, size_t n) {
-    const uint64_t B = 1ull << pcs.log_blowup, D = 2;
+    const uint64_t B = 1ull << pcs.log_blowup;
+    uint64_t D = 1;
+    for (size_t i = 0; i < n; i++) D = std::max<uint64_t>(D, 1ull << inst_log_qd(inst[i]));
     uint64_t words = 0, max_hw = 0, hmax = 0;
     for (size_t i = 0; i < n; i++) {
-        uint64_t hw = inst[i].height * inst[i].width;
+        const uint64_t hw = inst[i].height * inst[i].width, aw2 = 2 * inst_aux_width(inst[i]);
         if (!inst[i].trace_on_device) words += hw;  // uploaded trace
         words += hw * B;                             // main LDE
-        words += inst[i].height * 2 * (B + 1);       // aux trace + LDE
-        max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, 2));
+        words += inst[i].height * aw2 * (B + 1);     // aux trace + LDE
+        max_hw = std::max(max_hw, inst[i].height * std::max<uint64_t>(inst[i].width, aw2));
         hmax = std::max(hmax, inst[i].height);
     }
     max_hw = std::max(max_hw, hmax * 2 * D);

@@ -17,6 +17,8 @@
 #pragma once
 #include <cstdint>
 
+#include "gl.cuh"
+
 namespace tgen {
 
 constexpr int K_STEP = 0, K_EXPORT = 24, K_PRE = 25, K_A = 125, K_C = 225, K_CP = 545, K_AP = 865, K_APP = 2465,
@@ -121,6 +123,36 @@ __global__ void __launch_bounds__(128) keccak_trace_kernel(const uint64_t *input
             }
             base[(uint64_t)r * K_NCOLS + col] = val;
         }
+    }
+}
+
+// Forward iteration of the cubic AIR's trace (the rows after row 0):
+// row r+1 = row_r^3 + rotate(row_r, 1) + k, column i of row r+1 reading
+// columns i and i+1 of row r. Rows depend on each other, columns do not, so
+// one block iterates one trace: thread t owns columns t, t + T, ...; row r
+// sits in shared memory (two buffers), and each row is stored to HBM by
+// consecutive threads (coalesced). Widths up to kCubicMaxWidth.
+constexpr uint64_t kCubicMaxWidth = 8192;
+__global__ void __launch_bounds__(1024) cubic_trace_kernel(const uint64_t *row0, const uint64_t *k, uint64_t w,
+                                                           uint64_t h, uint64_t *out) {
+    extern __shared__ uint64_t buf[];  // 2 x w
+    uint64_t *cur = buf, *nxt = buf + w;
+    for (uint64_t i = threadIdx.x; i < w; i += blockDim.x) {
+        cur[i] = row0[i];
+        out[i] = row0[i];
+    }
+    __syncthreads();
+    for (uint64_t r = 1; r < h; r++) {
+        for (uint64_t i = threadIdx.x; i < w; i += blockDim.x) {
+            const uint64_t x = cur[i];
+            const uint64_t v = gl::add(gl::add(gl::mul(gl::sqr(x), x), cur[i + 1 == w ? 0 : i + 1]), __ldg(k + i));
+            nxt[i] = v;
+            out[r * w + i] = v;
+        }
+        __syncthreads();
+        uint64_t *t = cur;
+        cur = nxt;
+        nxt = t;
     }
 }
 

@@ -180,3 +180,23 @@ def test_periodic_lde_matches_oracle(product, gpu_ctx, log_h, log_blowup, period
     got = product.to_host(product.periodic_lde(gpu_ctx, product.to_device(repeated), log_blowup, log_h, shift))
     want = O.periodic_lde(repeated, log_blowup, log_h, shift)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("log_h,w", [(1, 1), (4, 1), (8, 3), (10, 64), (12, 1024), (16, 2), (6, 3000)])
+def test_cubic_trace_device_matches_host(product, gpu_ctx, log_h, w):
+    """The cubic AIR's forward iteration on the device equals the host
+    generator (k and every row), including widths above one block's threads."""
+    k_d, t_d = product.generate_cubic_trace_device(gpu_ctx, log_h, w, 40 + w)
+    k_h, t_h = O.cubic_trace(log_h, w, 40 + w)
+    assert np.array_equal(k_d, k_h)
+    assert np.array_equal(product.to_host(t_d), t_h)
+
+
+def test_proof_from_device_cubic_trace(product, gpu_ctx):
+    k, t = product.generate_cubic_trace_device(gpu_ctx, 10, 16, 9)
+    pcs = product.PcsParams(3, 2, 0, 6, 0, 20, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k)])
+    kh, th = O.cubic_trace(10, 16, 9)
+    orc = O.prove(O.default_p2(), dict(log_blowup=3, log_folding_arity=2, log_final_degree=0, folding_pow_bits=6,
+                                       deep_pow_bits=0, num_queries=20, query_pow_bits=0), [(O.AIR_CUBIC, th, kh)])
+    assert np.array_equal(gpu.proof.fields, orc["fields"]) and np.array_equal(gpu.digest, orc["digest"])
