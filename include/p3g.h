@@ -298,6 +298,26 @@ int p3g_coset_lde_noalloc(const uint64_t *d_in, uint64_t height, uint64_t width,
                           uint64_t *d_out, void *stream);
 uint64_t p3g_coset_lde_noalloc_max_words(void);
 
+/* ------------------------------------------------------------ autotuning */
+/* No counterpart in the reference. Launch shapes of this library timed on
+ * the context's device with CUDA events; every choice computes the same
+ * values, so only the time changes. p3g_autotune_lde times the candidate
+ * splits of a 2^log_height-row coset LDE into bit ranges of at most 10 bits
+ * (each range is one shared-memory pass) on random data, keeps the fastest
+ * for this context and returns it (best_sizes, *n_sizes capacity on entry,
+ * count on return) with its time per LDE and the default split's.
+ * p3g_autotune_slabs does the same for the column-slab width of the main
+ * commit (LDE + leaf sponge + tree of a device trace). The setters load a
+ * saved choice (n = 0 / cols = 0 restore the defaults; a split must have
+ * ranges of 1..10 bits adding up to log_height, a slab width must be a
+ * multiple of 8, the sponge rate). */
+int p3g_autotune_lde(p3g_ctx *ctx, uint32_t log_height, uint64_t width, uint32_t log_blowup, uint32_t reps,
+                     uint32_t *best_sizes, uint32_t *n_sizes, double *best_ms, double *default_ms);
+int p3g_autotune_slabs(p3g_ctx *ctx, uint32_t log_height, uint64_t width, uint32_t log_blowup, uint32_t reps,
+                       uint64_t *best_cols, double *best_ms, double *default_ms);
+int p3g_ctx_set_lde_split(p3g_ctx *ctx, uint32_t log_height, const uint32_t *sizes, uint32_t n);
+int p3g_ctx_set_slab_columns(p3g_ctx *ctx, uint64_t cols);
+
 /* ------------------------------------------------------------ verifier */
 /* verify_multi (p3-miden-lifted-stark/src/verifier/mod.rs:170-364) of a
  * proof made by p3g_prove, with the LMCS openings, the DEEP and the FRI

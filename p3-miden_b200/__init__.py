@@ -143,6 +143,13 @@ def lib():
             "p3g_cubic_trace": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, u64p, u64p]),
             "p3g_air_num_constraints": (C.c_uint64, [C.c_int32, C.c_uint64]),
             "p3g_cubic_trace_device": (C.c_int, [vp, C.c_uint32, C.c_uint64, C.c_uint64, u64p, C.c_void_p]),
+            "p3g_autotune_lde": (C.c_int, [vp, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
+                                           C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double)]),
+            "p3g_autotune_slabs": (C.c_int, [vp, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
+                                             C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+            "p3g_ctx_set_lde_split": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+            "p3g_ctx_set_slab_columns": (C.c_int, [vp, C.c_uint64]),
             "p3g_verify": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, u64p, C.c_uint64,
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
             "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
@@ -227,6 +234,40 @@ class Context:
 
     def check(self, status: int):
         _check(status, self._h)
+
+    # ---- launch-shape tuning (p3g_autotune_*, p3g_ctx_set_*)
+    def autotune_lde(self, log_h: int, width: int, log_blowup: int, reps: int = 3) -> dict:
+        """Time the candidate bit-range splits of a 2^log_h x width coset LDE;
+        the fastest is kept for this context. Returns it with both times."""
+        sizes = (C.c_uint32 * 8)()
+        n, best, dflt = C.c_uint32(8), C.c_double(), C.c_double()
+        self.check(lib().p3g_autotune_lde(self._h, log_h, width, log_blowup, reps, sizes, C.byref(n), C.byref(best),
+                                          C.byref(dflt)))
+        return {"log_h": log_h, "width": width, "log_blowup": log_blowup, "split": list(sizes[:n.value]),
+                "ms": best.value, "default_ms": dflt.value}
+
+    def autotune_slabs(self, log_h: int, width: int, log_blowup: int, reps: int = 2) -> dict:
+        """Time the main commit for several column-slab widths; the fastest is
+        kept for this context (0 = the default rule)."""
+        cols, best, dflt = C.c_uint64(), C.c_double(), C.c_double()
+        self.check(lib().p3g_autotune_slabs(self._h, log_h, width, log_blowup, reps, C.byref(cols), C.byref(best),
+                                            C.byref(dflt)))
+        return {"log_h": log_h, "width": width, "log_blowup": log_blowup, "slab_cols": cols.value, "ms": best.value,
+                "default_ms": dflt.value}
+
+    def set_lde_split(self, log_h: int, sizes):
+        arr = (C.c_uint32 * max(1, len(sizes)))(*sizes)
+        self.check(lib().p3g_ctx_set_lde_split(self._h, log_h, arr, len(sizes)))
+
+    def set_slab_columns(self, cols: int):
+        self.check(lib().p3g_ctx_set_slab_columns(self._h, cols))
+
+    def load_tuning(self, table: dict):
+        """Apply a saved tuning table ({"lde_split": {L: [..]}, "slab_cols": n})."""
+        for L, sizes in table.get("lde_split", {}).items():
+            self.set_lde_split(int(L), sizes)
+        if table.get("slab_cols"):
+            self.set_slab_columns(int(table["slab_cols"]))
 
 
 # ------------------------------------------------------------------ torch

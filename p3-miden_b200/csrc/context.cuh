@@ -86,6 +86,12 @@ struct Ctx {
     size_t pinned_words = 0;
     uint64_t launches = 0;       // kernels launched by this context
     cudaStream_t lde_stream = nullptr, copy_stream = nullptr;  // main-commit pipeline
+    // Tuned launch shapes (p3g_autotune / p3g_ctx_set_*): the bit ranges of
+    // an LDE of 2^L rows, and the column-slab width of the main commit (0:
+    // the default of about 8 slabs for wide traces). Results do not depend on
+    // them: every choice computes the same values.
+    std::map<uint32_t, std::vector<uint32_t>> lde_split;
+    uint64_t slab_cols = 0;
 
     void pipeline_streams() {
         if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
@@ -205,6 +211,24 @@ inline void pow_table(uint64_t v, uint32_t L, uint32_t lo_bits, std::vector<uint
     for (size_t i = 0; i < nhi; i++) out_hi[i] = y, y = gl::mul(y, x);
 }
 
+// A split of L bits into LDE bit ranges is valid when every range has 1..10
+// bits (the kernels' shared-memory groups) and the ranges add up to L.
+inline bool valid_split(uint32_t L, const std::vector<uint32_t> &sizes) {
+    if (sizes.empty() || sizes.size() > 8) return false;
+    uint32_t sum = 0;
+    for (uint32_t k : sizes) {
+        if (k == 0 || k > 10) return false;
+        sum += k;
+    }
+    return sum == L;
+}
+
+// split L bits into n ranges, sizes as even as possible
+inline std::vector<uint32_t> pass_sizes_n(uint32_t L, uint32_t n) {
+    std::vector<uint32_t> v(n, L / n);
+    for (uint32_t i = 0; i < L % n; i++) v[i]++;
+    return v;
+}
 // split L bits into passes of at most 10 bits, sizes as even as possible
 inline std::vector<uint32_t> pass_sizes(uint32_t L) {
     uint32_t n = L == 0 ? 1 : (L + 9) / 10;
@@ -239,7 +263,8 @@ inline LdePlan lde_plan(Ctx &ctx, uint64_t h, uint32_t log_blowup, uint64_t shif
     p.h = h;
     p.log_blowup = log_blowup;
     p.tw = &ctx.twiddles(p.L);
-    p.sizes = pass_sizes(p.L);
+    auto tuned = ctx.lde_split.find(p.L);
+    p.sizes = tuned != ctx.lde_split.end() ? tuned->second : pass_sizes(p.L);
     p.scale_lo_bits = p.L < 12 ? p.L : 12;
     const uint64_t wb = gl::root(p.L + log_blowup);
     const uint64_t hinv = gl::inv(h % gl::P);

@@ -4,3 +4,4 @@
 #include "capi_prove.cuh"
 #include "capi_server.cuh"
 #include "capi_verify.cuh"
+#include "capi_tune.cuh"

@@ -180,6 +180,7 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
     for (size_t i = 0; i < n_inst; i++) {
         uint64_t w = inst[i].width, h = inst[i].height;
         uint64_t sw = w >= 256 ? ((w + 7) / 8 + 7) / 8 * 8 : w;  // about 8 slabs for wide traces
+        if (ctx.slab_cols) sw = std::min<uint64_t>(w, ctx.slab_cols);  // tuned: a multiple of the rate (8)
         for (uint64_t c0 = 0; c0 < w; c0 += sw) {
             slabs.push_back({i, c0, std::min(sw, w - c0)});
             max_slab_hw = std::max(max_slab_hw, h * std::min(sw, w - c0));
@@ -654,14 +655,14 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             static std::once_flag attr_once;
             std::call_once(attr_once, [] {
                 CK(cudaFuncSetAttribute(quot::keccak_eval_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)quot::KEC_SMEM));
+                                        (int)quot::KEC_SMEM_MAX));
             });
             int dev_sms = 148;
             CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx.device));
             uint64_t blocks = std::min<uint64_t>(qh, (uint64_t)dev_sms * 3);
             uint64_t ppb = (qh + blocks - 1) / blocks;
             blocks = (qh + ppb - 1) / ppb;
-            L(quot::keccak_eval_block_kernel, (unsigned)blocks, quot::KEC_THREADS, quot::KEC_SMEM, a, ppb);
+            L(quot::keccak_eval_block_kernel, (unsigned)blocks, quot::KEC_THREADS, quot::kec_smem(D), a, ppb);
         }
         ctx.sync();  // keep d_ap / d_consts alive until the kernel ran
     }

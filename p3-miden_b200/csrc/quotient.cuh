@@ -252,16 +252,18 @@ GL_HD void keccak_task(int t, const T *L, const T *N, T first, T trans, F &f) {
 }
 
 // Persistent blocks over contiguous point ranges. Rows are staged in a ring
-// of 3 shared-memory slots: point m needs rows m and m + 2 (D = 2), so each
-// LDE row is read from HBM once per block range. Selectors for the next 256
-// points are computed cooperatively (one inversion per point).
+// of D + 1 shared-memory slots: point m needs rows m and m + D (D = 2 for
+// this AIR alone; up to 8 when it is proved beside an AIR of higher degree),
+// so each LDE row is read from HBM once per block range. Selectors for the
+// next 256 points are computed cooperatively (one inversion per point).
 constexpr int KEC_THREADS = 256;
 __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __grid_constant__ EvalArgs a,
                                                                          uint64_t points_per_block) {
     extern __shared__ uint64_t sm[];
-    uint64_t *ring = sm;                    // 3 x 2633
-    uint64_t *sel = sm + 3 * KC_NCOLS;      // 256 x {first, trans}
-    uint64_t *red = sel + 2 * KEC_THREADS;  // 8 warps x 2
+    const uint32_t slots = (uint32_t)a.D + 1;
+    uint64_t *ring = sm;                        // (D + 1) x 2633
+    uint64_t *sel = sm + slots * KC_NCOLS;      // 256 x {first, trans}
+    uint64_t *red = sel + 2 * KEC_THREADS;      // 8 warps x 2
     const uint64_t qh = 1ull << a.log_qh;
     const uint64_t m0 = (uint64_t)blockIdx.x * points_per_block;
     if (m0 >= qh) return;
@@ -272,8 +274,7 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
         uint64_t *dst = ring + slot * KC_NCOLS;
         for (int c = tid; c < KC_NCOLS; c += KEC_THREADS) dst[c] = __ldg(src + c);
     };
-    load_row(m0, (int)(m0 % 3));
-    load_row(m0 + 1, (int)((m0 + 1) % 3));
+    for (uint64_t j = 0; j < a.D; j++) load_row(m0 + j, (int)((m0 + j) % slots));
     for (uint64_t m = m0; m < m1; m++) {
         const uint64_t j = m - m0;
         if ((j & (KEC_THREADS - 1)) == 0) {
@@ -284,10 +285,10 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
                 sel[2 * tid + 1] = gl::sub(x, a.omega_h_inv);
             }
         }
-        load_row(m + 2, (int)((m + 2) % 3));
+        load_row(m + a.D, (int)((m + a.D) % slots));
         __syncthreads();
-        const uint64_t *L = ring + (m % 3) * KC_NCOLS;
-        const uint64_t *N = ring + ((m + 2) % 3) * KC_NCOLS;
+        const uint64_t *L = ring + (m % slots) * KC_NCOLS;
+        const uint64_t *N = ring + ((m + a.D) % slots) * KC_NCOLS;
         const uint64_t first = sel[2 * (j & (KEC_THREADS - 1))], trans = sel[2 * (j & (KEC_THREADS - 1)) + 1];
         KFold f(a.alpha_pows);
         for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task<uint64_t, KTabDev>(t, L, N, first, trans, f);
@@ -311,11 +312,13 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
             o[0] = gl::add(o[0], c0);
             o[1] = gl::add(o[1], c1);
         }
-        // slot (m % 3) is overwritten by row m + 3 in the next iteration
+        // slot (m % (D + 1)) is overwritten by row m + D + 1 in the next iteration
         __syncthreads();
     }
 }
-constexpr size_t KEC_SMEM = (3 * KC_NCOLS + 2 * KEC_THREADS + 16) * 8;
+// shared memory of a launch with quotient degree D (at most 8: 194 KB)
+inline size_t kec_smem(uint64_t D) { return ((D + 1) * KC_NCOLS + 2 * KEC_THREADS + 16) * 8; }
+constexpr size_t KEC_SMEM_MAX = (9 * KC_NCOLS + 2 * KEC_THREADS + 16) * 8;
 
 // acc[0..old) *= beta (EF); then acc[i] = acc[i mod old] for i in [old, new)
 __global__ void scale_ef_kernel(uint64_t *acc, uint64_t n, gl::ef beta) {

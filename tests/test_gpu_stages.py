@@ -200,3 +200,35 @@ def test_proof_from_device_cubic_trace(product, gpu_ctx):
     orc = O.prove(O.default_p2(), dict(log_blowup=3, log_folding_arity=2, log_final_degree=0, folding_pow_bits=6,
                                        deep_pow_bits=0, num_queries=20, query_pow_bits=0), [(O.AIR_CUBIC, th, kh)])
     assert np.array_equal(gpu.proof.fields, orc["fields"]) and np.array_equal(gpu.digest, orc["digest"])
+
+
+@pytest.mark.parametrize("split", [(6, 6), (4, 8), (10, 2), (3, 3, 3, 3), (2, 10)])
+def test_lde_split_does_not_change_values(product, gpu_ctx, split):
+    """Any split of the transform's bits into passes computes the same LDE
+    (the autotuner only changes the time)."""
+    rng = np.random.default_rng(sum(split))
+    t = rand_mat(rng, 1 << 12, 24)
+    want = O.coset_lde_bitrev(t, 2, 7)
+    gpu_ctx.set_lde_split(12, list(split))
+    try:
+        got = product.to_host(product.coset_lde(gpu_ctx, product.to_device(t), 2, 7))
+    finally:
+        gpu_ctx.set_lde_split(12, [])
+    assert np.array_equal(got, want)
+
+
+def test_autotuner_keeps_a_valid_split(product, gpu_ctx):
+    r = gpu_ctx.autotune_lde(14, 16, 1, 1)
+    assert sum(r["split"]) == 14 and all(1 <= k <= 10 for k in r["split"]) and r["ms"] <= r["default_ms"] + 1e-9
+    rng = np.random.default_rng(3)
+    t = rand_mat(rng, 1 << 14, 16)
+    try:
+        got = product.to_host(product.coset_lde(gpu_ctx, product.to_device(t), 1, 7))
+    finally:
+        gpu_ctx.set_lde_split(14, [])
+    assert np.array_equal(got, O.coset_lde_bitrev(t, 1, 7))
+    s = gpu_ctx.autotune_slabs(12, 64, 1, 1)
+    assert s["slab_cols"] % 8 == 0
+    gpu_ctx.set_slab_columns(0)
+    with pytest.raises(product.P3gError):
+        gpu_ctx.set_lde_split(12, [11, 1])
