@@ -534,6 +534,39 @@ def run_named(args):
     return 0
 
 
+def run_symbolic(args):
+    """The headline proof (Keccak AIR, 10922 permutations, 2^18 x 2633) with
+    the AIR given as symbolic constraints (tests/sym_airs.py's AirBuilder
+    form) and its constraint kernels generated and compiled by the library,
+    next to the hand-written Keccak kernel on the same trace: per-stage
+    device time of both, and the generated kernels' compile time."""
+    import torch
+    dev = 0
+    torch.cuda.set_device(dev)
+    P = load_product()
+    sys.path.insert(0, str(ROOT / "tests"))
+    import sym_airs as S
+    ctx = P.Context(dev)
+    tuning = apply_tuning(ctx)
+    t0 = time.perf_counter()
+    air = P.Air(ctx, P.build_air(S.keccak_eval, S.KC_NCOLS))
+    compile_s = time.perf_counter() - t0
+    t = P.generate_keccak_trace(P.keccak_inputs(1, N_PERMS))
+    d = torch.from_numpy(t.view(np.int64)).to(f"cuda:{dev}")
+    del t
+    pcs = P.PcsParams(**PCS)
+    out = {}
+    for name, a in (("generated", air), ("hand-written", P.AIR_KECCAK)):
+        lat, stages, launches, o, clk = time_proofs(P, ctx, pcs, [P.AirWitness(a, d)], args.steps, args.warmup, dev)
+        out[name] = {"ms_per_proof": float(np.mean(lat)), "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages)},
+                     "digest": [int(x) for x in o.digest[:4]], "clocks": clk}
+    assert out["generated"]["digest"] == out["hand-written"]["digest"], "generated and hand-written proofs differ"
+    print(json.dumps({"workload": f"{workload_name()}, AIR as symbolic constraints (3182, 40470 DAG nodes)",
+                      "compile_s": compile_s, "tuning": tuning, **out}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_verify(args):
     """Verification of the headline proof (2^18 x 2633 Keccak, the example's
     parameters) through the public call p3g_verify: transcript replay on the
@@ -779,11 +812,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--log-h", type=int, default=18,
                     help="trace height (log2); 18 is the measured workload, smaller values are profiling cases")
-    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve", "slab", "verify"],
+    ap.add_argument("--workload", default="keccak", choices=["keccak", "small", "lifted", "batch", "serve", "slab", "verify", "symbolic"],
                     help="keccak: the plain prover at scale (headline); small: 42-permutation Keccak proof; "
                          "lifted: three cubic traces lifted to 2^20; batch: 64-proof uneven mix; serve: Poisson stream; "
                          "slab: one 2^18 x 336 column slab through the LDE and the tree (kernel profiling); "
-                         "verify: the device-side verifier on the headline proof")
+                         "verify: the device-side verifier on the headline proof; "
+                         "symbolic: the headline proof through generated constraint kernels")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3, help="batch: alternating passes per arm (median kept)")
@@ -812,6 +846,8 @@ def main():
         return run_slab(args)
     if args.workload == "verify":
         return run_verify(args)
+    if args.workload == "symbolic":
+        return run_symbolic(args)
     return run_gpu(args)
 
 

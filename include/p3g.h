@@ -307,7 +307,9 @@ uint64_t p3g_coset_lde_noalloc_max_words(void);
  * for this context and returns it (best_sizes, *n_sizes capacity on entry,
  * count on return) with its time per LDE and the default split's.
  * p3g_autotune_slabs does the same for the column-slab width of the main
- * commit (LDE + leaf sponge + tree of a device trace). The setters load a
+ * commit (LDE + leaf sponge + tree of a device trace; the tuned width
+ * applies to device-resident traces, host traces keep about 8 slabs so their
+ * upload overlaps the hash). The setters load a
  * saved choice (n = 0 / cols = 0 restore the defaults; a split must have
  * ranges of 1..10 bits adding up to log_height, a slab width must be a
  * multiple of 8, the sponge rate). */

@@ -91,7 +91,8 @@ P3G_API int p3g_autotune_lde(p3g_ctx *x, uint32_t log_height, uint64_t width, ui
 
 // Times the main commit (coset LDE of every slab plus the leaf sponge and
 // the tree) of a device-resident 2^log_height x width trace at log_blowup
-// for slab widths of about width/16 .. width (multiples of 8), keeps the
+// for slab widths of about width/16 .. width (multiples of 8, the last one
+// rounded up past the width: one slab), keeps the
 // fastest for this context and returns it with its time and the default's.
 P3G_API int p3g_autotune_slabs(p3g_ctx *x, uint32_t log_height, uint64_t width, uint32_t log_blowup, uint32_t reps,
                                uint64_t *best_cols, double *best_ms, double *default_ms) {
@@ -107,7 +108,8 @@ P3G_API int p3g_autotune_slabs(p3g_ctx *x, uint32_t log_height, uint64_t width, 
         p3g::Instance I{p3g::AIR_CUBIC, 1, h, width, tr.p, nullptr, 0};
         std::vector<uint64_t> cands;
         for (uint64_t div : {16, 8, 4, 2, 1}) {
-            uint64_t sw = std::min<uint64_t>(width, ((width + div - 1) / div + 7) / 8 * 8);
+            // a multiple of the rate: the last slab of a trace takes what is left
+            uint64_t sw = ((width + div - 1) / div + 7) / 8 * 8;
             if (std::find(cands.begin(), cands.end(), sw) == cands.end()) cands.push_back(sw);
         }
         cands.push_back(0);  // the default rule

@@ -180,7 +180,9 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
     for (size_t i = 0; i < n_inst; i++) {
         uint64_t w = inst[i].width, h = inst[i].height;
         uint64_t sw = w >= 256 ? ((w + 7) / 8 + 7) / 8 * 8 : w;  // about 8 slabs for wide traces
-        if (ctx.slab_cols) sw = std::min<uint64_t>(w, ctx.slab_cols);  // tuned: a multiple of the rate (8)
+        // tuned width (a multiple of the rate, 8) for device-resident traces; a
+        // host trace keeps about 8 slabs so that its upload hides under the hash
+        if (ctx.slab_cols && inst[i].trace_on_device) sw = std::min<uint64_t>(w, ctx.slab_cols);
         for (uint64_t c0 = 0; c0 < w; c0 += sw) {
             slabs.push_back({i, c0, std::min(sw, w - c0)});
             max_slab_hw = std::max(max_slab_hw, h * std::min(sw, w - c0));
