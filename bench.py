@@ -738,10 +738,22 @@ def run_batch(args):
     run_pool(P, jobs, 1, dev, args.budget)
     # alternate the two arms and keep the median pass of each: single passes
     # of the same list vary by several percent
-    p_runs, b_runs = [], []
-    for _ in range(args.reps):
-        p_runs.append(run_pool(P, jobs, 1, dev, args.budget))
-        b_runs.append(run_pool(P, jobs, args.workers, dev, args.budget))
+    p_runs, b_runs, diag = [], [], []
+    import psutil
+
+    def note(arm, run):
+        res, span = run[0], run[1]
+        free, total = torch.cuda.mem_get_info(dev)
+        diag.append({"arm": arm, "proofs_per_s": len(jobs) / span,
+                     "device_ms_sum": float(sum(r.output.device_ms for r in res)),
+                     "device_free_gb": free / 1e9, "host_rss_gb": psutil.Process().memory_info().rss / 1e9})
+
+    with ClockSampler(dev) as clocks:
+        for _ in range(args.reps):
+            p_runs.append(run_pool(P, jobs, 1, dev, args.budget))
+            note("plain", p_runs[-1])
+            b_runs.append(run_pool(P, jobs, args.workers, dev, args.budget))
+            note("pooled", b_runs[-1])
     p_runs.sort(key=lambda r: r[1])
     b_runs.sort(key=lambda r: r[1])
     plain, span1, _, lat1, _ = p_runs[len(p_runs) // 2]
@@ -762,6 +774,8 @@ def run_batch(args):
         "passes": {"plain_proofs_per_s": [len(jobs) / r[1] for r in p_runs],
                    "batched_proofs_per_s": [len(jobs) / r[1] for r in b_runs]},
         "bit_identical_to_plain": True,
+        "pass_diagnostics": diag,
+        "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0

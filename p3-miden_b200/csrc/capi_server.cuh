@@ -75,10 +75,6 @@ P3G_API int p3g_server_create(int device, const uint64_t *poseidon2_params130, u
         CK(cudaSetDevice(device));
         p3g::ensure_keccak_tables(device);
         srv->device = device;
-        cudaMemPool_t pool;
-        CK(cudaDeviceGetDefaultMemPool(&pool, device));
-        uint64_t thr = UINT64_MAX;
-        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
         srv->s = std::make_unique<p3g::Server>(device, poseidon2_params130, n_workers, hbm_budget_bytes);
     } catch (const p3g::CudaError &e) {
         delete srv;

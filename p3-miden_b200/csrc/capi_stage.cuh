@@ -36,11 +36,7 @@ P3G_API int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_
         CK(cudaStreamCreateWithFlags(&x->c.stream, cudaStreamNonBlocking));
         memcpy(x->c.p2, poseidon2_params130, sizeof(x->c.p2));
         p3g::bind_p2(x->c);
-        // keep freed blocks in the pool across proofs
-        cudaMemPool_t pool;
-        CK(cudaDeviceGetDefaultMemPool(&pool, device));
-        uint64_t thr = UINT64_MAX;
-        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        x->c.make_pool();
     } catch (const p3g::CudaError &e) {
         delete x;
         return e.status;

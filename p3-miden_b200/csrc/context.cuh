@@ -93,6 +93,22 @@ struct Ctx {
     std::map<uint32_t, std::vector<uint32_t>> lde_split;
     uint64_t slab_cols = 0;
 
+    // This context's own stream-ordered memory pool. Buffers freed by one
+    // context are reused only by that context, so two contexts driving the
+    // same device (server workers) never wait on each other's frees, and the
+    // memory goes back to the device when the context is released. Freed
+    // blocks stay in the pool between proofs (release threshold: unlimited).
+    cudaMemPool_t pool = nullptr;
+    void make_pool() {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        CK(cudaMemPoolCreate(&pool, &props));
+        uint64_t thr = UINT64_MAX;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    }
     void pipeline_streams() {
         if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
         if (!copy_stream) CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
@@ -110,13 +126,20 @@ struct Ctx {
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
         lde_stream = copy_stream = stream = nullptr;
+        // buffers still held elsewhere (a tree the caller has not freed) keep
+        // the pool alive until they are freed
+        if (pool) cudaMemPoolDestroy(pool);
+        pool = nullptr;
     }
 
     DBuf alloc(size_t words) {
         DBuf b;
         b.s = stream;
         b.words = words;
-        if (words) CK(cudaMallocAsync((void **)&b.p, words * 8, stream));
+        if (words) {
+            if (pool) CK(cudaMallocFromPoolAsync((void **)&b.p, words * 8, pool, stream));
+            else CK(cudaMallocAsync((void **)&b.p, words * 8, stream));
+        }
         return b;
     }
     uint64_t *stage(size_t words) {

@@ -83,6 +83,13 @@ class Server {
             auto c = std::make_unique<Ctx>();
             c->device = device;
             CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            c->make_pool();
+            // a worker's pool keeps at most its share of the budget between
+            // jobs; memory above it goes back to the device at the next
+            // synchronisation, so the workers' pools together stay within
+            // the budget the admission rule assumes
+            uint64_t share = hbm_budget / n_workers;
+            CK(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &share));
             memcpy(c->p2, p2, sizeof(c->p2));
             ctxs_.push_back(std::move(c));
         }
