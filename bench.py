@@ -710,15 +710,13 @@ def build_jobs(P, specs, device, pinned):
     return jobs
 
 
-def run_pool(P, jobs, workers, device, budget, self_check=False):
-    srv = P.ProofServer(device, n_workers=workers, hbm_budget=budget, self_check=self_check)
-    try:
-        t0 = time.perf_counter()
-        res = srv.run(jobs)
-        wall = time.perf_counter() - t0
-        peak = srv.peak_admitted_bytes()
-    finally:
-        srv.close()
+def run_pool(P, jobs, srv):
+    """One pass of a job list through a running server (its workers, streams
+    and memory pools persist across passes, as in a serving process)."""
+    t0 = time.perf_counter()
+    res = srv.run(jobs)
+    wall = time.perf_counter() - t0
+    peak = srv.peak_admitted_bytes()
     bad = [r.status for r in res if r.status != P.OK]
     assert not bad, f"failed jobs: {bad}"
     span = max(r.end_s for r in res) - min(r.submit_s for r in res)
@@ -733,9 +731,12 @@ def run_batch(args):
     P = load_product()
     specs = job_specs(args.jobs, args.seed, args.max_log_cubic, args.max_log_keccak)
     jobs = build_jobs(P, specs, dev, pinned=False)
-    # warm-up over the whole list, so that neither arm pays for growing the
-    # stream-ordered memory pool or for first-use tables
-    run_pool(P, jobs, 1, dev, args.budget)
+    srv_plain = P.ProofServer(dev, n_workers=1, hbm_budget=args.budget)
+    srv_pool = P.ProofServer(dev, n_workers=args.workers, hbm_budget=args.budget)
+    # warm-up over the whole list on both servers, so that neither arm pays
+    # for growing its memory pools or for first-use tables in the timed passes
+    run_pool(P, jobs, srv_plain)
+    run_pool(P, jobs, srv_pool)
     # alternate the two arms and keep the median pass of each: single passes
     # of the same list vary by several percent
     p_runs, b_runs, diag = [], [], []
@@ -750,10 +751,12 @@ def run_batch(args):
 
     with ClockSampler(dev) as clocks:
         for _ in range(args.reps):
-            p_runs.append(run_pool(P, jobs, 1, dev, args.budget))
+            p_runs.append(run_pool(P, jobs, srv_plain))
             note("plain", p_runs[-1])
-            b_runs.append(run_pool(P, jobs, args.workers, dev, args.budget))
+            b_runs.append(run_pool(P, jobs, srv_pool))
             note("pooled", b_runs[-1])
+    srv_plain.close()
+    srv_pool.close()
     p_runs.sort(key=lambda r: r[1])
     b_runs.sort(key=lambda r: r[1])
     plain, span1, _, lat1, _ = p_runs[len(p_runs) // 2]
@@ -792,13 +795,15 @@ def run_serve(args):
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=args.jobs))
     picks = rng.integers(0, len(pool), size=args.jobs)
     stream = [P.Job(pool[k].pcs, pool[k].instances, float(a)) for k, a in zip(picks, arrivals)]
-    run_pool(P, pool, 1, dev, args.budget)  # warm-up over every distinct job
     out = {}
     arms = [("plain", 1, False), ("served", args.workers, False)]
     if args.self_check:  # every served proof verified on the device before it is returned
         arms.append(("served+self-check", args.workers, True))
     for name, workers, check in arms:
-        res, span, wall, lat, peak = run_pool(P, stream, workers, dev, args.budget, self_check=check)
+        srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check)
+        run_pool(P, pool, srv)  # warm-up over every distinct job
+        res, span, wall, lat, peak = run_pool(P, stream, srv)
+        srv.close()
         out[name] = {"proofs_per_s": len(stream) / span, "p50_ms": float(np.percentile(lat, 50)),
                      "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "peak_admitted_gb": peak / 1e9,
                      "workers": workers}
