@@ -482,9 +482,10 @@ SMALL_PCS = PCS
 def time_proofs(P, ctx, pcs, wits, steps, warmup, dev):
     """Device-timed prove_multi on resident witnesses: per-proof ms, stage ms, last output."""
     import torch
+    ref = None
     for _ in range(warmup):
         out = P.prove_multi(ctx, pcs, wits)
-    ref = out.digest.copy()
+        ref = out.digest.copy()
     torch.cuda.synchronize(dev)
     lat, stages, launches = [], np.zeros(len(P.STAGES)), 0
     with ClockSampler(dev) as clocks:
@@ -493,6 +494,8 @@ def time_proofs(P, ctx, pcs, wits, steps, warmup, dev):
             lat.append(out.device_ms)
             stages += np.array(out.stage_ms)
             launches += out.gpu_launches
+            if ref is None:
+                ref = out.digest.copy()
             assert np.array_equal(out.digest, ref), "non-deterministic proof"
     return lat, stages / steps, launches, out, clocks.summary()
 
