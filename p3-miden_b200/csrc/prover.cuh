@@ -659,9 +659,11 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
                 CK(cudaFuncSetAttribute(quot::keccak_eval_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)quot::KEC_SMEM_MAX));
             });
-            int dev_sms = 148;
+            int dev_sms = 148, per_sm = 1;
             CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx.device));
-            uint64_t blocks = std::min<uint64_t>(qh, (uint64_t)dev_sms * 3);
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, quot::keccak_eval_block_kernel,
+                                                             quot::KEC_THREADS, quot::kec_smem(D)));
+            uint64_t blocks = std::min<uint64_t>(qh, (uint64_t)dev_sms * std::max(1, per_sm));
             uint64_t ppb = (qh + blocks - 1) / blocks;
             blocks = (qh + ppb - 1) / ppb;
             L(quot::keccak_eval_block_kernel, (unsigned)blocks, quot::KEC_THREADS, quot::kec_smem(D), a, ppb);

@@ -210,7 +210,7 @@ struct KArgs {
 // each chunk is one kernel that adds its part of the fold into acc. The fold
 // is linear, so launching the chunks one after another on the same stream
 // gives the same sum. A small AIR is one chunk.
-constexpr size_t kChunkNodes = 400;
+constexpr size_t kChunkNodes = 800;
 
 inline void split_chunks(Air &A) {
     const Desc &d = A.d;
@@ -311,8 +311,13 @@ struct KArgs {
             if (last) o << "    const uint64_t s_last = gl::mul(zh, gl::inv(gl::sub(x, a.omega_h_inv)));\n";
             if (trans) o << "    const uint64_t s_trans = gl::sub(x, a.omega_h_inv);\n";
         }
+        // two passes over the live nodes: first every load (trace cells,
+        // constants of the call, periodic values), so that they are all in
+        // flight together, then the arithmetic in topological order
+        auto is_leaf = [](uint32_t op) { return op != ADD && op != SUB && op != MUL && op != NEG; };
+        for (int pass = 0; pass < 2; pass++)
         for (size_t i = 0; i < n; i++) {
-            if (!live[i]) continue;
+            if (!live[i] || is_leaf(d.nodes[i].op) != (pass == 0)) continue;
             const Node &x = d.nodes[i];
             const std::string v = "v" + std::to_string(i);
             const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
@@ -449,8 +454,13 @@ inline void compile(Air &A, int device) {
         cudaLibrary_t lib = nullptr;
         CK(cudaLibraryLoadData(&lib, A.cubins[g].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
         A.libs.push_back(lib);
-        for (size_t c = nch * g / groups; c < nch * (g + 1) / groups; c++)
+        for (size_t c = nch * g / groups; c < nch * (g + 1) / groups; c++) {
             CK(cudaLibraryGetKernel(&A.kernels[c], lib, ("p3g_sym_eval_" + std::to_string(c)).c_str()));
+            // load the kernel into the device's context now rather than at its
+            // first launch (lazy loading would put it inside the first proof)
+            cudaFuncAttributes attr;
+            CK(cudaFuncGetAttributes(&attr, (const void *)A.kernels[c]));
+        }
     }
     A.device = device;
 }
