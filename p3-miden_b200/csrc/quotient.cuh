@@ -251,24 +251,19 @@ GL_HD void keccak_task(int t, const T *L, const T *N, T first, T trans, F &f) {
     }
 }
 
-// Persistent blocks over contiguous point ranges, one barrier per point.
-// Rows are staged in a ring of D + 2 shared-memory slots: point m needs rows
-// m and m + D (D = 2 for this AIR alone; up to 8 when it is proved beside an
-// AIR of higher degree), and row m + D + 1 is fetched while point m is
-// evaluated, into the slot of row m - 1, which nobody reads after the
-// previous barrier. Each LDE row is read from HBM once per block range.
-// Selectors (one inversion per point) are computed cooperatively 256 points
-// ahead into the other half of a double buffer, and the per-warp partial
-// sums alternate between two buffers, so a value written in one iteration is
-// read only after the next barrier.
+// Persistent blocks over contiguous point ranges. Rows are staged in a ring
+// of D + 1 shared-memory slots: point m needs rows m and m + D (D = 2 for
+// this AIR alone; up to 8 when it is proved beside an AIR of higher degree),
+// so each LDE row is read from HBM once per block range. Selectors for the
+// next 256 points are computed cooperatively (one inversion per point).
 constexpr int KEC_THREADS = 256;
 __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __grid_constant__ EvalArgs a,
                                                                          uint64_t points_per_block) {
     extern __shared__ uint64_t sm[];
-    const uint32_t slots = (uint32_t)a.D + 2;
-    uint64_t *ring = sm;                        // (D + 2) x 2633
-    uint64_t *sel = sm + slots * KC_NCOLS;      // 2 halves x 256 x {first, trans}
-    uint64_t *red = sel + 4 * KEC_THREADS;      // 2 buffers x 8 warps x 2
+    const uint32_t slots = (uint32_t)a.D + 1;
+    uint64_t *ring = sm;                        // (D + 1) x 2633
+    uint64_t *sel = sm + slots * KC_NCOLS;      // 256 x {first, trans}
+    uint64_t *red = sel + 2 * KEC_THREADS;      // 8 warps x 2
     const uint64_t qh = 1ull << a.log_qh;
     const uint64_t m0 = (uint64_t)blockIdx.x * points_per_block;
     if (m0 >= qh) return;
@@ -279,25 +274,22 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
         uint64_t *dst = ring + slot * KC_NCOLS;
         for (int c = tid; c < KC_NCOLS; c += KEC_THREADS) dst[c] = __ldg(src + c);
     };
-    auto fill_sel = [&](uint64_t base, int half) {
-        const uint64_t pm = base + tid;
-        if (pm < m1) {
-            const uint64_t x = point_x(a, pm);
-            sel[half * 2 * KEC_THREADS + 2 * tid] = gl::mul(a.zh[pm & (a.D - 1)], gl::inv(gl::sub(x, 1)));
-            sel[half * 2 * KEC_THREADS + 2 * tid + 1] = gl::sub(x, a.omega_h_inv);
-        }
-    };
-    for (uint64_t j = 0; j <= a.D; j++) load_row(m0 + j, (int)((m0 + j) % slots));
-    fill_sel(m0, 0);
-    __syncthreads();
+    for (uint64_t j = 0; j < a.D; j++) load_row(m0 + j, (int)((m0 + j) % slots));
     for (uint64_t m = m0; m < m1; m++) {
         const uint64_t j = m - m0;
-        if (m + 1 < m1) load_row(m + a.D + 1, (int)((m + a.D + 1) % slots));
-        if ((j & (KEC_THREADS - 1)) == 0) fill_sel(m + KEC_THREADS, (int)(((j >> 8) + 1) & 1));
+        if ((j & (KEC_THREADS - 1)) == 0) {
+            uint64_t pm = m + tid;
+            if (pm < m1) {
+                uint64_t x = point_x(a, pm);
+                sel[2 * tid] = gl::mul(a.zh[pm & (a.D - 1)], gl::inv(gl::sub(x, 1)));
+                sel[2 * tid + 1] = gl::sub(x, a.omega_h_inv);
+            }
+        }
+        load_row(m + a.D, (int)((m + a.D) % slots));
+        __syncthreads();
         const uint64_t *L = ring + (m % slots) * KC_NCOLS;
         const uint64_t *N = ring + ((m + a.D) % slots) * KC_NCOLS;
-        const uint64_t *sh = sel + ((j >> 8) & 1) * 2 * KEC_THREADS + 2 * (j & (KEC_THREADS - 1));
-        const uint64_t first = sh[0], trans = sh[1];
+        const uint64_t first = sel[2 * (j & (KEC_THREADS - 1))], trans = sel[2 * (j & (KEC_THREADS - 1)) + 1];
         KFold f(a.alpha_pows);
         for (int t = tid; t < KEC_TASKS; t += KEC_THREADS) keccak_task<uint64_t, KTabDev>(t, L, N, first, trans, f);
         uint64_t c0 = f.c0.reduce(), c1 = f.c1.reduce();
@@ -306,26 +298,27 @@ __global__ void __launch_bounds__(KEC_THREADS) keccak_eval_block_kernel(const __
             c0 = gl::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
             c1 = gl::add(c1, __shfl_xor_sync(0xffffffffu, c1, off));
         }
-        uint64_t *rb = red + (j & 1) * 16;
         if (lane == 0) {
-            rb[2 * wid] = c0;
-            rb[2 * wid + 1] = c1;
+            red[2 * wid] = c0;
+            red[2 * wid + 1] = c1;
         }
         __syncthreads();
         if (tid == 0) {
             for (int w = 1; w < KEC_THREADS / 32; w++) {
-                c0 = gl::add(c0, rb[2 * w]);
-                c1 = gl::add(c1, rb[2 * w + 1]);
+                c0 = gl::add(c0, red[2 * w]);
+                c1 = gl::add(c1, red[2 * w + 1]);
             }
             uint64_t *o = a.acc + 2 * m;
             o[0] = gl::add(o[0], c0);
             o[1] = gl::add(o[1], c1);
         }
+        // slot (m % (D + 1)) is overwritten by row m + D + 1 in the next iteration
+        __syncthreads();
     }
 }
-// shared memory of a launch with quotient degree D (at most 8: 212 KB)
-inline size_t kec_smem(uint64_t D) { return ((D + 2) * KC_NCOLS + 4 * KEC_THREADS + 32) * 8; }
-constexpr size_t KEC_SMEM_MAX = (10 * KC_NCOLS + 4 * KEC_THREADS + 32) * 8;
+// shared memory of a launch with quotient degree D (at most 8: 194 KB)
+inline size_t kec_smem(uint64_t D) { return ((D + 1) * KC_NCOLS + 2 * KEC_THREADS + 16) * 8; }
+constexpr size_t KEC_SMEM_MAX = (9 * KC_NCOLS + 2 * KEC_THREADS + 16) * 8;
 
 // acc[0..old) *= beta (EF); then acc[i] = acc[i mod old] for i in [old, new)
 __global__ void scale_ef_kernel(uint64_t *acc, uint64_t n, gl::ef beta) {
