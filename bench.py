@@ -58,7 +58,8 @@ TUNING = ROOT / "p3-miden_b200" / "tuning" / "b200.json"
 
 
 def apply_tuning(ctx):
-    """Launch shapes chosen by p3-miden_b200/autotune.py on a B200, if saved."""
+    """Launch shapes chosen by p3-miden_b200/autotune.py on a B200, if saved
+    (a Context or a ProofServer)."""
     try:
         table = json.loads(TUNING.read_text())
     except Exception:
@@ -736,6 +737,8 @@ def run_batch(args):
     jobs = build_jobs(P, specs, dev, pinned=False)
     srv_plain = P.ProofServer(dev, n_workers=1, hbm_budget=args.budget)
     srv_pool = P.ProofServer(dev, n_workers=args.workers, hbm_budget=args.budget)
+    apply_tuning(srv_plain)
+    tuning = apply_tuning(srv_pool)
     # warm-up over the whole list on both servers, so that neither arm pays
     # for growing its memory pools or for first-use tables in the timed passes
     run_pool(P, jobs, srv_plain)
@@ -780,6 +783,7 @@ def run_batch(args):
         "passes": {"plain_proofs_per_s": [len(jobs) / r[1] for r in p_runs],
                    "batched_proofs_per_s": [len(jobs) / r[1] for r in b_runs]},
         "bit_identical_to_plain": True,
+        "tuning": tuning,
         "pass_diagnostics": diag,
         "clocks": clocks.summary(),
     }
@@ -804,6 +808,7 @@ def run_serve(args):
         arms.append(("served+self-check", args.workers, True))
     for name, workers, check in arms:
         srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check)
+        apply_tuning(srv)
         run_pool(P, pool, srv)  # warm-up over every distinct job
         res, span, wall, lat, peak = run_pool(P, stream, srv)
         srv.close()

@@ -400,6 +400,11 @@ int p3g_server_create(int device, const uint64_t *poseidon2_params130, uint32_t 
  * its proof with p3g_verify's checks, on its own stream, before the job ends;
  * a rejected proof ends the job with P3G_ERR_REJECTED and its verdict. */
 int p3g_server_set_self_check(p3g_server *srv, int32_t enabled);
+/* No counterpart in the reference: saved launch shapes (as
+ * p3g_ctx_set_lde_split / p3g_ctx_set_slab_columns) for every worker; call
+ * before submitting jobs. */
+int p3g_server_set_lde_split(p3g_server *srv, uint32_t log_height, const uint32_t *sizes, uint32_t n);
+int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols);
 /* Waits for every submitted job, then releases the workers. */
 void p3g_server_destroy(p3g_server *srv);
 int p3g_server_submit(p3g_server *srv, const p3g_job *job, uint64_t *ticket);

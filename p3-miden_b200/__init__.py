@@ -930,6 +930,8 @@ class ProofServer:
             ("p3g_server_run", C.c_int, [vp, C.POINTER(JobC), C.c_uint64, C.POINTER(JobResultC)]),
             ("p3g_server_peak_admitted_bytes", C.c_uint64, [vp]),
             ("p3g_server_set_self_check", C.c_int, [vp, C.c_int32]),
+            ("p3g_server_set_lde_split", C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+            ("p3g_server_set_slab_columns", C.c_int, [vp, C.c_uint64]),
             ("p3g_job_footprint_bytes", C.c_uint64, [C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64]),
         ]:
             fn = getattr(L, name)
@@ -941,6 +943,15 @@ class ProofServer:
         self._pending = {}
         if self_check:
             _check(L.p3g_server_set_self_check(self._h, 1))
+
+    def load_tuning(self, table: dict):
+        """Apply a saved tuning table to every worker (Context.load_tuning's format)."""
+        L = lib()
+        for lh, sizes in table.get("lde_split", {}).items():
+            arr = (C.c_uint32 * max(1, len(sizes)))(*sizes)
+            _check(L.p3g_server_set_lde_split(self._h, int(lh), arr, len(sizes)))
+        if table.get("slab_cols"):
+            _check(L.p3g_server_set_slab_columns(self._h, int(table["slab_cols"])))
 
     def run(self, jobs: list[Job]) -> list[JobResult]:
         """Submit every job at its arrival time (seconds from now) and wait for all."""

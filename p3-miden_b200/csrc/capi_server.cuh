@@ -99,6 +99,21 @@ P3G_API int p3g_server_set_self_check(p3g_server *srv, int32_t enabled) {
     return p3g::OK;
 }
 
+// Saved launch shapes (p3g_ctx_set_lde_split / p3g_ctx_set_slab_columns) for
+// every worker of the server; call before submitting jobs.
+P3G_API int p3g_server_set_lde_split(p3g_server *srv, uint32_t log_height, const uint32_t *sizes, uint32_t n) {
+    if (!srv || (n && !sizes)) return p3g::ERR_INVALID;
+    std::vector<uint32_t> v(sizes, sizes + n);
+    if (n && !p3g::valid_split(log_height, v)) return p3g::ERR_INVALID;
+    srv->s->set_lde_split(log_height, v);
+    return p3g::OK;
+}
+P3G_API int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols) {
+    if (!srv || (cols % 8) != 0) return p3g::ERR_INVALID;
+    srv->s->set_slab_columns(cols);
+    return p3g::OK;
+}
+
 P3G_API int p3g_server_submit(p3g_server *srv, const p3g_job_c *job, uint64_t *ticket) {
     if (!srv || !job || !ticket) return p3g::ERR_INVALID;
     int v = p3g::validate(&job->pcs, job->instances, job->n_instances);

@@ -133,6 +133,19 @@ class Server {
     // the worker's own stream); a rejected proof ends its job with
     // ERR_REJECTED.
     void set_self_check(bool on) { self_check_ = on; }
+    // Tuned launch shapes for every worker (p3g_autotune_*); call before
+    // submitting jobs.
+    void set_lde_split(uint32_t log_h, const std::vector<uint32_t> &sizes) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto &c : ctxs_) {
+            if (sizes.empty()) c->lde_split.erase(log_h);
+            else c->lde_split[log_h] = sizes;
+        }
+    }
+    void set_slab_columns(uint64_t cols) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto &c : ctxs_) c->slab_cols = cols;
+    }
 
    private:
     void worker(uint32_t w) {
