@@ -222,6 +222,37 @@ __global__ void bitrev_rows_kernel(const uint64_t *in, uint64_t *out, uint32_t L
     out[r * w + c] = in[gl::bitrev(r, L) * w + c];
 }
 
+// Column-major copy of the first n rows of a row-major matrix of w columns
+// (row stride ld words): out[c * n + r] = in[r * ld + c]. 32 x 32 tiles
+// through shared memory, rows on grid.x and column tiles on grid.y; both the
+// loads (32 columns of a row) and the stores (32 rows of a column) are
+// 256-byte runs.
+__global__ void __launch_bounds__(256) transpose_kernel(const uint64_t *in, uint64_t ld, uint64_t *out, uint64_t n,
+                                                        uint64_t w) {
+    __shared__ uint64_t t[32][33];
+    const uint64_t r0 = (uint64_t)blockIdx.x * 32, c0 = (uint64_t)blockIdx.y * 32;
+    const uint32_t tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (uint32_t j = 0; j < 32; j += 8) {
+        const uint64_t r = r0 + ty + j, c = c0 + tx;
+        if (r < n && c < w) t[ty + j][tx] = __ldg(in + r * ld + c);
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t j = 0; j < 32; j += 8) {
+        const uint64_t c = c0 + ty + j, r = r0 + tx;
+        if (r < n && c < w) out[c * n + r] = t[tx][ty + j];
+    }
+}
+inline void transpose(Ctx &ctx, const uint64_t *in, uint64_t ld, uint64_t *out, uint64_t n, uint64_t w) {
+    if (!n || !w) return;
+    if ((w + 31) / 32 > 65535) throw CudaError{ERR_INVALID, "transpose: too many columns"};
+    transpose_kernel<<<dim3((unsigned)((n + 31) / 32), (unsigned)((w + 31) / 32)), dim3(32, 8), 0, ctx.stream>>>(
+        in, ld, out, n, w);
+    CK(cudaGetLastError());
+    ctx.launches++;
+}
+
 // Host-built two-level power table of v for exponents < 2^L.
 inline void pow_table(uint64_t v, uint32_t L, uint32_t lo_bits, std::vector<uint64_t> &out_lo,
                       std::vector<uint64_t> &out_hi) {

@@ -293,6 +293,8 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
 
 // Constraint evaluation of a symbolic AIR on gJ with its generated kernel
 // (symair.cuh): one thread per point, acc[m] += sum_k alpha^{K-1-k} C_k(x_m).
+// The kernels read column-major copies of gJ's rows of the main and aux LDEs
+// (one transpose each), so that every cell load of a warp is one 256-byte run.
 // Periodic columns: PeriodicLde::build on the quotient coset (blowup D,
 // shift (g^{2^lift})^{h / max_period}, natural order; periodic.rs:49-98).
 inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde, const uint64_t *aux_lde,
@@ -328,10 +330,17 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde,
         ctx.sync();
     }
     const TwTables &twq = ctx.twiddles(log_h + log_qd);
+    // the generated kernels read gJ's rows of the LDEs column-major
+    DBuf main_cm = ctx.alloc(qh * I.width), aux_cm;
+    transpose(ctx, main_lde, I.width, main_cm.p, qh, I.width);
+    if (d.aux_width && aux_lde) {
+        aux_cm = ctx.alloc(qh * 2 * d.aux_width);
+        transpose(ctx, aux_lde, 2 * d.aux_width, aux_cm.p, qh, 2 * d.aux_width);
+    }
     sym::KArgs a{};
-    a.main = main_lde;
+    a.main = main_cm.p;
     a.main_w = I.width;
-    a.aux = aux_lde;
+    a.aux = aux_cm.p;
     a.aux_w2 = 2 * d.aux_width;
     a.per = per_nat.p;
     a.per_h = per_h ? per_h : 1;

@@ -187,9 +187,12 @@ inline void analyse(Air &A) {
 // Arguments of the generated kernel (the same layout is declared in the
 // generated source).
 struct KArgs {
-    const uint64_t *main;  // bit-reversed LDE of the main trace
+    // the first qh rows (the quotient domain gJ, bit-reversed) of the main
+    // and aux LDEs, column-major: cell (row r, word c) at [c * qh + r]; the
+    // aux trace has 2 words per EF column
+    const uint64_t *main;
     uint64_t main_w;
-    const uint64_t *aux;   // bit-reversed LDE of the aux trace (2 words per EF column)
+    const uint64_t *aux;
     uint64_t aux_w2;
     const uint64_t *per;   // periodic LDE on gJ, natural order
     uint64_t per_h, per_w;
@@ -292,14 +295,18 @@ struct KArgs {
         }
         o << "extern \"C\" __global__ void __launch_bounds__(128) p3g_sym_eval_" << c
           << "(const __grid_constant__ KArgs a) {\n";
-        o << R"K(    const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= a.qh) return;
-    const uint64_t rl = gl::bitrev(m, a.log_qh), rn = gl::bitrev((m + a.D) & (a.qh - 1), a.log_qh);
-    const uint64_t *ML = a.main + rl * a.main_w, *MN = a.main + rn * a.main_w;
-    const uint64_t *AL = a.aux + rl * a.aux_w2, *AN = a.aux + rn * a.aux_w2;
+        // thread r reads storage row r (point m = bitrev(r)) and the row of
+        // the point m + D: a warp's 32 rows, and its 32 next rows, each lie in
+        // one aligned 32-row block, so every column load is one 256-byte run
+        o << R"K(    const uint64_t rl = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (rl >= a.qh) return;
+    const uint32_t lq = a.log_qh;
+    const uint64_t m = gl::bitrev(rl, lq), rn = gl::bitrev((m + a.D) & (a.qh - 1), lq);
+    const uint64_t *ML = a.main + rl, *MN = a.main + rn;
+    const uint64_t *AL = a.aux ? a.aux + rl : a.aux, *AN = a.aux ? a.aux + rn : a.aux;
     const uint64_t *PR = a.per ? a.per + (m % a.per_h) * a.per_w : a.per;
     const uint64_t *K = a.k;
-    (void)ML; (void)MN; (void)AL; (void)AN; (void)PR; (void)K;
+    (void)ML; (void)MN; (void)AL; (void)AN; (void)PR; (void)K; (void)lq;
 )K";
         if (first || last || trans) {
             o << "    const uint64_t mlo = m & ((1ull << a.wq_lo_bits) - 1), mhi = m >> a.wq_lo_bits;\n"
@@ -324,10 +331,10 @@ struct KArgs {
             o << "    " << ty << v << " = ";
             switch (x.op) {
                 case CONST: o << x.value << "ull"; break;
-                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + " << x.a << ")"; break;
+                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + (" << x.a << "ull << lq))"; break;
                 case AUX:
-                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + " << 2 * x.a << "), __ldg(" << (x.b ? "AN" : "AL")
-                      << " + " << 2 * x.a + 1 << ")}";
+                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + (" << 2 * x.a << "ull << lq)), __ldg("
+                      << (x.b ? "AN" : "AL") << " + (" << 2 * x.a + 1 << "ull << lq))}";
                     break;
                 case PUBLIC: o << "__ldg(K + " << A.kl.pub + x.a << ")"; break;
                 case RANDOMNESS:
