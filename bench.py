@@ -480,8 +480,10 @@ LIFTED_PCS = dict(log_blowup=3, log_folding_arity=2, log_final_degree=0, folding
 SMALL_PCS = PCS
 
 
-def time_proofs(P, ctx, pcs, wits, steps, warmup, dev):
-    """Device-timed prove_multi on resident witnesses: per-proof ms, stage ms, last output."""
+def time_proofs(P, ctx, pcs, wits, steps, warmup, dev, per_proof=None):
+    """Device-timed prove_multi on resident witnesses: per-proof ms, stage ms
+    (mean), last output; per_proof, when given, receives each timed proof's
+    stage ms."""
     import torch
     ref = None
     for _ in range(warmup):
@@ -494,6 +496,8 @@ def time_proofs(P, ctx, pcs, wits, steps, warmup, dev):
             out = P.prove_multi(ctx, pcs, wits)
             lat.append(out.device_ms)
             stages += np.array(out.stage_ms)
+            if per_proof is not None:
+                per_proof.append([round(float(v), 2) for v in out.stage_ms])
             launches += out.gpu_launches
             if ref is None:
                 ref = out.digest.copy()
@@ -561,8 +565,11 @@ def run_symbolic(args):
     pcs = P.PcsParams(**PCS)
     out = {}
     for name, a in (("generated", air), ("hand-written", P.AIR_KECCAK)):
-        lat, stages, launches, o, clk = time_proofs(P, ctx, pcs, [P.AirWitness(a, d)], args.steps, args.warmup, dev)
+        each = []
+        lat, stages, launches, o, clk = time_proofs(P, ctx, pcs, [P.AirWitness(a, d)], args.steps, args.warmup, dev,
+                                                    each)
         out[name] = {"ms_per_proof": float(np.mean(lat)), "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages)},
+                     "ms_each": [round(float(v), 2) for v in lat], "stage_ms_each": each,
                      "digest": [int(x) for x in o.digest[:4]], "clocks": clk}
     assert out["generated"]["digest"] == out["hand-written"]["digest"], "generated and hand-written proofs differ"
     print(json.dumps({"workload": f"{workload_name()}, AIR as symbolic constraints (3182, 40470 DAG nodes)",
@@ -802,19 +809,28 @@ def run_serve(args):
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=args.jobs))
     picks = rng.integers(0, len(pool), size=args.jobs)
     stream = [P.Job(pool[k].pcs, pool[k].instances, float(a)) for k, a in zip(picks, arrivals)]
+    # the server's heavy class: LDEs above 2^26 words (every Keccak job of the mix)
+    heavy = [sum((i.trace.shape[0] << MIX_PCS["log_blowup"]) * i.trace.shape[1] for i in pool[k].instances) > 1 << 26
+             for k in picks]
     out = {}
-    arms = [("plain", 1, False), ("served", args.workers, False)]
+    arms = [("plain", 1, False, False), ("served", args.workers, False, False),
+            ("served+heavy-priority", args.workers, False, True)]
     if args.self_check:  # every served proof verified on the device before it is returned
-        arms.append(("served+self-check", args.workers, True))
-    for name, workers, check in arms:
-        srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check)
+        arms.append(("served+self-check", args.workers, True, False))
+    for name, workers, check, prio in arms:
+        srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check, heavy_priority=prio)
         apply_tuning(srv)
         run_pool(P, pool, srv)  # warm-up over every distinct job
         res, span, wall, lat, peak = run_pool(P, stream, srv)
         srv.close()
+        lat = np.asarray(lat)
+        hv = np.asarray(heavy)
         out[name] = {"proofs_per_s": len(stream) / span, "p50_ms": float(np.percentile(lat, 50)),
                      "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "peak_admitted_gb": peak / 1e9,
-                     "workers": workers}
+                     "workers": workers,
+                     "by_class": {c: {"jobs": int(m.sum()), "p50_ms": float(np.percentile(lat[m], 50)),
+                                      "p99_ms": float(np.percentile(lat[m], 99))}
+                                  for c, m in (("heavy", hv), ("light", ~hv)) if m.any()}}
         if check:
             assert all(r.verdict == 0 for r in res)
             out[name]["verify_ms_mean"] = float(np.mean([r.verify_ms for r in res]))

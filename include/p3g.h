@@ -405,6 +405,11 @@ int p3g_server_set_self_check(p3g_server *srv, int32_t enabled);
  * before submitting jobs. */
 int p3g_server_set_lde_split(p3g_server *srv, uint32_t log_height, const uint32_t *sizes, uint32_t n);
 int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols);
+/* No counterpart in the reference: heavy-job priority. Worker 0 alone takes
+ * heavy jobs (LDEs above 2^26 words), on streams of the device's greatest
+ * priority, and the other workers' light jobs fill the SMs it leaves idle.
+ * Call while no job is queued or running (P3G_ERR_INVALID otherwise). */
+int p3g_server_set_heavy_priority(p3g_server *srv, int32_t enabled);
 /* Waits for every submitted job, then releases the workers. */
 void p3g_server_destroy(p3g_server *srv);
 int p3g_server_submit(p3g_server *srv, const p3g_job *job, uint64_t *ticket);

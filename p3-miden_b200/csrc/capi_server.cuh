@@ -114,6 +114,17 @@ P3G_API int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols) {
     return p3g::OK;
 }
 
+// Heavy jobs on worker 0 at the device's greatest stream priority (see
+// Server::set_heavy_priority); call while the server is idle.
+P3G_API int p3g_server_set_heavy_priority(p3g_server *srv, int32_t enabled) {
+    if (!srv) return p3g::ERR_INVALID;
+    try {
+        return srv->s->set_heavy_priority(enabled != 0) ? p3g::OK : p3g::ERR_INVALID;
+    } catch (const p3g::CudaError &e) {
+        return e.status;
+    }
+}
+
 P3G_API int p3g_server_submit(p3g_server *srv, const p3g_job_c *job, uint64_t *ticket) {
     if (!srv || !job || !ticket) return p3g::ERR_INVALID;
     int v = p3g::validate(&job->pcs, job->instances, job->n_instances);

@@ -109,9 +109,25 @@ struct Ctx {
         uint64_t thr = UINT64_MAX;
         CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     }
+    int priority = 0;  // of this context's streams (cudaStreamCreateWithPriority; lower runs first)
     void pipeline_streams() {
-        if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
-        if (!copy_stream) CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+        if (!lde_stream) CK(cudaStreamCreateWithPriority(&lde_stream, cudaStreamNonBlocking, priority));
+        if (!copy_stream) CK(cudaStreamCreateWithPriority(&copy_stream, cudaStreamNonBlocking, priority));
+    }
+    // New streams of priority p for an idle context: buffers ordered on the
+    // old streams (the twiddle tables) are freed first and rebuilt on use.
+    void set_priority(int p) {
+        if (stream) CK(cudaStreamSynchronize(stream));
+        if (lde_stream) CK(cudaStreamSynchronize(lde_stream));
+        if (copy_stream) CK(cudaStreamSynchronize(copy_stream));
+        tw.clear();
+        if (stream) CK(cudaStreamSynchronize(stream));
+        if (lde_stream) cudaStreamDestroy(lde_stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (stream) cudaStreamDestroy(stream);
+        lde_stream = copy_stream = stream = nullptr;
+        priority = p;
+        CK(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, priority));
     }
     // free stream-ordered buffers, then the streams (used at teardown)
     void release() {

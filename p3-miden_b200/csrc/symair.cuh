@@ -318,13 +318,16 @@ struct KArgs {
             if (last) o << "    const uint64_t s_last = gl::mul(zh, gl::inv(gl::sub(x, a.omega_h_inv)));\n";
             if (trans) o << "    const uint64_t s_trans = gl::sub(x, a.omega_h_inv);\n";
         }
-        // two passes over the live nodes: first every load (trace cells,
-        // constants of the call, periodic values), so that they are all in
-        // flight together, then the arithmetic in topological order
-        auto is_leaf = [](uint32_t op) { return op != ADD && op != SUB && op != MUL && op != NEG; };
-        for (int pass = 0; pass < 2; pass++)
-        for (size_t i = 0; i < n; i++) {
-            if (!live[i] || is_leaf(d.nodes[i].op) != (pass == 0)) continue;
+        // constraint by constraint: the nodes of its expression not emitted
+        // yet, in post-order (each load just before its first use), then its
+        // term of the fold, so that a value lives only while a later node of
+        // the chunk still reads it (register pressure sets the occupancy of
+        // these long straight-line kernels). Base constraints go into two lazy
+        // accumulators (one per coordinate of alpha^{K-1-k}), extension
+        // constraints into an extension sum.
+        std::vector<uint8_t> done(n, 0);
+        std::vector<std::pair<uint32_t, bool>> st;
+        auto emit_node = [&](size_t i) {
             const Node &x = d.nodes[i];
             const std::string v = "v" + std::to_string(i);
             const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
@@ -365,13 +368,26 @@ struct KArgs {
                     break;
             }
             o << ";\n";
-        }
-        // this chunk's part of the fold: base constraints on two lazy
-        // accumulators (one per coordinate of alpha^{K-1-k}), extension
-        // constraints as extension products
+        };
         o << "    gl::Acc f0, f1;\n    gl::ef fe = gl::ef_zero();\n";
         for (uint32_t k : ks) {
             const uint32_t cn = d.constraints[k];
+            st.assign(1, {cn, false});
+            while (!st.empty()) {  // iterative post-order over the nodes not emitted yet
+                const auto [i, expanded] = st.back();
+                st.pop_back();
+                if (done[i]) continue;
+                const Node &x = d.nodes[i];
+                const bool binary = x.op == ADD || x.op == SUB || x.op == MUL;
+                if (!expanded && (binary || x.op == NEG)) {
+                    st.push_back({i, true});
+                    if (binary) st.push_back({x.b, false});
+                    st.push_back({x.a, false});
+                    continue;
+                }
+                done[i] = 1;
+                emit_node(i);
+            }
             const uint64_t ap = A.kl.alpha + 2ull * k;
             if (!A.ext[cn])
                 o << "    f0.mac(v" << cn << ", __ldg(K + " << ap << ")); f1.mac(v" << cn << ", __ldg(K + " << ap + 1
