@@ -482,8 +482,9 @@ SMALL_PCS = PCS
 
 def time_proofs(P, ctx, pcs, wits, steps, warmup, dev, per_proof=None):
     """Device-timed prove_multi on resident witnesses: per-proof ms, stage ms
-    (mean), last output; per_proof, when given, receives each timed proof's
-    stage ms."""
+    (mean), last output; per_proof, when given, receives per timed proof its
+    8 stage ms, the context's cumulative host ms in allocation calls and its
+    pool's reserved GB."""
     import torch
     ref = None
     for _ in range(warmup):
@@ -497,7 +498,9 @@ def time_proofs(P, ctx, pcs, wits, steps, warmup, dev, per_proof=None):
             lat.append(out.device_ms)
             stages += np.array(out.stage_ms)
             if per_proof is not None:
-                per_proof.append([round(float(v), 2) for v in out.stage_ms])
+                m = ctx.memory_stats()
+                per_proof.append([round(float(v), 2) for v in out.stage_ms[:8]] +
+                                 [round(m["alloc_ms"], 2), round(m["reserved_bytes"] / 1e9, 2)])
             launches += out.gpu_launches
             if ref is None:
                 ref = out.digest.copy()
@@ -556,6 +559,8 @@ def run_symbolic(args):
     import sym_airs as S
     ctx = P.Context(dev)
     tuning = apply_tuning(ctx)
+    if args.chunk_nodes:
+        ctx.set_air_chunk_nodes(args.chunk_nodes)
     t0 = time.perf_counter()
     air = P.Air(ctx, P.build_air(S.keccak_eval, S.KC_NCOLS))
     compile_s = time.perf_counter() - t0
@@ -573,7 +578,7 @@ def run_symbolic(args):
                      "digest": [int(x) for x in o.digest[:4]], "clocks": clk}
     assert out["generated"]["digest"] == out["hand-written"]["digest"], "generated and hand-written proofs differ"
     print(json.dumps({"workload": f"{workload_name()}, AIR as symbolic constraints (3182, 40470 DAG nodes)",
-                      "compile_s": compile_s, "tuning": tuning, **out}), flush=True)
+                      "compile_s": compile_s, "kernels": air.num_kernels, "tuning": tuning, **out}), flush=True)
     ctx.close()
     return 0
 
@@ -872,6 +877,8 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="verify: proofs per p3g_verify_batch call")
     ap.add_argument("--max-log-cubic", type=int, default=18)
     ap.add_argument("--max-log-keccak", type=int, default=16)
+    ap.add_argument("--chunk-nodes", type=int, default=0,
+                    help="symbolic: DAG nodes per generated constraint kernel (0: the library default)")
     args = ap.parse_args()
     if args.workload == "batch":
         return run_batch(args)

@@ -94,6 +94,8 @@ void p3g_air_free(p3g_sym_air *air);
 uint32_t p3g_air_log_quotient_degree(const p3g_sym_air *air);
 uint32_t p3g_air_max_degree(const p3g_sym_air *air);
 uint64_t p3g_air_num_constraints_of(const p3g_sym_air *air);
+/* Generated constraint kernels (chunks) of the AIR. */
+uint64_t p3g_air_num_kernels(const p3g_sym_air *air);
 /* ConstraintLayout: base_indices / ext_indices; *n_base and *n_ext are
  * capacities on entry and counts on return. */
 int p3g_air_layout(const p3g_sym_air *air, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext);
@@ -319,6 +321,14 @@ int p3g_autotune_slabs(p3g_ctx *ctx, uint32_t log_height, uint64_t width, uint32
                        uint64_t *best_cols, double *best_ms, double *default_ms);
 int p3g_ctx_set_lde_split(p3g_ctx *ctx, uint32_t log_height, const uint32_t *sizes, uint32_t n);
 int p3g_ctx_set_slab_columns(p3g_ctx *ctx, uint64_t cols);
+/* No counterpart in the reference: the context's memory pool, bytes reserved
+ * from the device and in use, and the host time spent in allocation calls
+ * since creation (growth of the pool maps device memory inside them). */
+/* No counterpart in the reference: DAG nodes per generated constraint kernel
+ * for symbolic AIRs created on this context afterwards (0: default 800;
+ * otherwise at least 16). Results do not depend on it. */
+int p3g_ctx_set_air_chunk_nodes(p3g_ctx *ctx, uint64_t nodes);
+int p3g_ctx_memory_stats(p3g_ctx *ctx, uint64_t *reserved_bytes, uint64_t *used_bytes, double *alloc_ms);
 
 /* ------------------------------------------------------------ verifier */
 /* verify_multi (p3-miden-lifted-stark/src/verifier/mod.rs:170-364) of a

@@ -150,6 +150,7 @@ def lib():
                                              C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "p3g_ctx_set_lde_split": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
             "p3g_ctx_set_slab_columns": (C.c_int, [vp, C.c_uint64]),
+            "p3g_ctx_memory_stats": (C.c_int, [vp, u64p, u64p, C.POINTER(C.c_double)]),
             "p3g_verify": (C.c_int, [vp, C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64, u64p, C.c_uint64,
                                      u64p, C.c_uint64, u64p, C.POINTER(C.c_int32), C.POINTER(VerifyStatsC)]),
             "p3g_verify_batch": (C.c_int, [vp, C.POINTER(VerifyJobC), C.c_uint64, C.c_uint32, C.POINTER(C.c_int32),
@@ -168,6 +169,8 @@ def lib():
             "p3g_air_log_quotient_degree": (C.c_uint32, [vp]),
             "p3g_air_max_degree": (C.c_uint32, [vp]),
             "p3g_air_num_constraints_of": (C.c_uint64, [vp]),
+            "p3g_air_num_kernels": (C.c_uint64, [vp]),
+            "p3g_ctx_set_air_chunk_nodes": (C.c_int, [vp, C.c_uint64]),
             "p3g_air_layout": (C.c_int, [vp, u64p, C.POINTER(C.c_uint64), u64p, C.POINTER(C.c_uint64)]),
             "p3g_air_free": (None, [vp]),
         }
@@ -261,6 +264,18 @@ class Context:
 
     def set_slab_columns(self, cols: int):
         self.check(lib().p3g_ctx_set_slab_columns(self._h, cols))
+
+    def set_air_chunk_nodes(self, nodes: int):
+        """DAG nodes per generated constraint kernel of symbolic AIRs created
+        on this context from now on (0: the default)."""
+        self.check(lib().p3g_ctx_set_air_chunk_nodes(self._h, nodes))
+
+    def memory_stats(self) -> dict:
+        """The context pool's reserved and used bytes, and the host ms spent in
+        allocation calls since the context was created."""
+        r, u, ms = C.c_uint64(), C.c_uint64(), C.c_double()
+        self.check(lib().p3g_ctx_memory_stats(self._h, C.byref(r), C.byref(u), C.byref(ms)))
+        return {"reserved_bytes": r.value, "used_bytes": u.value, "alloc_ms": ms.value}
 
     def load_tuning(self, table: dict):
         """Apply a saved tuning table ({"lde_split": {L: [..]}, "slab_cols": n})."""
@@ -541,6 +556,11 @@ class Air:
     @property
     def max_degree(self) -> int:
         return int(lib().p3g_air_max_degree(self._h))
+
+    @property
+    def num_kernels(self) -> int:
+        """Generated constraint kernels (chunks of the constraint DAG)."""
+        return int(lib().p3g_air_num_kernels(self._h))
 
     def layout(self):
         """ConstraintLayout: (base_indices, ext_indices) in emission order."""

@@ -593,6 +593,7 @@ P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_sym_air *
     try {
         CK(cudaSetDevice(x->c.device));
         sym::analyse(a->a);
+        if (x->c.air_chunk_nodes) a->a.chunk_nodes = x->c.air_chunk_nodes;
         sym::split_chunks(a->a);
         sym::compile(a->a, x->c.device);
     } catch (const p3g::CudaError &e) {
@@ -606,6 +607,7 @@ P3G_API int p3g_air_create(p3g_ctx *x, const p3g_air_desc_c *desc, p3g_sym_air *
 P3G_API uint32_t p3g_air_log_quotient_degree(const p3g_sym_air *a) { return a ? a->a.log_qd : 0; }
 P3G_API uint32_t p3g_air_max_degree(const p3g_sym_air *a) { return a ? a->a.max_degree : 0; }
 P3G_API uint64_t p3g_air_num_constraints_of(const p3g_sym_air *a) { return a ? a->a.d.constraints.size() : 0; }
+P3G_API uint64_t p3g_air_num_kernels(const p3g_sym_air *a) { return a ? a->a.kernels.size() : 0; }
 // ConstraintLayout: base_indices / ext_indices in emission order; *n_base and
 // *n_ext are capacities on entry and counts on return.
 P3G_API int p3g_air_layout(const p3g_sym_air *a, uint64_t *base_idx, uint64_t *n_base, uint64_t *ext_idx, uint64_t *n_ext) {

@@ -172,3 +172,29 @@ P3G_API int p3g_ctx_set_slab_columns(p3g_ctx *x, uint64_t cols) {
     x->c.slab_cols = cols;
     return p3g::OK;
 }
+// DAG nodes per generated constraint kernel for the symbolic AIRs this
+// context creates afterwards (0 restores the default). Fewer nodes: shorter
+// kernels (instruction cache) but more launches re-reading shared cells.
+P3G_API int p3g_ctx_set_air_chunk_nodes(p3g_ctx *x, uint64_t nodes) {
+    if (!x || (nodes && nodes < 16)) return p3g::ERR_INVALID;
+    x->c.air_chunk_nodes = nodes;
+    return p3g::OK;
+}
+
+// Memory statistics of the context's pool: bytes reserved from the device,
+// bytes in use by live buffers, and the host time spent in allocation calls
+// since the context was created (a pool that grows maps new device memory
+// inside those calls).
+P3G_API int p3g_ctx_memory_stats(p3g_ctx *x, uint64_t *reserved_bytes, uint64_t *used_bytes, double *alloc_ms) {
+    if (!x || !reserved_bytes || !used_bytes || !alloc_ms) return p3g::ERR_INVALID;
+    *reserved_bytes = *used_bytes = 0;
+    if (x->c.pool) {
+        uint64_t r = 0, u = 0;  // the attributes are 64-bit values
+        if (cudaMemPoolGetAttribute(x->c.pool, cudaMemPoolAttrReservedMemCurrent, &r) != cudaSuccess ||
+            cudaMemPoolGetAttribute(x->c.pool, cudaMemPoolAttrUsedMemCurrent, &u) != cudaSuccess)
+            return p3g::ERR_CUDA;
+        *reserved_bytes = r, *used_bytes = u;
+    }
+    *alloc_ms = x->c.alloc_ms;
+    return p3g::OK;
+}

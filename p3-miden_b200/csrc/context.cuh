@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <memory>
@@ -92,6 +93,9 @@ struct Ctx {
     // them: every choice computes the same values.
     std::map<uint32_t, std::vector<uint32_t>> lde_split;
     uint64_t slab_cols = 0;
+    // DAG nodes per generated constraint kernel of the symbolic AIRs created
+    // on this context (0: the default, 800)
+    uint64_t air_chunk_nodes = 0;
 
     // This context's own stream-ordered memory pool. Buffers freed by one
     // context are reused only by that context, so two contexts driving the
@@ -148,13 +152,16 @@ struct Ctx {
         pool = nullptr;
     }
 
+    double alloc_ms = 0;  // host time spent in device allocation calls (memory statistics)
     DBuf alloc(size_t words) {
         DBuf b;
         b.s = stream;
         b.words = words;
         if (words) {
+            const auto t0 = std::chrono::steady_clock::now();
             if (pool) CK(cudaMallocFromPoolAsync((void **)&b.p, words * 8, pool, stream));
             else CK(cudaMallocAsync((void **)&b.p, words * 8, stream));
+            alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         return b;
     }

@@ -85,6 +85,7 @@ struct Air {
     std::vector<uint64_t> base_idx, ext_idx;  // ConstraintLayout
     KLayout kl;
     std::vector<std::vector<uint32_t>> chunks;  // constraint indices of each generated kernel
+    size_t chunk_nodes = 800;  // DAG nodes per chunk (a launch-shape choice; every value gives the same sums)
     std::string source, log;
     std::vector<std::vector<char>> cubins;  // one per compiled group of chunks
     std::vector<cudaLibrary_t> libs;
@@ -209,11 +210,10 @@ struct KArgs {
 };
 
 // Constraints are split into chunks of bounded code size (at most
-// kChunkNodes DAG nodes each, shared subexpressions counted once per chunk);
+// A.chunk_nodes DAG nodes each, shared subexpressions counted once per chunk);
 // each chunk is one kernel that adds its part of the fold into acc. The fold
 // is linear, so launching the chunks one after another on the same stream
 // gives the same sum. A small AIR is one chunk.
-constexpr size_t kChunkNodes = 800;
 
 inline void split_chunks(Air &A) {
     const Desc &d = A.d;
@@ -240,7 +240,7 @@ inline void split_chunks(Air &A) {
     };
     for (size_t k = 0; k < d.constraints.size(); k++) {
         collect(d.constraints[k]);
-        if (!A.chunks.back().empty() && in_chunk + walk.size() > kChunkNodes) {
+        if (!A.chunks.back().empty() && in_chunk + walk.size() > A.chunk_nodes) {
             A.chunks.emplace_back();
             cid++;
             in_chunk = 0;
