@@ -818,12 +818,12 @@ def run_serve(args):
     heavy = [sum((i.trace.shape[0] << MIX_PCS["log_blowup"]) * i.trace.shape[1] for i in pool[k].instances) > 1 << 26
              for k in picks]
     out = {}
-    arms = [("plain", 1, False, False), ("served", args.workers, False, False),
-            ("served+heavy-priority", args.workers, False, True)]
+    arms = [("plain", 1, False, 1), ("served", args.workers, False, 1),
+            ("served, 2 heavy at once", args.workers, False, 2)]
     if args.self_check:  # every served proof verified on the device before it is returned
-        arms.append(("served+self-check", args.workers, True, False))
-    for name, workers, check, prio in arms:
-        srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check, heavy_priority=prio)
+        arms.append(("served+self-check", args.workers, True, 1))
+    for name, workers, check, max_heavy in arms:
+        srv = P.ProofServer(dev, n_workers=workers, hbm_budget=args.budget, self_check=check, max_heavy=max_heavy)
         apply_tuning(srv)
         run_pool(P, pool, srv)  # warm-up over every distinct job
         res, span, wall, lat, peak = run_pool(P, stream, srv)

@@ -325,7 +325,7 @@ int p3g_ctx_set_slab_columns(p3g_ctx *ctx, uint64_t cols);
  * from the device and in use, and the host time spent in allocation calls
  * since creation (growth of the pool maps device memory inside them). */
 /* No counterpart in the reference: DAG nodes per generated constraint kernel
- * for symbolic AIRs created on this context afterwards (0: default 800;
+ * for symbolic AIRs created on this context afterwards (0: default 500;
  * otherwise at least 16). Results do not depend on it. */
 int p3g_ctx_set_air_chunk_nodes(p3g_ctx *ctx, uint64_t nodes);
 int p3g_ctx_memory_stats(p3g_ctx *ctx, uint64_t *reserved_bytes, uint64_t *used_bytes, double *alloc_ms);
@@ -415,11 +415,9 @@ int p3g_server_set_self_check(p3g_server *srv, int32_t enabled);
  * before submitting jobs. */
 int p3g_server_set_lde_split(p3g_server *srv, uint32_t log_height, const uint32_t *sizes, uint32_t n);
 int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols);
-/* No counterpart in the reference: heavy-job priority. Worker 0 alone takes
- * heavy jobs (LDEs above 2^26 words), on streams of the device's greatest
- * priority, and the other workers' light jobs fill the SMs it leaves idle.
- * Call while no job is queued or running (P3G_ERR_INVALID otherwise). */
-int p3g_server_set_heavy_priority(p3g_server *srv, int32_t enabled);
+/* No counterpart in the reference: at most n heavy jobs (LDEs above 2^26
+ * words) run at a time; 0 lifts the limit (default 1). */
+int p3g_server_set_max_heavy(p3g_server *srv, uint32_t n);
 /* Waits for every submitted job, then releases the workers. */
 void p3g_server_destroy(p3g_server *srv);
 int p3g_server_submit(p3g_server *srv, const p3g_job *job, uint64_t *ticket);

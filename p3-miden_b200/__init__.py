@@ -940,7 +940,7 @@ class ProofServer:
 
     def __init__(self, device: int = 0, n_workers: int = 4, hbm_budget: int = 150 * 10**9,
                  poseidon2_params: np.ndarray | None = None, self_check: bool = False,
-                 heavy_priority: bool = False):
+                 max_heavy: int = 1):
         L = lib()
         vp = C.c_void_p
         for name, res, args in [
@@ -953,7 +953,7 @@ class ProofServer:
             ("p3g_server_set_self_check", C.c_int, [vp, C.c_int32]),
             ("p3g_server_set_lde_split", C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
             ("p3g_server_set_slab_columns", C.c_int, [vp, C.c_uint64]),
-            ("p3g_server_set_heavy_priority", C.c_int, [vp, C.c_int32]),
+            ("p3g_server_set_max_heavy", C.c_int, [vp, C.c_uint32]),
             ("p3g_job_footprint_bytes", C.c_uint64, [C.POINTER(PcsParamsC), C.POINTER(InstanceC), C.c_uint64]),
         ]:
             fn = getattr(L, name)
@@ -965,8 +965,8 @@ class ProofServer:
         self._pending = {}
         if self_check:
             _check(L.p3g_server_set_self_check(self._h, 1))
-        if heavy_priority:  # heavy jobs on worker 0 at the greatest stream priority
-            _check(L.p3g_server_set_heavy_priority(self._h, 1))
+        if max_heavy != 1:  # heavy jobs (LDEs above 2^26 words) allowed at once; 0: no limit
+            _check(L.p3g_server_set_max_heavy(self._h, max_heavy))
 
     def load_tuning(self, table: dict):
         """Apply a saved tuning table to every worker (Context.load_tuning's format)."""

@@ -114,15 +114,11 @@ P3G_API int p3g_server_set_slab_columns(p3g_server *srv, uint64_t cols) {
     return p3g::OK;
 }
 
-// Heavy jobs on worker 0 at the device's greatest stream priority (see
-// Server::set_heavy_priority); call while the server is idle.
-P3G_API int p3g_server_set_heavy_priority(p3g_server *srv, int32_t enabled) {
+// At most n heavy jobs (LDEs above 2^26 words) at a time; 0 lifts the limit.
+P3G_API int p3g_server_set_max_heavy(p3g_server *srv, uint32_t n) {
     if (!srv) return p3g::ERR_INVALID;
-    try {
-        return srv->s->set_heavy_priority(enabled != 0) ? p3g::OK : p3g::ERR_INVALID;
-    } catch (const p3g::CudaError &e) {
-        return e.status;
-    }
+    srv->s->set_max_heavy(n);
+    return p3g::OK;
 }
 
 P3G_API int p3g_server_submit(p3g_server *srv, const p3g_job_c *job, uint64_t *ticket) {

@@ -94,7 +94,7 @@ struct Ctx {
     std::map<uint32_t, std::vector<uint32_t>> lde_split;
     uint64_t slab_cols = 0;
     // DAG nodes per generated constraint kernel of the symbolic AIRs created
-    // on this context (0: the default, 800)
+    // on this context (0: the default, 500)
     uint64_t air_chunk_nodes = 0;
 
     // This context's own stream-ordered memory pool. Buffers freed by one
@@ -113,25 +113,9 @@ struct Ctx {
         uint64_t thr = UINT64_MAX;
         CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     }
-    int priority = 0;  // of this context's streams (cudaStreamCreateWithPriority; lower runs first)
     void pipeline_streams() {
-        if (!lde_stream) CK(cudaStreamCreateWithPriority(&lde_stream, cudaStreamNonBlocking, priority));
-        if (!copy_stream) CK(cudaStreamCreateWithPriority(&copy_stream, cudaStreamNonBlocking, priority));
-    }
-    // New streams of priority p for an idle context: buffers ordered on the
-    // old streams (the twiddle tables) are freed first and rebuilt on use.
-    void set_priority(int p) {
-        if (stream) CK(cudaStreamSynchronize(stream));
-        if (lde_stream) CK(cudaStreamSynchronize(lde_stream));
-        if (copy_stream) CK(cudaStreamSynchronize(copy_stream));
-        tw.clear();
-        if (stream) CK(cudaStreamSynchronize(stream));
-        if (lde_stream) cudaStreamDestroy(lde_stream);
-        if (copy_stream) cudaStreamDestroy(copy_stream);
-        if (stream) cudaStreamDestroy(stream);
-        lde_stream = copy_stream = stream = nullptr;
-        priority = p;
-        CK(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, priority));
+        if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
+        if (!copy_stream) CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
     }
     // free stream-ordered buffers, then the streams (used at teardown)
     void release() {
@@ -139,6 +123,7 @@ struct Ctx {
         if (lde_stream) cudaStreamSynchronize(lde_stream);
         if (copy_stream) cudaStreamSynchronize(copy_stream);
         tw.clear();
+        ws.release();
         if (stream) cudaStreamSynchronize(stream);
         if (pinned) cudaFreeHost(pinned);
         pinned = nullptr;
@@ -152,6 +137,18 @@ struct Ctx {
         pool = nullptr;
     }
 
+    // Workspace kept between proofs: the column-major copies of the LDE rows
+    // that the generated constraint kernels read. Allocating and freeing a
+    // multi-GB buffer every proof made the pool's allocation calls stall the
+    // host for up to about 0.1 s now and then; kept, it is allocated once.
+    DBuf ws;
+    uint64_t *workspace(size_t words) {
+        if (ws.words < words) {
+            ws.release();
+            ws = alloc(words);
+        }
+        return ws.p;
+    }
     double alloc_ms = 0;  // host time spent in device allocation calls (memory statistics)
     DBuf alloc(size_t words) {
         DBuf b;

@@ -330,17 +330,16 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde,
         ctx.sync();
     }
     const TwTables &twq = ctx.twiddles(log_h + log_qd);
-    // the generated kernels read gJ's rows of the LDEs column-major
-    DBuf main_cm = ctx.alloc(qh * I.width), aux_cm;
-    transpose(ctx, main_lde, I.width, main_cm.p, qh, I.width);
-    if (d.aux_width && aux_lde) {
-        aux_cm = ctx.alloc(qh * 2 * d.aux_width);
-        transpose(ctx, aux_lde, 2 * d.aux_width, aux_cm.p, qh, 2 * d.aux_width);
-    }
+    // the generated kernels read gJ's rows of the LDEs column-major, from the
+    // context's workspace
+    const uint64_t aw2 = (d.aux_width && aux_lde) ? 2 * d.aux_width : 0;
+    uint64_t *main_cm = ctx.workspace(qh * (I.width + aw2)), *aux_cm = aw2 ? main_cm + qh * I.width : nullptr;
+    transpose(ctx, main_lde, I.width, main_cm, qh, I.width);
+    if (aw2) transpose(ctx, aux_lde, aw2, aux_cm, qh, aw2);
     sym::KArgs a{};
-    a.main = main_cm.p;
+    a.main = main_cm;
     a.main_w = I.width;
-    a.aux = aux_cm.p;
+    a.aux = aux_cm;
     a.aux_w2 = 2 * d.aux_width;
     a.per = per_nat.p;
     a.per_h = per_h ? per_h : 1;

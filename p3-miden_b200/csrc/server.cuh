@@ -149,22 +149,10 @@ class Server {
         std::lock_guard<std::mutex> lk(mu_);
         for (auto &c : ctxs_) c->slab_cols = cols;
     }
-    // Heavy-job priority: worker 0 alone takes heavy jobs, on streams of the
-    // device's greatest priority, so that the GPU schedules their kernels
-    // first and the light jobs of the other workers fill the SMs they leave
-    // idle (a heavy proof then runs at nearly its time alone, and a light job
-    // that arrived later no longer slows it down). Worker 0 also takes light
-    // jobs when no heavy job is admissible. Call while no job is queued or
-    // running; returns false otherwise.
-    bool set_heavy_priority(bool on) {
+    // At most n heavy jobs at a time (0: no limit; default 1).
+    void set_max_heavy(uint32_t n) {
         std::lock_guard<std::mutex> lk(mu_);
-        if (pending_ != 0) return false;
-        int least = 0, greatest = 0;
-        CK(cudaSetDevice(device_));
-        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        ctxs_[0]->set_priority(on ? greatest : 0);
-        heavy_priority_ = on && ctxs_.size() > 1;
-        return true;
+        max_heavy_ = n ? n : UINT32_MAX;
     }
 
    private:
@@ -184,8 +172,7 @@ class Server {
                         const uint64_t f = job_footprint_bytes(j->pcs, j->inst.data(), j->inst.size());
                         const bool h = job_is_heavy(j->pcs, j->inst.data(), j->inst.size());
                         const bool fits = in_use_ == 0 || in_use_ + f <= budget_;
-                        if (h && heavy_priority_ && w != 0) continue;  // heavy jobs go to worker 0
-                        if (fits && !(h && heavy_running_)) return it;
+                        if (fits && !(h && heavy_running_ >= max_heavy_)) return it;
                         if (!fits && !h) break;  // keep arrival order among light jobs when memory is short
                     }
                     return queue_.end();
@@ -203,7 +190,7 @@ class Server {
                 queue_.erase(it);
                 fp = job_footprint_bytes(job->pcs, job->inst.data(), job->inst.size());
                 heavy = job_is_heavy(job->pcs, job->inst.data(), job->inst.size());
-                if (heavy) heavy_running_ = true;
+                if (heavy) heavy_running_++;
                 in_use_ += fp;
                 peak_ = std::max(peak_, in_use_);
             }
@@ -234,11 +221,14 @@ class Server {
                 st = ERR_OOM;
                 job->error = "host allocation failed";
             }
+            // the workspace is part of the job's footprint: give it back to the
+            // worker's pool, which keeps memory only within its budget share
+            ctx.ws.release();
             job->end_s = now_s();
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 in_use_ -= fp;
-                if (heavy) heavy_running_ = false;
+                if (heavy) heavy_running_--;
                 job->status = st;
                 pending_--;
             }
@@ -255,7 +245,7 @@ class Server {
     std::condition_variable cv_, done_cv_;
     std::deque<ServerJob *> queue_;
     uint64_t in_use_ = 0, peak_ = 0;
-    bool heavy_running_ = false, heavy_priority_ = false;
+    uint32_t heavy_running_ = 0, max_heavy_ = 1;
     uint64_t pending_ = 0;
     bool stop_ = false;
     std::atomic<bool> self_check_{false};

@@ -85,7 +85,7 @@ struct Air {
     std::vector<uint64_t> base_idx, ext_idx;  // ConstraintLayout
     KLayout kl;
     std::vector<std::vector<uint32_t>> chunks;  // constraint indices of each generated kernel
-    size_t chunk_nodes = 800;  // DAG nodes per chunk (a launch-shape choice; every value gives the same sums)
+    size_t chunk_nodes = 500;  // DAG nodes per chunk (a launch-shape choice; every value gives the same sums)
     std::string source, log;
     std::vector<std::vector<char>> cubins;  // one per compiled group of chunks
     std::vector<cudaLibrary_t> libs;
