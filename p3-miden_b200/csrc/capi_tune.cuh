@@ -129,7 +129,7 @@ P3G_API int p3g_autotune_slabs(p3g_ctx *x, uint32_t log_height, uint64_t width, 
                 p3g::Tree t;
                 p3g::ProofOut po;
                 CK(cudaEventRecord(e0, c.stream));
-                p3g::commit_main_pipelined(c, &I, 1, log_blowup, log_height, lde, mats, t, po, ev_lde);
+                p3g::commit_main_pipelined(c, &I, 1, log_blowup, log_height, lde, mats, t, po, ev_lde, {nullptr});
                 CK(cudaEventRecord(e1, c.stream));
                 CK(cudaEventSynchronize(e1));
                 float ms = 0;

@@ -517,10 +517,15 @@ struct Tree {
 // Leaf sponge of one height class of n leaves: one thread per leaf, or one
 // 16-lane group per leaf when the class is small (latency-bound).
 inline void launch_leaf_class(Ctx &ctx, const merkle::ClassArgs &a, uint64_t n) {
-    if (n <= merkle::kCoopLeaves)
-        merkle::leaf_class_coop_kernel<<<(unsigned)((n * 16 + 127) / 128), 128, 0, ctx.stream>>>(a);
-    else
-        merkle::leaf_class_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx.stream>>>(a);
+    const unsigned coop_blocks = (unsigned)((n * 16 + 127) / 128), blocks = (unsigned)((n + 127) / 128);
+    if (a.cm && a.n_mats != 1) throw CudaError{ERR_INVALID, "column-major copy of a multi-matrix class"};
+    if (n <= merkle::kCoopLeaves) {
+        if (a.cm) merkle::leaf_class_coop_kernel<true><<<coop_blocks, 128, 0, ctx.stream>>>(a);
+        else merkle::leaf_class_coop_kernel<false><<<coop_blocks, 128, 0, ctx.stream>>>(a);
+    } else {
+        if (a.cm) merkle::leaf_class_kernel<true><<<blocks, 128, 0, ctx.stream>>>(a);
+        else merkle::leaf_class_kernel<false><<<blocks, 128, 0, ctx.stream>>>(a);
+    }
     CK(cudaGetLastError());
     ctx.launches++;
 }

@@ -265,19 +265,37 @@ struct ClassArgs {
     uint32_t prev_log_h;
     uint64_t *states_out;   // 12 words per leaf, or null when squeezing
     uint64_t *digests_out;  // 4 words per leaf, or null
+    // optional column-major copy of the absorbed rows (n_mats == 1): word c
+    // of row j < cm_rows is also written to cm[c * cm_ld + j] (the cells the
+    // generated constraint kernels read; a warp's 32 rows make one 256-byte run)
+    uint64_t *cm;
+    uint64_t cm_ld, cm_rows;
 };
 
 // absorb one row (rate 8, overwrite mode, zero-padded last chunk); a single
 // permutation call site
-__device__ __forceinline__ void absorb_row(uint64_t *s, const uint64_t *row, uint64_t w) {
+// permutation call site; with CM, each word is also stored at cmj[c * cm_ld]
+// (cmj = cm + row index, or null for rows past cm_rows)
+template <bool CM>
+__device__ __forceinline__ void absorb_row(uint64_t *s, const uint64_t *row, uint64_t w, uint64_t *cmj,
+                                           uint64_t cm_ld) {
 #pragma unroll 1
     for (uint64_t i = 0; i < w; i += 8) {
         if (i + 8 <= w) {
 #pragma unroll
             for (int j = 0; j < 8; j++) s[j] = __ldg(row + i + j);
+            if (CM && cmj) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) cmj[(i + j) * cm_ld] = s[j];
+            }
         } else {
 #pragma unroll
             for (int j = 0; j < 8; j++) s[j] = i + j < w ? __ldg(row + i + j) : 0;
+            if (CM && cmj) {
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (i + j < w) cmj[(i + j) * cm_ld] = s[j];
+            }
         }
         p2_permute_dev(s);
     }
@@ -285,6 +303,7 @@ __device__ __forceinline__ void absorb_row(uint64_t *s, const uint64_t *row, uin
 
 // At most 64 registers: eight 128-thread blocks per SM (measured: 66
 // registers, seven blocks, made the slab's tree 9 % slower).
+template <bool CM>
 __global__ void __launch_bounds__(128, 8) leaf_class_kernel(const __grid_constant__ ClassArgs a) {
     uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >> a.log_h) return;
@@ -297,7 +316,8 @@ __global__ void __launch_bounds__(128, 8) leaf_class_kernel(const __grid_constan
 #pragma unroll
         for (int i = 0; i < 12; i++) s[i] = 0;
     }
-    for (int m = 0; m < a.n_mats; m++) absorb_row(s, a.data[m] + j * a.ld[m], a.width[m]);
+    for (int m = 0; m < a.n_mats; m++)
+        absorb_row<CM>(s, a.data[m] + j * a.ld[m], a.width[m], CM && j < a.cm_rows ? a.cm + j : nullptr, a.cm_ld);
     if (a.digests_out) {
 #pragma unroll
         for (int i = 0; i < 4; i++) a.digests_out[j * 4 + i] = p2w::canon(s[i]);
@@ -313,6 +333,7 @@ __global__ void __launch_bounds__(128, 8) leaf_class_kernel(const __grid_constan
 // States are weakly reduced like leaf_class_kernel's (congruent mod p, not
 // always the same words), so classes may mix the two kernels.
 constexpr uint64_t kCoopLeaves = 4096;
+template <bool CM>
 __global__ void __launch_bounds__(128) leaf_class_coop_kernel(const __grid_constant__ ClassArgs a) {
     __shared__ uint64_t sc[p2::N_PARAMS];
     p2x::stage_consts(sc);
@@ -330,6 +351,7 @@ __global__ void __launch_bounds__(128) leaf_class_coop_kernel(const __grid_const
 #pragma unroll 1
         for (uint64_t i = 0; i < w; i += 8) {
             if (l < 8) x = ok && i + l < w ? __ldg(row + i + l) : 0;
+            if (CM && l < 8 && ok && i + l < w && j < a.cm_rows) a.cm[(i + l) * a.cm_ld + j] = x;
             x = p2x::permute(x, l, sc, k);
         }
     }

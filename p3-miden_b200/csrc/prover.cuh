@@ -162,9 +162,12 @@ inline const uint64_t *trace_on_device(Ctx &ctx, const Instance &in, DBuf &hold,
 // The LDE (HBM-bound) of slab s+1 and the copy of slab s+2 run under the
 // hash (integer-bound) of slab s. `ev_lde_done` is recorded on the context
 // stream once every LDE slab is written (stage timing).
+// cm[i], when not null, receives a column-major copy of the first
+// h_i << log_qd_i LDE rows of trace i (written by the leaf kernels as they
+// absorb the rows; the generated constraint kernels read it).
 inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst, uint32_t lb, uint32_t log_max_h,
                                   std::vector<DBuf> &main_lde, std::vector<Mat> &main_mats, Tree &t, ProofOut &po,
-                                  cudaEvent_t ev_lde_done) {
+                                  cudaEvent_t ev_lde_done, const std::vector<uint64_t *> &cm) {
     ctx.pipeline_streams();
     const uint64_t H = inst[n_inst - 1].height << lb;
     t.alignment = 8;
@@ -259,6 +262,12 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
         a.log_h = log2u(h << lb);
         a.prev = prev;
         a.prev_log_h = prev_log;
+        if (cm[sl.trace]) {
+            const uint64_t qh = h << inst_log_qd(I);
+            a.cm = cm[sl.trace] + sl.c0 * qh;
+            a.cm_ld = qh;
+            a.cm_rows = qh;
+        }
         const bool last = s + 1 == slabs.size();
         uint64_t *out_states = st[s & 1].p;
         a.states_out = last ? nullptr : out_states;
@@ -294,10 +303,11 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
 // Constraint evaluation of a symbolic AIR on gJ with its generated kernel
 // (symair.cuh): one thread per point, acc[m] += sum_k alpha^{K-1-k} C_k(x_m).
 // The kernels read column-major copies of gJ's rows of the main and aux LDEs
-// (one transpose each), so that every cell load of a warp is one 256-byte run.
+// (cm: the main part from the main commit's leaf kernels, the aux part from one
+// transpose), so that every cell load of a warp is one 256-byte run.
 // Periodic columns: PeriodicLde::build on the quotient coset (blowup D,
 // shift (g^{2^lift})^{h / max_period}, natural order; periodic.rs:49-98).
-inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde, const uint64_t *aux_lde,
+inline void eval_symbolic(Ctx &ctx, const Instance &I, uint64_t *cm, const uint64_t *aux_lde,
                           uint32_t log_h, uint32_t log_qd, uint32_t log_max_h, const std::vector<uint64_t> &rnd,
                           const std::vector<uint64_t> &auxv, const std::vector<uint64_t> &alpha_pows, uint64_t *acc) {
     const sym::Air &A = *I.sym;
@@ -330,11 +340,11 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, const uint64_t *main_lde,
         ctx.sync();
     }
     const TwTables &twq = ctx.twiddles(log_h + log_qd);
-    // the generated kernels read gJ's rows of the LDEs column-major, from the
-    // context's workspace
+    // the generated kernels read gJ's rows of the LDEs column-major: the main
+    // part of cm was written by the main commit's leaf kernels; the aux part
+    // is copied here
     const uint64_t aw2 = (d.aux_width && aux_lde) ? 2 * d.aux_width : 0;
-    uint64_t *main_cm = ctx.workspace(qh * (I.width + aw2)), *aux_cm = aw2 ? main_cm + qh * I.width : nullptr;
-    transpose(ctx, main_lde, I.width, main_cm, qh, I.width);
+    uint64_t *main_cm = cm, *aux_cm = aw2 ? cm + qh * I.width : nullptr;
     if (aw2) transpose(ctx, aux_lde, aw2, aux_cm, qh, aw2);
     sym::KArgs a{};
     a.main = main_cm;
@@ -546,7 +556,25 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
     std::vector<Mat> main_mats, aux_mats;
     const uint64_t launches_before = ctx.launches;
     Tree main_tree;
-    commit_main_pipelined(ctx, inst, n_inst, lb, log_max_h, main_lde, main_mats, main_tree, po, ev[1]);
+    // column-major copies of the quotient-domain rows for the generated
+    // constraint kernels of symbolic AIRs (main part written during the main
+    // commit, aux part before the constraints), in the context's workspace
+    std::vector<uint64_t *> sym_cm(n_inst, nullptr);
+    {
+        std::vector<uint64_t> off(n_inst, 0);
+        uint64_t words = 0;
+        for (size_t i = 0; i < n_inst; i++)
+            if (inst[i].air == AIR_SYMBOLIC) {
+                off[i] = words;
+                words += (inst[i].height << inst_log_qd(inst[i])) * (inst[i].width + 2 * inst_aux_width(inst[i]));
+            }
+        if (words) {
+            uint64_t *ws = ctx.workspace(words);
+            for (size_t i = 0; i < n_inst; i++)
+                if (inst[i].air == AIR_SYMBOLIC) sym_cm[i] = ws + off[i];
+        }
+    }
+    commit_main_pipelined(ctx, inst, n_inst, lb, log_max_h, main_lde, main_mats, main_tree, po, ev[1], sym_cm);
     tr.send_commit(main_tree.root);
     CK(cudaEventRecord(ev[2], ctx.stream));
 
@@ -635,7 +663,7 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
             p = gl::ef_mul(p, alpha);
         }
         if (I.air == AIR_SYMBOLIC) {
-            eval_symbolic(ctx, I, main_lde[ii].p, aux_lde[ii].p, log_h, log_qd, log_max_h, rnd, aux_vals[ii], ap,
+            eval_symbolic(ctx, I, sym_cm[ii], aux_lde[ii].p, log_h, log_qd, log_max_h, rnd, aux_vals[ii], ap,
                           acc.p);
             L.n++;
             continue;

@@ -34,7 +34,7 @@ inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, 
     for (size_t i = 0; i < n; i++) {
         const uint64_t hw = inst[i].height * inst[i].width, aw2 = 2 * inst_aux_width(inst[i]);
         if (inst[i].air == AIR_SYMBOLIC)  // column-major copies of gJ's rows for the generated kernels
-            max_cm = std::max(max_cm, (inst[i].height << inst_log_qd(inst[i])) * (inst[i].width + aw2));
+            max_cm += (inst[i].height << inst_log_qd(inst[i])) * (inst[i].width + aw2);
         if (!inst[i].trace_on_device) words += hw;  // uploaded trace
         words += hw * B;                             // main LDE
         words += inst[i].height * aw2 * (B + 1);     // aux trace + LDE

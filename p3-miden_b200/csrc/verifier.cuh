@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(128) leaf_thread_kernel(const LeafJob *jobs, u
     for (int i = 0; i < 12; i++) s[i] = 0;
     for (uint32_t m = 0; m < job.n_w; m++) {
         const uint32_t w = widths[job.w_off + m];
-        merkle::absorb_row(s, row, w);
+        merkle::absorb_row<false>(s, row, w, nullptr, 0);
         row += w;
     }
 #pragma unroll
