@@ -818,8 +818,7 @@ def run_serve(args):
     heavy = [sum((i.trace.shape[0] << MIX_PCS["log_blowup"]) * i.trace.shape[1] for i in pool[k].instances) > 1 << 26
              for k in picks]
     out = {}
-    arms = [("plain", 1, False, 1), ("served", args.workers, False, 1),
-            ("served, 2 heavy at once", args.workers, False, 2)]
+    arms = [("plain", 1, False, 1), ("served", args.workers, False, 1)]
     if args.self_check:  # every served proof verified on the device before it is returned
         arms.append(("served+self-check", args.workers, True, 1))
     for name, workers, check, max_heavy in arms:

@@ -37,6 +37,7 @@ P3G_API int p3g_ctx_create(int device, const uint64_t *poseidon2_params130, p3g_
         memcpy(x->c.p2, poseidon2_params130, sizeof(x->c.p2));
         p3g::bind_p2(x->c);
         x->c.make_pool();
+        x->c.enable_cache(8ull << 30);  // up to 64 GB of large buffers kept between proofs
     } catch (const p3g::CudaError &e) {
         delete x;
         return e.status;

@@ -50,24 +50,61 @@ inline unsigned log2u(uint64_t n) {
     return l;
 }
 
+// Buffer cache of a context. Repeated proofs of one shape allocate the same
+// large buffers every time; from the pool, such allocations now and then
+// stalled the host for 10-100 ms (the pool's reserved memory did not grow).
+// Buffers of at least kMinWords allocated and released on the context's own
+// stream are kept, up to limit_words, and handed out again for an allocation
+// of exactly the same size on that stream: stream order makes that reuse as
+// safe as the pool's own same-stream reuse. Buffers released after the
+// context is gone (alive false) are freed as before.
+struct BufCache {
+    static constexpr size_t kMinWords = 1ull << 20;  // 8 MB
+    bool alive = true;
+    cudaStream_t home = nullptr;
+    size_t limit_words = 0, cached_words = 0;
+    std::multimap<size_t, uint64_t *> free;
+    bool put(uint64_t *p, size_t words, cudaStream_t s) {
+        if (!alive || s != home || words < kMinWords || cached_words + words > limit_words) return false;
+        free.insert({words, p});
+        cached_words += words;
+        return true;
+    }
+    uint64_t *take(size_t words) {
+        auto it = free.find(words);
+        if (it == free.end()) return nullptr;
+        uint64_t *p = it->second;
+        free.erase(it);
+        cached_words -= words;
+        return p;
+    }
+    void clear() {
+        for (auto &e : free) cudaFreeAsync(e.second, home);
+        free.clear();
+        cached_words = 0;
+    }
+};
+
 // A device buffer owned by a context, freed stream-ordered.
 struct DBuf {
     uint64_t *p = nullptr;
     size_t words = 0;
     cudaStream_t s = nullptr;
+    std::shared_ptr<BufCache> cache;  // where the buffer goes back to, or null
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
-    DBuf(DBuf &&o) noexcept : p(o.p), words(o.words), s(o.s) { o.p = nullptr; }
+    DBuf(DBuf &&o) noexcept : p(o.p), words(o.words), s(o.s), cache(std::move(o.cache)) { o.p = nullptr; }
     DBuf &operator=(DBuf &&o) noexcept {
         release();
-        p = o.p, words = o.words, s = o.s;
+        p = o.p, words = o.words, s = o.s, cache = std::move(o.cache);
         o.p = nullptr;
         return *this;
     }
     void release() {
-        if (p) cudaFreeAsync(p, s);
+        if (p && !(cache && cache->put(p, words, s))) cudaFreeAsync(p, s);
         p = nullptr;
+        cache.reset();
     }
     ~DBuf() { release(); }
 };
@@ -117,6 +154,15 @@ struct Ctx {
         if (!lde_stream) CK(cudaStreamCreateWithFlags(&lde_stream, cudaStreamNonBlocking));
         if (!copy_stream) CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
     }
+    // Buffer cache (BufCache) on the context's own stream; off until
+    // enable_cache is called.
+    std::shared_ptr<BufCache> bc;
+    void enable_cache(size_t limit_words) {
+        bc = std::make_shared<BufCache>();
+        bc->home = stream;
+        bc->limit_words = limit_words;
+    }
+
     // free stream-ordered buffers, then the streams (used at teardown)
     void release() {
         if (stream) cudaStreamSynchronize(stream);
@@ -124,6 +170,11 @@ struct Ctx {
         if (copy_stream) cudaStreamSynchronize(copy_stream);
         tw.clear();
         ws.release();
+        if (bc) {
+            bc->clear();
+            bc->alive = false;
+            bc.reset();
+        }
         if (stream) cudaStreamSynchronize(stream);
         if (pinned) cudaFreeHost(pinned);
         pinned = nullptr;
@@ -154,6 +205,10 @@ struct Ctx {
         DBuf b;
         b.s = stream;
         b.words = words;
+        if (bc && stream == bc->home) {
+            b.cache = bc;
+            if (words >= BufCache::kMinWords && (b.p = bc->take(words))) return b;
+        }
         if (words) {
             const auto t0 = std::chrono::steady_clock::now();
             if (pool) CK(cudaMallocFromPoolAsync((void **)&b.p, words * 8, pool, stream));
