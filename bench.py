@@ -339,6 +339,16 @@ def run_gpu(args):
     ctx = P.Context(dev)
     tuning = apply_tuning(ctx)
     pcs = P.PcsParams(**PCS)
+    # the Keccak AIR: by default given as its symbolic constraints, whose
+    # constraint kernels the library generates and compiles once, here, before
+    # any proof (the built-in AIR's hand-written kernel gives the same proof)
+    air, air_setup = P.AIR_KECCAK, {"constraints": "hand-written kernel (built-in AIR)"}
+    if args.constraints == "generated":
+        import p3_miden_b200.airs as airs
+        t0 = time.perf_counter()
+        air = P.Air(ctx, P.build_air(airs.keccak_eval, airs.KC_NCOLS))
+        air_setup = {"constraints": "generated from the AIR's symbolic constraints (p3_miden_b200.airs)",
+                     "kernels": air.num_kernels, "compile_s": time.perf_counter() - t0}
 
     # trace: seeded inputs (one distinct seed per rank), host-generated
     inputs = P.keccak_inputs(1 + rank, N_PERMS)
@@ -346,13 +356,18 @@ def run_gpu(args):
     P.generate_keccak_trace(inputs, out=host.numpy().view(np.uint64))
     dev_trace = host.to(f"cuda:{dev}", non_blocking=False)
     torch.cuda.synchronize(dev)
-    wit_dev = [P.AirWitness(P.AIR_KECCAK, dev_trace)]
-    wit_host = [P.AirWitness(P.AIR_KECCAK, host)]
+    wit_dev = [P.AirWitness(air, dev_trace)]
+    wit_host = [P.AirWitness(air, host)]
 
     # ---- device-resident arm (value): trace already in HBM
     for _ in range(args.warmup):
         out = P.prove_multi(ctx, pcs, wit_dev)
     ref_digest = out.digest.copy()
+    if air is not P.AIR_KECCAK:  # one untimed proof through the hand-written kernel: the same proof
+        hw = P.prove_multi(ctx, pcs, [P.AirWitness(P.AIR_KECCAK, dev_trace)])
+        assert np.array_equal(hw.digest, ref_digest), "generated and hand-written constraint kernels differ"
+        air_setup["same_proof_as_hand_written"] = True
+        del hw
     barrier(pg, dev)
     torch.cuda.synchronize(dev)
     lat, launches, stages, lde_k, leaf_k = [], 0, np.zeros(len(P.STAGES)), [], []
@@ -397,7 +412,7 @@ def run_gpu(args):
     def from_inputs():
         inputs_dev.copy_(inputs_pinned, non_blocking=True)
         P.generate_keccak_trace_device(ctx, inputs_dev, LOG_H, out=trace_dev)
-        return P.prove_multi(ctx, pcs, [P.AirWitness(P.AIR_KECCAK, trace_dev)])
+        return P.prove_multi(ctx, pcs, [P.AirWitness(air, trace_dev)])
 
     for _ in range(max(1, args.warmup // 2)):
         from_inputs()
@@ -437,7 +452,7 @@ def run_gpu(args):
         "data": "synthetic (seeded Keccak-f inputs)",
         "config": base_config(),
         "arm": {"parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (5.5 GB trace, 11 GB LDE)",
-                "timing": "CUDA events on the prover stream", "tuning": tuning},
+                "timing": "CUDA events on the prover stream", "tuning": tuning, "air": air_setup},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "wall_per_step": wall / args.steps * 1e3},
         "stage_ms": {n: float(v) for n, v in zip(P.STAGES, stages_ms)},
@@ -547,7 +562,7 @@ def run_named(args):
 
 def run_symbolic(args):
     """The headline proof (Keccak AIR, 10922 permutations, 2^18 x 2633) with
-    the AIR given as symbolic constraints (tests/sym_airs.py's AirBuilder
+    the AIR given as symbolic constraints (p3_miden_b200.airs, the AirBuilder
     form) and its constraint kernels generated and compiled by the library,
     next to the hand-written Keccak kernel on the same trace: per-stage
     device time of both, and the generated kernels' compile time."""
@@ -555,8 +570,7 @@ def run_symbolic(args):
     dev = 0
     torch.cuda.set_device(dev)
     P = load_product()
-    sys.path.insert(0, str(ROOT / "tests"))
-    import sym_airs as S
+    import p3_miden_b200.airs as S
     ctx = P.Context(dev)
     tuning = apply_tuning(ctx)
     if args.chunk_nodes:
@@ -876,6 +890,9 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="verify: proofs per p3g_verify_batch call")
     ap.add_argument("--max-log-cubic", type=int, default=18)
     ap.add_argument("--max-log-keccak", type=int, default=16)
+    ap.add_argument("--constraints", default="generated", choices=["generated", "hand-written"],
+                    help="keccak: the AIR as symbolic constraints with generated kernels (default) or the built-in "
+                         "AIR's hand-written kernel (the same proof)")
     ap.add_argument("--chunk-nodes", type=int, default=0,
                     help="symbolic: DAG nodes per generated constraint kernel (0: the library default)")
     args = ap.parse_args()
