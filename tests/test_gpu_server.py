@@ -118,3 +118,30 @@ def test_self_check(product, gpu_ctx):
     finally:
         srv.close()
     assert all(r.verdict == -1 for r in plain)
+
+
+def test_heavy_and_symbolic_jobs(product, gpu_ctx):
+    """Heavy jobs (LDEs above 2^26 words: Keccak 2^12 rows at blowup 8), with
+    two allowed at once, beside light built-in and symbolic jobs (the
+    symbolic ones use the worker's workspace for their column-major rows):
+    every proof equals the same job proven alone."""
+    import sym_airs as S
+    jobs = []
+    pcs_h = product.PcsParams(3, 1, 0, 8, 0, 20, 0)
+    for i in range(2):
+        t = product.generate_keccak_trace(product.keccak_inputs(300 + i, 170))
+        jobs.append(product.Job(pcs_h, [product.AirWitness(product.AIR_KECCAK, t)]))
+    for i in range(3):
+        k, t = product.generate_cubic_trace(8 + i, 16, 400 + i)
+        air = product.Air(gpu_ctx, product.build_air(S.cubic_eval(k), 16))
+        jobs.append(product.Job(product.PcsParams(2, 1, 0, 8, 0, 20, 0), [product.AirWitness(air, t)]))
+    alone = [product.prove_multi(gpu_ctx, j.pcs, j.instances) for j in jobs]
+    srv = product.ProofServer(0, n_workers=3, max_heavy=2)
+    try:
+        res = srv.run(jobs)
+    finally:
+        srv.close()
+    for a, r in zip(alone, res):
+        assert r.status == product.OK
+        assert np.array_equal(a.proof.fields, r.output.proof.fields)
+        assert np.array_equal(a.digest, r.output.digest)

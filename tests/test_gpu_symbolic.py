@@ -160,3 +160,33 @@ def test_symbolic_keccak_2e13_matches_oracle(product, gpu_ctx):
     dev = torch.from_numpy(t.view(np.int64)).to("cuda:0")
     again = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(air, dev)])
     assert np.array_equal(again.digest, sym.digest)
+
+
+def test_chunk_size_does_not_change_the_proof(product):
+    """The chunk size of the generated kernels is a launch-shape choice: the
+    cubic AIR (w = 24) cut into 16-node chunks (many kernels, each adding its
+    part of the fold) gives the built-in kernel's proof. The context's memory
+    statistics stay consistent across repeated proofs (large buffers come
+    back from the context's cache)."""
+    ctx = product.Context(0)
+    try:
+        ctx.set_air_chunk_nodes(16)
+        k, t = O.cubic_trace(12, 24, 77)
+        air = product.Air(ctx, product.build_air(S.cubic_eval(k), 24))
+        assert air.num_kernels > 4
+        pcs = product.PcsParams(1, 1, 0, 8, 0, 30, 0)
+        sym = product.prove_multi(ctx, pcs, [product.AirWitness(air, t)])
+        builtin = product.prove_multi(ctx, pcs, [product.AirWitness(product.AIR_CUBIC, t, k)])
+        assert np.array_equal(sym.proof.fields, builtin.proof.fields)
+        assert np.array_equal(sym.digest, builtin.digest)
+        m0 = ctx.memory_stats()
+        again = [product.prove_multi(ctx, pcs, [product.AirWitness(air, t)]) for _ in range(3)]
+        m1 = ctx.memory_stats()
+        assert all(np.array_equal(a.digest, sym.digest) for a in again)
+        assert m1["reserved_bytes"] >= m1["used_bytes"] > 0
+        assert m1["reserved_bytes"] == m0["reserved_bytes"]  # repeated proofs do not grow the pool
+        assert m1["alloc_ms"] >= m0["alloc_ms"] >= 0
+        with pytest.raises(product.P3gError):
+            ctx.set_air_chunk_nodes(3)
+    finally:
+        ctx.close()
