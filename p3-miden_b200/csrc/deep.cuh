@@ -85,7 +85,19 @@ __global__ void __launch_bounds__(256) colsum_kernel(const uint64_t *M, uint64_t
     const uint64_t r1 = min(d, r0 + rows_per_chunk);
     gl::Acc acc[4];
     if (col < w) {
-        for (uint64_t i = r0 + rl; i < r1; i += 8) {
+        // four rows per step: their loads are issued together, so that each
+        // thread keeps several DRAM reads in flight
+        uint64_t i = r0 + rl;
+        for (; i + 24 < r1; i += 32) {
+            uint64_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) v[u] = __ldg(M + (i + 8 * u) * w + col);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) acc[k].mac(v[u], __ldg(W + 4 * (i + 8 * u) + k));
+        }
+        for (; i < r1; i += 8) {
             uint64_t v = __ldg(M + i * w + col);
 #pragma unroll
             for (int k = 0; k < 4; k++) acc[k].mac(v, __ldg(W + 4 * i + k));
@@ -131,7 +143,18 @@ __global__ void __launch_bounds__(256) rowdot_warp_kernel(const uint64_t *M, uin
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < h; i += warps) {
         const uint64_t *row = M + i * w;
         gl::Acc a0, a1;
-        for (uint64_t col = lane; col < w; col += 32) {
+        uint64_t col = lane;
+        for (; col + 96 < w; col += 128) {  // four loads in flight per lane
+            uint64_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) v[u] = __ldg(row + col + 32 * u);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                a0.mac(v[u], sc[2 * (col + 32 * u)]);
+                a1.mac(v[u], sc[2 * (col + 32 * u) + 1]);
+            }
+        }
+        for (; col < w; col += 32) {
             uint64_t v = __ldg(row + col);
             a0.mac(v, sc[2 * col]);
             a1.mac(v, sc[2 * col + 1]);

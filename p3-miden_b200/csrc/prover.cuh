@@ -435,8 +435,16 @@ inline std::vector<uint64_t> deep_evals(Ctx &ctx, Launcher &L, const std::vector
         for (const Mat *m : all) {
             uint64_t dm = m->h >> lb;
             uint64_t col_tiles = (m->w + 31) / 32;
-            uint64_t target_blocks = 4 * 148;
-            uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, (target_blocks + col_tiles - 1) / col_tiles));
+            // one wave of resident blocks: as many row chunks as fit beside the
+            // column tiles (a second, partial wave would double the time)
+            static int bps = 0, sms = 0;
+            if (!bps) {
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, deep::colsum_kernel, 256, 0));
+                CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+                bps = std::max(1, bps);
+            }
+            const uint64_t target_blocks = (uint64_t)sms * bps;
+            uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, target_blocks / col_tiles));
             uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
             n_chunks = (dm + rpc - 1) / rpc;
             DBuf part = ctx.alloc(n_chunks * m->w * 4);
