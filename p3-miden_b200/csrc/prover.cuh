@@ -182,13 +182,29 @@ inline void commit_main_pipelined(Ctx &ctx, const Instance *inst, size_t n_inst,
     uint64_t max_slab_hw = 0, max_state_h = 0;
     for (size_t i = 0; i < n_inst; i++) {
         uint64_t w = inst[i].width, h = inst[i].height;
-        uint64_t sw = w >= 256 ? ((w + 7) / 8 + 7) / 8 * 8 : w;  // about 8 slabs for wide traces
-        // tuned width (a multiple of the rate, 8) for device-resident traces; a
-        // host trace keeps about 8 slabs so that its upload hides under the hash
-        if (ctx.slab_cols && inst[i].trace_on_device) sw = std::min<uint64_t>(w, ctx.slab_cols);
-        for (uint64_t c0 = 0; c0 < w; c0 += sw) {
-            slabs.push_back({i, c0, std::min(sw, w - c0)});
-            max_slab_hw = std::max(max_slab_hw, h * std::min(sw, w - c0));
+        if (!inst[i].trace_on_device && w >= 256) {
+            // a wide host trace: slabs that grow geometrically (x1.5, multiples of
+            // the rate 8) from about 1/64 of the width, so that only the small
+            // first slab's upload is exposed and each later upload (PCIe) fits
+            // under the LDE and hash of the slab before it (about 1.6x the
+            // upload time per column on a B200 at blowup 2, more at larger
+            // blowups)
+            uint64_t cur = std::max<uint64_t>(8, (w / 64 + 7) / 8 * 8);
+            for (uint64_t c0 = 0; c0 < w;) {
+                const uint64_t take = std::min(cur, w - c0);
+                slabs.push_back({i, c0, take});
+                max_slab_hw = std::max(max_slab_hw, h * take);
+                c0 += take;
+                cur = (cur * 3 / 2 + 7) / 8 * 8;
+            }
+        } else {
+            uint64_t sw = w >= 256 ? ((w + 7) / 8 + 7) / 8 * 8 : w;  // about 8 slabs for wide traces
+            // tuned width (a multiple of the rate, 8) for device-resident traces
+            if (ctx.slab_cols) sw = std::min<uint64_t>(w, ctx.slab_cols);
+            for (uint64_t c0 = 0; c0 < w; c0 += sw) {
+                slabs.push_back({i, c0, std::min(sw, w - c0)});
+                max_slab_hw = std::max(max_slab_hw, h * std::min(sw, w - c0));
+            }
         }
         main_lde[i] = ctx.alloc((h << lb) * w);
         main_mats.push_back({main_lde[i].p, h << lb, w});
