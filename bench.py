@@ -765,10 +765,11 @@ def run_batch(args):
     srv_pool = P.ProofServer(dev, n_workers=args.workers, hbm_budget=args.budget)
     apply_tuning(srv_plain)
     tuning = apply_tuning(srv_pool)
-    # warm-up over the whole list on both servers, so that neither arm pays
-    # for growing its memory pools or for first-use tables in the timed passes
-    run_pool(P, jobs, srv_plain)
-    run_pool(P, jobs, srv_pool)
+    # warm-up over the whole list on both servers (twice), so that neither arm
+    # pays for growing its memory pools or for first-use tables in the timed passes
+    for _ in range(2):  # one pass left the plain arm's first timed pass slower on some boxes
+        run_pool(P, jobs, srv_plain)
+        run_pool(P, jobs, srv_pool)
     # alternate the two arms and keep the median pass of each: single passes
     # of the same list vary by several percent
     p_runs, b_runs, diag = [], [], []
