@@ -276,6 +276,10 @@ struct KArgs {
 };
 )K";
     const size_t n = d.nodes.size();
+    auto as_ef = [&](uint32_t j) {
+        std::string v = "v" + std::to_string(j);
+        return A.ext[j] ? v : "gl::ef{" + v + ", 0}";
+    };
     std::vector<uint8_t> live(n);
     for (size_t c = c0; c < c1; c++) {
         const std::vector<uint32_t> &ks = A.chunks[c];
@@ -323,110 +327,47 @@ struct KArgs {
         // constraints into an extension sum.
         std::vector<uint8_t> done(n, 0);
         std::vector<std::pair<uint32_t, bool>> st;
-        // Base values are kept lazily: a sum, difference or negation is a Wide
-        // (96-bit, "w<i>", below 2^bits[i]) that is never reduced on its own; a
-        // product or a load is below 2^64 ("v<i>", canonical for loads,
-        // constants and selectors). A product, the fold and the extension
-        // arithmetic take reduced copies, emitted once where first needed:
-        // "u<i>" (below 2^64) and "c<i>" (canonical).
-        std::vector<uint8_t> wide(n, 0), bits(n, 64), canon(n, 0), has_u(n, 0), has_c(n, 0);
-        auto u_of = [&](uint32_t j) -> std::string {
-            if (!wide[j]) return "v" + std::to_string(j);
-            if (!has_u[j]) {
-                o << "    const uint64_t u" << j << " = gl::wide_reduce(w" << j << ");\n";
-                has_u[j] = 1;
-            }
-            return "u" + std::to_string(j);
-        };
-        auto c_of = [&](uint32_t j) -> std::string {
-            if (!wide[j] && canon[j]) return "v" + std::to_string(j);
-            if (!has_c[j]) {
-                const std::string u = u_of(j);
-                o << "    const uint64_t c" << j << " = gl::canon_dev(" << u << ");\n";
-                has_c[j] = 1;
-            }
-            return "c" + std::to_string(j);
-        };
-        // operand j of a sum as a Wide below 2^b (b set here); with `narrow`
-        // a wide operand is reduced first (keeps the result below 2^96)
-        auto w_of = [&](uint32_t j, bool narrow, unsigned &b) -> std::string {
-            if (wide[j] && !narrow) {
-                b = bits[j];
-                return "w" + std::to_string(j);
-            }
-            b = 64;
-            return "gl::Wide{" + u_of(j) + ", 0}";
-        };
-        // a multiple of p at or above 2^b (64 <= b <= 95), as "lo, hi"
-        auto p_multiple = [](unsigned b) {
-            const unsigned t = b - 63;  // p * 2^t > 2^(63 + t)
-            const unsigned __int128 c = (unsigned __int128)gl::P << t;
-            return std::to_string((uint64_t)c) + "ull, " + std::to_string((uint32_t)(c >> 64)) + "u";
-        };
-        auto as_ef = [&](uint32_t j) { return A.ext[j] ? "v" + std::to_string(j) : "gl::ef{" + c_of(j) + ", 0}"; };
         auto emit_node = [&](size_t i) {
             const Node &x = d.nodes[i];
             const std::string v = "v" + std::to_string(i);
-            std::string rhs;
-            const bool base_arith = !A.ext[i] && (x.op == ADD || x.op == SUB || x.op == NEG);
-            if (base_arith) {
-                for (int narrow = 0; narrow < 2; narrow++) {  // reduce the operands if the bound would pass 2^95
-                    unsigned ba = 64, bb = 64, nb;
-                    std::string ea, eb;
-                    ea = w_of(x.a, narrow, ba);
-                    if (x.op != NEG) eb = w_of(x.b, narrow, bb);
-                    if (x.op == ADD) nb = std::max(ba, bb) + 1;
-                    else if (x.op == SUB) nb = std::max(ba, bb + 1) + 1;
-                    else nb = ba + 1;
-                    if (nb > 95 && !narrow) continue;
-                    if (x.op == ADD) rhs = "gl::wide_add(" + ea + ", " + eb + ")";
-                    else if (x.op == SUB) rhs = "gl::wide_sub(" + ea + ", " + eb + ", " + p_multiple(bb) + ")";
-                    else rhs = "gl::wide_neg(" + ea + ", " + p_multiple(ba) + ")";
-                    wide[i] = 1;
-                    bits[i] = (uint8_t)nb;
-                    break;
-                }
-                o << "    const gl::Wide w" << i << " = " << rhs << ";\n";
-                return;
-            }
+            const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
+            o << "    " << ty << v << " = ";
             switch (x.op) {
-                case CONST: rhs = std::to_string(x.value) + "ull", canon[i] = x.value < gl::P; break;
-                case MAIN: rhs = "__ldg(" + std::string(x.b ? "MN" : "ML") + " + (" + std::to_string(x.a) + "ull << lq))", canon[i] = 1; break;
-                case AUX: {
-                    const std::string base = x.b ? "AN" : "AL";
-                    rhs = "gl::ef{__ldg(" + base + " + (" + std::to_string(2 * x.a) + "ull << lq)), __ldg(" + base + " + (" +
-                          std::to_string(2 * x.a + 1) + "ull << lq))}";
+                case CONST: o << x.value << "ull"; break;
+                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + (" << x.a << "ull << lq))"; break;
+                case AUX:
+                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + (" << 2 * x.a << "ull << lq)), __ldg("
+                      << (x.b ? "AN" : "AL") << " + (" << 2 * x.a + 1 << "ull << lq))}";
                     break;
-                }
-                case PUBLIC: rhs = "__ldg(K + " + std::to_string(A.kl.pub + x.a) + ")", canon[i] = 1; break;
+                case PUBLIC: o << "__ldg(K + " << A.kl.pub + x.a << ")"; break;
                 case RANDOMNESS:
-                    rhs = "gl::ef{__ldg(K + " + std::to_string(A.kl.rnd + 2 * x.a) + "), __ldg(K + " +
-                          std::to_string(A.kl.rnd + 2 * x.a + 1) + ")}";
+                    o << "gl::ef{__ldg(K + " << A.kl.rnd + 2 * x.a << "), __ldg(K + " << A.kl.rnd + 2 * x.a + 1 << ")}";
                     break;
                 case AUX_VALUE:
-                    rhs = "gl::ef{__ldg(K + " + std::to_string(A.kl.auxv + 2 * x.a) + "), __ldg(K + " +
-                          std::to_string(A.kl.auxv + 2 * x.a + 1) + ")}";
+                    o << "gl::ef{__ldg(K + " << A.kl.auxv + 2 * x.a << "), __ldg(K + " << A.kl.auxv + 2 * x.a + 1
+                      << ")}";
                     break;
-                case PERIODIC: rhs = "__ldg(PR + " + std::to_string(x.a) + ")", canon[i] = 1; break;
-                case IS_FIRST_ROW: rhs = "s_first", canon[i] = 1; break;
-                case IS_LAST_ROW: rhs = "s_last", canon[i] = 1; break;
-                case IS_TRANSITION: rhs = "s_trans", canon[i] = 1; break;
-                case ADD: case SUB:  // extension
-                    rhs = std::string("gl::ef_") + (x.op == ADD ? "add" : "sub") + "(" + as_ef(x.a) + ", " + as_ef(x.b) + ")";
+                case PERIODIC: o << "__ldg(PR + " << x.a << ")"; break;
+                case IS_FIRST_ROW: o << "s_first"; break;
+                case IS_LAST_ROW: o << "s_last"; break;
+                case IS_TRANSITION: o << "s_trans"; break;
+                case ADD: case SUB: {
+                    const char *f = x.op == ADD ? "add" : "sub";
+                    if (A.ext[i]) o << "gl::ef_" << f << "(" << as_ef(x.a) << ", " << as_ef(x.b) << ")";
+                    else o << "gl::" << f << "(v" << x.a << ", v" << x.b << ")";
                     break;
+                }
                 case MUL:
-                    if (!A.ext[i]) {
-                        const std::string ea = u_of(x.a), eb = u_of(x.b);
-                        rhs = "gl::mul_weak(" + ea + ", " + eb + ")";
-                    } else if (!A.ext[x.a]) rhs = "gl::ef_mulf(v" + std::to_string(x.b) + ", " + u_of(x.a) + ")";
-                    else if (!A.ext[x.b]) rhs = "gl::ef_mulf(v" + std::to_string(x.a) + ", " + u_of(x.b) + ")";
-                    else rhs = "gl::ef_mul(v" + std::to_string(x.a) + ", v" + std::to_string(x.b) + ")";
+                    if (!A.ext[i]) o << "gl::mul(v" << x.a << ", v" << x.b << ")";
+                    else if (!A.ext[x.a]) o << "gl::ef_mulf(v" << x.b << ", v" << x.a << ")";
+                    else if (!A.ext[x.b]) o << "gl::ef_mulf(v" << x.a << ", v" << x.b << ")";
+                    else o << "gl::ef_mul(v" << x.a << ", v" << x.b << ")";
                     break;
-                default:  // NEG, extension
-                    rhs = "gl::ef_neg(v" + std::to_string(x.a) + ")";
+                default:  // NEG
+                    o << (A.ext[i] ? "gl::ef_neg(v" : "gl::neg(v") << x.a << ")";
                     break;
             }
-            o << "    " << (A.ext[i] ? "const gl::ef " : "const uint64_t ") << v << " = " << rhs << ";\n";
+            o << ";\n";
         };
         o << "    gl::Acc f0, f1;\n    gl::ef fe = gl::ef_zero();\n";
         for (uint32_t k : ks) {
@@ -448,11 +389,9 @@ struct KArgs {
                 emit_node(i);
             }
             const uint64_t ap = A.kl.alpha + 2ull * k;
-            if (!A.ext[cn]) {
-                const std::string u = u_of(cn);
-                o << "    f0.mac(" << u << ", __ldg(K + " << ap << ")); f1.mac(" << u << ", __ldg(K + " << ap + 1
+            if (!A.ext[cn])
+                o << "    f0.mac(v" << cn << ", __ldg(K + " << ap << ")); f1.mac(v" << cn << ", __ldg(K + " << ap + 1
                   << "));\n";
-            }
             else
                 o << "    fe = gl::ef_add(fe, gl::ef_mul(v" << cn << ", gl::ef{__ldg(K + " << ap << "), __ldg(K + "
                   << ap + 1 << ")}));\n";
