@@ -40,6 +40,9 @@ METRIC = "proofs/s"
 # ncu summaries of the current kernels (profiles/): per-launch instruction
 # counts, pipe utilisation and DRAM traffic, each with the command that made it
 HASH_PROFILE = ROOT / "profiles" / "leaf_class_kernel_slab_2e18.json"
+# the same kernel writing the column-major rows the generated constraint
+# kernels read (the headline's main commit with a symbolic AIR)
+HASH_PROFILE_CM = ROOT / "profiles" / "leaf_class_kernel_cm_2e15.json"
 LDE_PROFILE = ROOT / "profiles" / "lde_kernels_slab_2e18.json"
 
 
@@ -272,7 +275,7 @@ def slab_widths(w: int):
 
 
 def hash_roofline(n_lde: int, w: int, leaf_ms: float, n_launches: int, hbm_peak: float, peak_src: str,
-                  sm_mhz):
+                  sm_mhz, profile: Path = HASH_PROFILE):
     """Roofline line of the dominant kernel, merkle::leaf_class_kernel (one
     launch per column slab). It is bound by the integer ALU pipe: achieved =
     this run's ALU-pipe warp instructions per second (the live launch time
@@ -290,20 +293,24 @@ def hash_roofline(n_lde: int, w: int, leaf_ms: float, n_launches: int, hbm_peak:
     base = {"kernel": "merkle::leaf_class_kernel (LMCS leaf sponge, Poseidon2-12)", "kernel_ms": launch_s * 1e3,
             "launches_per_proof": n_launches, "perms_per_launch": perms_per_launch,
             "perms_per_s": perms_per_launch / launch_s, "algorithmic_bytes": alg_bytes}
-    prof = load_profile(HASH_PROFILE)
+    prof = load_profile(profile)
     if not prof:
         return {**base, "bound": "hbm", "achieved": hbm_gbs, "peak": hbm_peak, "unit": "GB/s",
                 "frac": hbm_gbs / hbm_peak, "traffic": None, "peak_source": peak_src}
     alu_per_perm = prof["inst_alu"] / prof["perms_per_launch"]
-    peak_rate = prof["inst_alu"] / (prof["duration_ns"] * 1e-9) / (prof["alu_pct_of_peak"] / 100.0)
-    if sm_mhz and prof.get("sm_mhz"):
-        peak_rate *= sm_mhz / prof["sm_mhz"]
+    # the pipe's peak rate from the full-size slab capture (a small capture
+    # leaves SMs idle in its tail, which understates the rate)
+    pk = load_profile(HASH_PROFILE) or prof
+    peak_rate = pk["inst_alu"] / (pk["duration_ns"] * 1e-9) / (pk["alu_pct_of_peak"] / 100.0)
+    if sm_mhz and pk.get("sm_mhz"):
+        peak_rate *= sm_mhz / pk["sm_mhz"]
     achieved = perms_per_launch * alu_per_perm / launch_s
     return {**base, "bound": "int_alu", "achieved": achieved / 1e9, "peak": peak_rate / 1e9,
             "unit": "G warp-instructions/s (ALU pipe)", "frac": achieved / peak_rate,
             "traffic": prof["dram_bytes"] / prof["perms_per_launch"] * perms_per_launch,
             "alu_inst_per_perm": alu_per_perm, "issue_frac_in_profile": prof["issue_pct"] / 100.0,
-            "peak_source": f"ALU-pipe rate from {HASH_PROFILE.relative_to(ROOT)}", "hbm": hbm}
+            "peak_source": f"ALU-pipe rate from {HASH_PROFILE.relative_to(ROOT)}; instructions per permutation "
+                           f"and DRAM traffic from {profile.relative_to(ROOT)}", "hbm": hbm}
 
 
 def lde_roofline(w: int, B: int, lde_ms: float, hbm_peak: float, sm_mhz):
@@ -442,8 +449,13 @@ def run_gpu(args):
     perms = n_lde * ((w + 7) // 8) + n_lde - 1
     dominant = int(np.argmax(stages_ms))
     clk = clocks.summary()
+    cm = air is not P.AIR_KECCAK and HASH_PROFILE_CM.exists()
     roofline = hash_roofline(n_lde, w, float(np.mean(leaf_k)), int(leaf_n), hbm_peak,
-                             "measured" if "hbm_gbs" in pk else "fallback", clk.get("sm_mhz"))
+                             "measured" if "hbm_gbs" in pk else "fallback", clk.get("sm_mhz"),
+                             HASH_PROFILE_CM if cm else HASH_PROFILE)
+    if cm:
+        roofline["kernel"] = ("merkle::leaf_class_kernel<true> (LMCS leaf sponge, Poseidon2-12; also writes "
+                              "the column-major rows the generated constraint kernels read)")
     lde = lde_roofline(w, B, float(np.mean(lde_k)), hbm_peak, clk.get("sm_mhz"))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
