@@ -3,7 +3,8 @@
 //
 // Admission: a job is admitted while its estimated HBM footprint fits in the
 // budget still free (always when nothing else runs, so an oversized job
-// cannot starve), and at most one heavy job (job_is_heavy) runs at a time.
+// cannot starve), and at most one heavy job (job_is_heavy) runs at a time
+// (set_max_heavy changes the limit).
 // Jobs are taken in arrival order, except that light jobs may pass a heavy
 // job that waits for the running heavy one: they fill the GPU time the
 // heavy job leaves idle in its latency-bound phases. A worker keeps its job's LDEs,
@@ -30,11 +31,11 @@ inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, 
     const uint64_t B = 1ull << pcs.log_blowup;
     uint64_t D = 1;
     for (size_t i = 0; i < n; i++) D = std::max<uint64_t>(D, 1ull << inst_log_qd(inst[i]));
-    uint64_t words = 0, max_hw = 0, hmax = 0, max_cm = 0;
+    uint64_t words = 0, max_hw = 0, hmax = 0, cm_words = 0;
     for (size_t i = 0; i < n; i++) {
         const uint64_t hw = inst[i].height * inst[i].width, aw2 = 2 * inst_aux_width(inst[i]);
         if (inst[i].air == AIR_SYMBOLIC)  // column-major copies of gJ's rows for the generated kernels
-            max_cm += (inst[i].height << inst_log_qd(inst[i])) * (inst[i].width + aw2);
+            cm_words += (inst[i].height << inst_log_qd(inst[i])) * (inst[i].width + aw2);
         if (!inst[i].trace_on_device) words += hw;  // uploaded trace
         words += hw * B;                             // main LDE
         words += inst[i].height * aw2 * (B + 1);     // aux trace + LDE
@@ -44,7 +45,7 @@ inline uint64_t job_footprint_bytes(const PcsParams &pcs, const Instance *inst, 
     max_hw = std::max(max_hw, hmax * 2 * D);
     const uint64_t nl = hmax * B;
     words += max_hw;             // iNTT scratch
-    words += max_cm;             // symbolic AIRs: column-major LDE rows
+    words += cm_words;           // symbolic AIRs: column-major LDE rows
     words += 2 * hmax * D;       // quotient accumulator
     words += nl * 2 * D;         // quotient LDE
     words += 4 * nl;             // DEEP point quotients
