@@ -280,6 +280,33 @@ struct KArgs {
         std::string v = "v" + std::to_string(j);
         return A.ext[j] ? v : "gl::ef{" + v + ", 0}";
     };
+    // Two rewrites over the whole DAG (a node's readers can sit in any chunk):
+    // a base product read only by products (and the fold, which takes any
+    // value below 2^64) keeps its weakly reduced value, without the canonical
+    // step; a base (a + b) - (c + c) whose two inner sums have no other reader
+    // (the XOR of bits, a + b - 2ab) is emitted as (a - c) + (b - c).
+    std::vector<uint32_t> n_users(n, 0);
+    std::vector<uint8_t> only_mul(n, 1), is_root(n, 0), weak(n, 0), fused(n, 0);
+    for (uint32_t c : d.constraints) is_root[c] = 1;
+    for (size_t i = 0; i < n; i++) {
+        const Node &x = d.nodes[i];
+        auto use = [&](uint32_t j) {
+            n_users[j]++;
+            if (x.op != MUL) only_mul[j] = 0;
+        };
+        if (x.op == ADD || x.op == SUB || x.op == MUL) use(x.a), use(x.b);
+        if (x.op == NEG) use(x.a);
+    }
+    for (size_t i = 0; i < n; i++) {
+        const Node &x = d.nodes[i];
+        if (A.ext[i]) continue;
+        if (x.op == MUL && only_mul[i]) weak[i] = 1;
+        if (x.op == SUB && x.a != x.b) {
+            const Node &sa = d.nodes[x.a], &sb = d.nodes[x.b];
+            fused[i] = sa.op == ADD && sb.op == ADD && sb.a == sb.b && !A.ext[x.a] && !A.ext[x.b] &&
+                       n_users[x.a] == 1 && n_users[x.b] == 1 && !is_root[x.a] && !is_root[x.b];
+        }
+    }
     std::vector<uint8_t> live(n);
     for (size_t c = c0; c < c1; c++) {
         const std::vector<uint32_t> &ks = A.chunks[c];
@@ -353,12 +380,15 @@ struct KArgs {
                 case IS_TRANSITION: o << "s_trans"; break;
                 case ADD: case SUB: {
                     const char *f = x.op == ADD ? "add" : "sub";
-                    if (A.ext[i]) o << "gl::ef_" << f << "(" << as_ef(x.a) << ", " << as_ef(x.b) << ")";
+                    if (fused[i]) {
+                        const uint32_t a = d.nodes[x.a].a, b = d.nodes[x.a].b, c = d.nodes[x.b].a;
+                        o << "gl::add(gl::sub(v" << a << ", v" << c << "), gl::sub(v" << b << ", v" << c << "))";
+                    } else if (A.ext[i]) o << "gl::ef_" << f << "(" << as_ef(x.a) << ", " << as_ef(x.b) << ")";
                     else o << "gl::" << f << "(v" << x.a << ", v" << x.b << ")";
                     break;
                 }
                 case MUL:
-                    if (!A.ext[i]) o << "gl::mul(v" << x.a << ", v" << x.b << ")";
+                    if (!A.ext[i]) o << (weak[i] ? "gl::mul_weak(v" : "gl::mul(v") << x.a << ", v" << x.b << ")";
                     else if (!A.ext[x.a]) o << "gl::ef_mulf(v" << x.b << ", v" << x.a << ")";
                     else if (!A.ext[x.b]) o << "gl::ef_mulf(v" << x.a << ", v" << x.b << ")";
                     else o << "gl::ef_mul(v" << x.a << ", v" << x.b << ")";
@@ -381,6 +411,12 @@ struct KArgs {
                 const bool binary = x.op == ADD || x.op == SUB || x.op == MUL;
                 if (!expanded && (binary || x.op == NEG)) {
                     st.push_back({i, true});
+                    if (fused[i]) {  // (a + b) - (c + c): the inner sums are not emitted
+                        st.push_back({d.nodes[x.b].a, false});
+                        st.push_back({d.nodes[x.a].b, false});
+                        st.push_back({d.nodes[x.a].a, false});
+                        continue;
+                    }
                     if (binary) st.push_back({x.b, false});
                     st.push_back({x.a, false});
                     continue;
