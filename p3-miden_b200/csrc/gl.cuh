@@ -159,6 +159,54 @@ __device__ __forceinline__ uint64_t mul_weak(uint64_t a, uint64_t b) {
     mul128_dev(a, b, r0, r1, r2, r3);
     return reduce4_dev(r0, r1, r2, r3);
 }
+// Wide value lo + hi * 2^64 (below 2^96), an integer congruent mod p: a chain
+// of sums and differences accumulates here and is reduced once at its end.
+struct Wide {
+    uint64_t lo;
+    uint32_t hi;
+};
+__device__ __forceinline__ Wide wide_add(Wide a, Wide b) {  // the caller keeps a + b below 2^96
+    uint32_t r0, r1, h;
+    asm("add.cc.u32 %0, %3, %6;\n\t"
+        "addc.cc.u32 %1, %4, %7;\n\t"
+        "addc.u32 %2, %5, %8;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(h)
+        : "r"((uint32_t)a.lo), "r"((uint32_t)(a.lo >> 32)), "r"(a.hi), "r"((uint32_t)b.lo),
+          "r"((uint32_t)(b.lo >> 32)), "r"(b.hi));
+    return Wide{((uint64_t)r1 << 32) | r0, h};
+}
+// C - b for a constant multiple C = (c_hi : c_lo) of p with C >= b
+__device__ __forceinline__ Wide wide_neg(Wide b, uint64_t c_lo, uint32_t c_hi) {
+    uint32_t r0, r1, h;
+    asm("sub.cc.u32 %0, %6, %3;\n\t"
+        "subc.cc.u32 %1, %7, %4;\n\t"
+        "subc.u32 %2, %8, %5;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(h)
+        : "r"((uint32_t)b.lo), "r"((uint32_t)(b.lo >> 32)), "r"(b.hi), "r"((uint32_t)c_lo),
+          "r"((uint32_t)(c_lo >> 32)), "r"(c_hi));
+    return Wide{((uint64_t)r1 << 32) | r0, h};
+}
+// a + (C - b) = a - b (mod p), C as in wide_neg
+__device__ __forceinline__ Wide wide_sub(Wide a, Wide b, uint64_t c_lo, uint32_t c_hi) {
+    return wide_add(a, wide_neg(b, c_lo, c_hi));
+}
+// canonical value of a: lo + hi * eps (2^64 = eps mod p) with one wrap at
+// most, then one conditional subtraction of p
+__device__ __forceinline__ uint64_t wide_canon(Wide a) {
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 u0, u1, c;\n\t"
+        "sub.cc.u32 u0, 0, %4;\n\t"  // hi*eps = (hi << 32) - hi
+        "subc.u32 u1, %4, 0;\n\t"
+        "add.cc.u32 %0, %2, u0;\n\t"
+        "addc.cc.u32 %1, %3, u1;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"          // on carry add eps
+        "add.cc.u32 %0, %0, c;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "r"((uint32_t)a.lo), "r"((uint32_t)(a.lo >> 32)), "r"(a.hi));
+    return canon_dev(((uint64_t)r1 << 32) | r0);
+}
 #endif
 #if defined(__CUDACC__)
 // Lazy sum of products: sum a_i * b_i held in 160 bits (r4 counts the

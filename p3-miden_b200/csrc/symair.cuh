@@ -307,6 +307,21 @@ struct KArgs {
                        n_users[x.a] == 1 && n_users[x.b] == 1 && !is_root[x.a] && !is_root[x.b];
         }
     }
+    // A third: a chain of sums and differences whose inner links each have one
+    // reader, itself a link (such as the Horner recombination of a limb from
+    // its bits, acc + acc + bit), is accumulated as a Wide and reduced once at
+    // the chain's end (inner[i]: i is such a link).
+    std::vector<uint8_t> linear(n, 0), inner(n, 0);
+    std::vector<int64_t> reader(n, -1);  // the one node reading i, -1 for none, -2 for several
+    for (size_t i = 0; i < n; i++) {
+        const Node &x = d.nodes[i];
+        linear[i] = !A.ext[i] && !fused[i] && (x.op == ADD || x.op == SUB || x.op == NEG);
+        auto read = [&](uint32_t j) { reader[j] = reader[j] == -1 || reader[j] == (int64_t)i ? (int64_t)i : -2; };
+        if (x.op == ADD || x.op == SUB || x.op == MUL) read(x.a), read(x.b);
+        if (x.op == NEG) read(x.a);
+    }
+    for (size_t i = 0; i < n; i++)
+        inner[i] = linear[i] && !is_root[i] && reader[i] >= 0 && linear[reader[i]];
     std::vector<uint8_t> live(n);
     for (size_t c = c0; c < c1; c++) {
         const std::vector<uint32_t> &ks = A.chunks[c];
@@ -354,7 +369,52 @@ struct KArgs {
         // constraints into an extension sum.
         std::vector<uint8_t> done(n, 0);
         std::vector<std::pair<uint32_t, bool>> st;
+        std::vector<uint8_t> bits(n, 64);
+        // a multiple of p at or above 2^b (64 <= b <= 95), as "lo, hi"
+        auto p_multiple = [](unsigned b) {
+            const unsigned __int128 c = (unsigned __int128)gl::P << (b - 63);  // p * 2^t > 2^(63 + t)
+            return std::to_string((uint64_t)c) + "ull, " + std::to_string((uint32_t)(c >> 64)) + "u";
+        };
+        // a chain link or the end of a chain: Wide arithmetic on its operands
+        auto emit_wide = [&](size_t i) -> bool {
+            const Node &x = d.nodes[i];
+            if (!linear[i] || !(inner[x.a] || (x.op != NEG && inner[x.b]) || inner[i])) return false;
+            auto operand = [&](uint32_t j, unsigned &b) -> std::string {
+                if (inner[j]) {
+                    b = bits[j];
+                    return "w" + std::to_string(j);
+                }
+                b = 64;
+                return "gl::Wide{v" + std::to_string(j) + ", 0}";
+            };
+            unsigned ba = 64, bb = 64, nb;
+            std::string ea = operand(x.a, ba), eb = x.op == NEG ? "" : operand(x.b, bb);
+            nb = x.op == ADD ? std::max(ba, bb) + 1 : x.op == SUB ? std::max(ba, bb + 1) + 1 : ba + 1;
+            if (nb > 95) {  // close the operands' chains here (each is read by this node only)
+                for (uint32_t j : {x.a, x.b}) {
+                    if (x.op == NEG && j == x.b) continue;
+                    if (inner[j] && bits[j] > 64) {
+                        o << "    const uint64_t v" << j << " = gl::wide_canon(w" << j << ");\n";
+                        inner[j] = 0;
+                    }
+                }
+                ea = operand(x.a, ba);
+                if (x.op != NEG) eb = operand(x.b, bb);
+                nb = x.op == ADD ? std::max(ba, bb) + 1 : x.op == SUB ? std::max(ba, bb + 1) + 1 : ba + 1;
+            }
+            std::string rhs = x.op == ADD   ? "gl::wide_add(" + ea + ", " + eb + ")"
+                              : x.op == SUB ? "gl::wide_sub(" + ea + ", " + eb + ", " + p_multiple(bb) + ")"
+                                            : "gl::wide_neg(" + ea + ", " + p_multiple(ba) + ")";
+            if (inner[i]) {
+                o << "    const gl::Wide w" << i << " = " << rhs << ";\n";
+                bits[i] = (uint8_t)nb;
+            } else {
+                o << "    const uint64_t v" << i << " = gl::wide_canon(" << rhs << ");\n";
+            }
+            return true;
+        };
         auto emit_node = [&](size_t i) {
+            if (emit_wide(i)) return;
             const Node &x = d.nodes[i];
             const std::string v = "v" + std::to_string(i);
             const char *ty = A.ext[i] ? "const gl::ef " : "const uint64_t ";
