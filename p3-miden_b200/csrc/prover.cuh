@@ -336,7 +336,6 @@ inline void eval_symbolic(Ctx &ctx, const Instance &I, uint64_t *cm, const uint6
     for (size_t i = 0; i < alpha_pows.size(); i++) k[A.kl.alpha + i] = alpha_pows[i];
     DBuf dk = ctx.upload(k.empty() ? std::vector<uint64_t>{0} : k);
     const uint64_t h = 1ull << log_h, qh = h << log_qd, D = 1ull << log_qd;
-    if (qh > (1ull << 31)) throw CudaError{ERR_INVALID, "symbolic AIR: quotient domain above 2^31 rows"};
     const uint64_t shift = gl::exp2k(gl::GEN, log_max_h - log_h);
     DBuf per_nat;
     uint64_t per_h = 0;

@@ -343,13 +343,12 @@ struct KArgs {
         o << R"K(    const uint64_t rl = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (rl >= a.qh) return;
     const uint32_t lq = a.log_qh;
-    const uint32_t qs = (uint32_t)a.qh;  // column stride of the column-major copies (qh <= 2^31)
     const uint64_t m = gl::bitrev(rl, lq), rn = gl::bitrev((m + a.D) & (a.qh - 1), lq);
     const uint64_t *ML = a.main + rl, *MN = a.main + rn;
     const uint64_t *AL = a.aux ? a.aux + rl : a.aux, *AN = a.aux ? a.aux + rn : a.aux;
     const uint64_t *PR = a.per ? a.per + (m % a.per_h) * a.per_w : a.per;
     const uint64_t *K = a.k;
-    (void)ML; (void)MN; (void)AL; (void)AN; (void)PR; (void)K; (void)lq; (void)qs;
+    (void)ML; (void)MN; (void)AL; (void)AN; (void)PR; (void)K; (void)lq;
 )K";
         if (first || last || trans) {
             o << "    const uint64_t mlo = m & ((1ull << a.wq_lo_bits) - 1), mhi = m >> a.wq_lo_bits;\n"
@@ -422,10 +421,10 @@ struct KArgs {
             o << "    " << ty << v << " = ";
             switch (x.op) {
                 case CONST: o << x.value << "ull"; break;
-                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + " << x.a << "ull * qs)"; break;
+                case MAIN: o << "__ldg(" << (x.b ? "MN" : "ML") << " + (" << x.a << "ull << lq))"; break;
                 case AUX:
-                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + " << 2 * x.a << "ull * qs), __ldg("
-                      << (x.b ? "AN" : "AL") << " + " << 2 * x.a + 1 << "ull * qs)}";
+                    o << "gl::ef{__ldg(" << (x.b ? "AN" : "AL") << " + (" << 2 * x.a << "ull << lq)), __ldg("
+                      << (x.b ? "AN" : "AL") << " + (" << 2 * x.a + 1 << "ull << lq))}";
                     break;
                 case PUBLIC: o << "__ldg(K + " << A.kl.pub + x.a << ")"; break;
                 case RANDOMNESS:
