@@ -135,6 +135,36 @@ def miden_trace(width: int, log_h: int, seed: int) -> np.ndarray:
     return t
 
 
+# ---------------------------------------------------------------- chains
+def chains_eval(b):
+    """Linear chains for the code generator's rewrites: a 60-step Horner chain
+    over differences (its 96-bit accumulation reaches the 2^95 bound and is
+    closed and restarted), the XOR form a + b - (c + c), and a negation inside
+    a chain; column 7 holds their combination."""
+    L, _ = b.main()
+    acc = b.const(0)
+    for k in range(60):
+        acc = acc + acc + (L[k % 7] - L[(k + 2) % 7])
+    prod = L[0] * L[1]
+    x = L[0] + L[1] - (prod + prod)
+    y = -(L[2] - L[3]) + L[4] + L[4]
+    b.assert_zero(L[7] - acc - x * y)
+
+
+def chains_trace(log_h: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    t = rng.integers(0, P, size=(1 << log_h, 8), dtype=np.uint64)
+    for r in range(1 << log_h):
+        c = [int(v) for v in t[r, :7]]
+        acc = 0
+        for k in range(60):
+            acc = (2 * acc + c[k % 7] - c[(k + 2) % 7]) % P
+        x = (c[0] + c[1] - 2 * c[0] * c[1]) % P
+        y = (-(c[2] - c[3]) + 2 * c[4]) % P
+        t[r, 7] = (acc + x * y) % P
+    return t
+
+
 # ---------------------------------------------------------------- keccak
 # The Keccak AIR's symbolic form is part of the package (p3_miden_b200.airs),
 # where the bench also takes it from.

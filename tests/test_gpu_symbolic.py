@@ -190,3 +190,17 @@ def test_chunk_size_does_not_change_the_proof(product):
             ctx.set_air_chunk_nodes(3)
     finally:
         ctx.close()
+
+
+def test_linear_chain_rewrites_match_oracle(product, gpu_ctx):
+    """The generated code's rewrites (96-bit chains closed at the 2^95 bound,
+    the XOR form, weakly reduced products) give the oracle's proof."""
+    desc = product.build_air(S.chains_eval, 8)
+    src = product.air_source(desc)
+    assert "gl::wide_canon(" in src and "gl::add(gl::sub(" in src
+    air = product.Air(gpu_ctx, desc)
+    t = S.chains_trace(8, 5)
+    pcs = product.PcsParams(1, 1, 0, 8, 0, 24, 0)
+    gpu = product.prove_multi(gpu_ctx, pcs, [product.AirWitness(air, t)])
+    check_same(gpu, O.prove(O.default_p2(), pcs_dict(pcs), [(O.AIR_SYMBOLIC, t, None, {"sym": desc})]))
+    assert product.verify_output(gpu_ctx, pcs, [product.AirShape(air, 256, 8)], gpu).ok

@@ -148,3 +148,17 @@ def test_oracle_symbolic_keccak_equals_builtin(product):
     b = O.prove(O.default_p2(), pcs, [(O.AIR_KECCAK, t, None, {"sym": desc})])
     for key in ("fields", "commits", "digest"):
         assert np.array_equal(a[key], b[key]), key
+
+
+def test_chains_air_holds_on_its_trace(product):
+    """The rewrite test AIR's trace satisfies its constraint (oracle's
+    symbolic evaluation on the CPU), so its GPU proof must verify."""
+    desc = product.build_air(S.chains_eval, 8)
+    t = S.chains_trace(4, 5)
+    pcs = dict(log_blowup=1, log_folding_arity=1, log_final_degree=0, folding_pow_bits=4, deep_pow_bits=0,
+               num_queries=8, query_pow_bits=0)
+    out = O.prove(O.default_p2(), pcs, [(O.AIR_SYMBOLIC, t, None, {"sym": desc})])
+    assert O.verify(O.default_p2(), pcs, [(O.AIR_SYMBOLIC, t.shape[0], t.shape[1], None, {"sym": desc})],
+                    out["fields"], out["commits"], out["digest"]) == 0
+    # the generated source of this AIR compiles for sm_100a without a device
+    assert product.air_compile_check(desc) > 0
