@@ -139,8 +139,9 @@ def miden_trace(width: int, log_h: int, seed: int) -> np.ndarray:
 def chains_eval(b):
     """Linear chains for the code generator's rewrites: a 60-step Horner chain
     over differences (its 96-bit accumulation reaches the 2^95 bound and is
-    closed and restarted), the XOR form a + b - (c + c), and a negation inside
-    a chain; column 7 holds their combination."""
+    closed and restarted), the XOR form a + b - (c + c), a negation inside a
+    chain and a product read only by a product; column 7 holds their
+    combination."""
     L, _ = b.main()
     acc = b.const(0)
     for k in range(60):
@@ -148,7 +149,8 @@ def chains_eval(b):
     prod = L[0] * L[1]
     x = L[0] + L[1] - (prod + prod)
     y = -(L[2] - L[3]) + L[4] + L[4]
-    b.assert_zero(L[7] - acc - x * y)
+    z = (L[5] * L[6]) * L[5]  # a product read only by a product
+    b.assert_zero(L[7] - acc - x * y - z)
 
 
 def chains_trace(log_h: int, seed: int) -> np.ndarray:
@@ -161,7 +163,7 @@ def chains_trace(log_h: int, seed: int) -> np.ndarray:
             acc = (2 * acc + c[k % 7] - c[(k + 2) % 7]) % P
         x = (c[0] + c[1] - 2 * c[0] * c[1]) % P
         y = (-(c[2] - c[3]) + 2 * c[4]) % P
-        t[r, 7] = (acc + x * y) % P
+        t[r, 7] = (acc + x * y + c[5] * c[6] * c[5]) % P
     return t
 
 

@@ -197,7 +197,7 @@ def test_linear_chain_rewrites_match_oracle(product, gpu_ctx):
     the XOR form, weakly reduced products) give the oracle's proof."""
     desc = product.build_air(S.chains_eval, 8)
     src = product.air_source(desc)
-    assert "gl::wide_canon(" in src and "gl::add(gl::sub(" in src
+    assert "gl::wide_canon(" in src and "gl::add(gl::sub(" in src and "gl::mul_weak(" in src
     air = product.Air(gpu_ctx, desc)
     t = S.chains_trace(8, 5)
     pcs = product.PcsParams(1, 1, 0, 8, 0, 24, 0)
