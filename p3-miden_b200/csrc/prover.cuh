@@ -453,12 +453,10 @@ inline std::vector<uint64_t> deep_evals(Ctx &ctx, Launcher &L, const std::vector
             uint64_t col_tiles = (m->w + 31) / 32;
             // one wave of resident blocks: as many row chunks as fit beside the
             // column tiles (a second, partial wave would double the time)
-            static int bps = 0, sms = 0;
-            if (!bps) {
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, deep::colsum_kernel, 256, 0));
-                CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
-                bps = std::max(1, bps);
-            }
+            int bps = 0, sms = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, deep::colsum_kernel, 256, 0));
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+            bps = std::max(1, bps);
             const uint64_t target_blocks = (uint64_t)sms * bps;
             uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(dm / 64 + 1, target_blocks / col_tiles));
             uint64_t rpc = (dm + n_chunks - 1) / n_chunks;
