@@ -278,11 +278,8 @@ P3G_API int p3g_cubic_trace_device(p3g_ctx *x, uint32_t log_height, uint64_t wid
         p3g::DBuf d = x->c.upload(kr);
         const int threads = (int)std::min<uint64_t>(1024, (width + 31) / 32 * 32);
         const size_t smem = 2 * width * 8;
-        static std::once_flag attr_once;
-        std::call_once(attr_once, [] {
-            CK(cudaFuncSetAttribute(tgen::cubic_trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(2 * tgen::kCubicMaxWidth * 8)));
-        });
+        static std::atomic<uint64_t> attr_done{0};
+        p3g::smem_attr_once(attr_done, tgen::cubic_trace_kernel, (int)(2 * tgen::kCubicMaxWidth * 8));
         tgen::cubic_trace_kernel<<<1, threads, smem, x->c.stream>>>(d.p + width, d.p, width, 1ull << log_height, d_out);
         CK(cudaGetLastError());
         x->c.launches++;

@@ -5,6 +5,7 @@
 
 #include <cstdio>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <chrono>
 #include <map>
@@ -43,6 +44,19 @@ inline void check(cudaError_t e, const char *what) {
     }
 }
 #define CK(x) ::p3g::check((x), #x)
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) for a kernel, once per
+// device (function attributes belong to each device's copy of the module);
+// `done` is the call site's bit set of devices already set.
+template <typename K>
+inline void smem_attr_once(std::atomic<uint64_t> &done, K kernel, int bytes) {
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "cudaFuncSetAttribute");
+    done.fetch_or(bit, std::memory_order_release);
+}
 
 inline unsigned log2u(uint64_t n) {
     unsigned l = 0;
@@ -432,11 +446,8 @@ inline void launch_lde_pass(Ctx &ctx, const lde::PassArgs &a, uint64_t groups, u
     const uint32_t G = 1u << a.k;
     const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
     const size_t smem = ((size_t)G * C + G) * 8;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(lde::lde_pass_kernel<C, DIF, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (1024 * C + 1024) * 8));
-    });
+    static std::atomic<uint64_t> attr_done{0};
+    smem_attr_once(attr_done, lde::lde_pass_kernel<C, DIF, KT>, (1024 * C + 1024) * 8);
     lde::lde_pass_kernel<C, DIF, KT><<<dim3((unsigned)(groups * a.n_tiles), n_blocks_y), threads, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;
@@ -446,11 +457,8 @@ inline void launch_lde_fused(Ctx &ctx, const lde::FusedArgs &a, uint64_t groups)
     const uint32_t G = 1u << a.k;
     const unsigned threads = (G >= 8 ? G / 8 : 1) * C;
     const size_t smem = (2 * (size_t)G * C + 3 * (size_t)G) * 8;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
-        CK(cudaFuncSetAttribute(lde::lde_fused_kernel<C, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (2 * 1024 * C + 3 * 1024) * 8));
-    });
+    static std::atomic<uint64_t> attr_done{0};
+    smem_attr_once(attr_done, lde::lde_fused_kernel<C, KT>, (2 * 1024 * C + 3 * 1024) * 8);
     lde::lde_fused_kernel<C, KT><<<(unsigned)(groups * a.n_tiles), threads, smem, ctx.stream>>>(a);
     CK(cudaGetLastError());
     ctx.launches++;

@@ -522,11 +522,8 @@ inline DBuf deep_assemble(Ctx &ctx, Launcher &L, const std::vector<const Mat *> 
             const uint64_t *cf = d_coef.p + 2 * off;
             if (m->w >= 16) {
                 size_t smem = 16 * m->w;
-                static std::once_flag attr_once;
-                std::call_once(attr_once, [] {
-                    CK(cudaFuncSetAttribute(deep::rowdot_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            200 * 1024));
-                });
+                static std::atomic<uint64_t> attr_done{0};
+                smem_attr_once(attr_done, deep::rowdot_warp_kernel, 200 * 1024);
                 unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(m->h * 32, 256), 148 * 16);
                 L(deep::rowdot_warp_kernel, grid, 256, smem, m->d, m->h, m->w, cf, dots[mi].p);
             } else {
@@ -712,11 +709,8 @@ inline void prove(Ctx &ctx, const PcsParams &pcs, const Instance *inst, size_t n
         a.acc = acc.p;
         if (I.air == AIR_CUBIC) L(quot::cubic_eval_kernel, blocks_for(qh * 32, 256), 256, 0, a);
         else {
-            static std::once_flag attr_once;
-            std::call_once(attr_once, [] {
-                CK(cudaFuncSetAttribute(quot::keccak_eval_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)quot::KEC_SMEM_MAX));
-            });
+            static std::atomic<uint64_t> attr_done{0};
+            smem_attr_once(attr_done, quot::keccak_eval_block_kernel, (int)quot::KEC_SMEM_MAX);
             int dev_sms = 148, per_sm = 1;
             CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx.device));
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, quot::keccak_eval_block_kernel,
